@@ -1,0 +1,336 @@
+"""Refactor + solve throughput of the B200 engine on the 200k-row circuit system.
+
+Workload ("circuit-200k"): n = 200,000, ~1,000 Pareto(1.5, x_m = 10) diagonal
+blocks clipped to [1, 20000] plus 1x1 blocks, 6 stored entries per row on
+average, 50 bus rows/columns of 500 entries, log-uniform magnitudes in
+[1e-3, 1e3], random P/Q, seed 20262203 (synthetic stand-in, no dataset).
+One analyze + first factor (untimed), then steps of one value-only refactor
+(values x (1 + U(-0.1, 0.1)), fresh per step) followed by one 1-RHS solve.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Prints one JSON line on rank 0.  `value` is device-timed (inputs resident in
+HBM, CUDA events per step on the launching stream, L2 flushed between steps
+outside the timed window); `e2e` runs the same steps through the public C ABI
+call bdlu_refactor_solve with host buffers (values and b copied in, x copied
+out, every step).  Under torchrun each rank runs an independent replica
+(replicas only: one system is solved per GPU, no collective on the data path)
+and the slowest rank's time is used.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "block-daglu_b200")]
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = "circuit-200k"
+METRIC = "refactor+solves/s"
+N_ROWS = 200000
+CONFIG_INDEX = 1
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        return False
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def circuit_system():
+    import blockdaglu as bd
+    return bd.Synth(bd.FAMILY_CIRCUIT, bd.config_seed(CONFIG_INDEX), N_ROWS)
+
+
+def step_inputs(g, k):
+    """Values and b of step k: values x (1 + U(-0.1, 0.1)), b = A_k x_true."""
+    v = g.perturbed(1_000_003 + k)
+    b = np.zeros(g.n)
+    np.add.at(b, g.rows, v * g.x_true[g.cols, 0])
+    return v, b
+
+
+def cpu_baseline_port(g):
+    """Oracle port on the host: one full refactor + solve of the same system."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import blockdaglu as bd
+    import oracle
+    s = bd.Solver()
+    s.set_option("analysis_only", 1)
+    assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze()
+    d = s.decomposition()
+    v, b = step_inputs(g, 0)
+    t0 = time.perf_counter()
+    ref = oracle.System(g.n, g.rows, g.cols, v, d["P"], d["Q"], d["R"])
+    ok = ref.factor()
+    x = ref.solve(b)
+    dt = time.perf_counter() - t0
+    resid = oracle.metrics(g.rows, g.cols, v, x, b)[0]
+    return {"value": 1.0 / dt, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": "1 value-only refactor + 1-RHS solve of the full %s system by the oracle "
+                      "(reference dense micro-kernel on every merged block, reverse block solve, "
+                      "single thread): %.1f s, residual %.1e%s" % (WORKLOAD, dt, resid, "" if ok else ", FAILED")}
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU route on the same workload (rank 0 only)."""
+    if rank != 0:
+        return
+    g = circuit_system()
+    steps = max(1, min(args.steps, 2))
+    warm = 1 if args.warmup > 0 else 0
+    times = []
+    for k in range(warm + steps):
+        base = cpu_baseline_port(g)
+        if k >= warm:
+            times.append(1.0 / base["value"])
+    t = statistics.mean(times)
+    line = {"metric": METRIC, "value": 1.0 / t, "unit": METRIC, "n_gpus": args.gpus, "steps": steps,
+            "warmup": warm, "ms_per_step": 1000.0 * t, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n": g.n, "nnz": int(g.nnz), "nrhs": 1},
+            "impl": "reference",
+            "cpu_baseline": {"value": 1.0 / t, "unit": METRIC, "cores": 1, "kind": "port",
+                             "sample": "%d timed full refactor+solve steps (of --steps %d, bounded to keep the run "
+                                       "within minutes) by the oracle port; SuiteSparse KLU is unavailable on this "
+                                       "box" % (steps, args.steps)},
+            "e2e": {"value": 1.0 / t, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    import blockdaglu as bd
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    g = circuit_system()
+    s = bd.Solver()
+    assert s.set_matrix((g.rows, g.cols, g.vals), g.n), s.last_error_message()
+    t0 = time.perf_counter()
+    assert s.analyze(), s.last_error_message()
+    analyze_s = time.perf_counter() - t0
+    assert s.factor(), s.last_error_message()
+    first = s.stats()
+    nnz = int(g.nnz)
+    total = args.warmup + args.steps
+    inputs = [step_inputs(g, k) for k in range(total)]
+    d_vals = [torch.from_numpy(v).to(dev) for v, _ in inputs]
+    d_b = [torch.from_numpy(b).to(dev) for _, b in inputs]
+    d_x = torch.empty(g.n, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    sh = stream.cuda_stream
+
+    def device_step(k):
+        assert s.refactor_values_device(d_vals[k].data_ptr(), nnz, sh), s.last_error_message()
+        assert s.solve_device(d_x.data_ptr(), g.n, 1, sh), s.last_error_message()
+
+    # Warm-up (untimed).
+    for k in range(args.warmup):
+        d_x.copy_(d_b[k])
+        device_step(k)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms, phases, resid, launches = [], [], [], []
+    with ClockSampler(local) as clocks:
+        for k in range(args.warmup, total):
+            flush.fill_(float(k))
+            d_x.copy_(d_b[k])
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            device_step(k)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            phases.append(s.phase_times())
+            st = s.stats()
+            launches.append(st["factor_launches"] + st["solve_launches"] + 0)
+            x = d_x.cpu().numpy()
+            v, b = inputs[k]
+            r = b.copy()
+            np.subtract.at(r, g.rows, v * x[g.cols])
+            arow = np.zeros(g.n)
+            np.add.at(arow, g.rows, np.abs(v))
+            resid.append(float(np.max(np.abs(r)) / (arow.max() * np.max(np.abs(x)) + np.max(np.abs(b)))))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    my_ms = float(sum(step_ms))
+    if dist:
+        t = torch.tensor([my_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        my_ms = float(t.item())
+    ms_per_step = my_ms / args.steps
+    value = world * 1000.0 / ms_per_step
+
+    # End to end through the C ABI with pinned host buffers.
+    pin_v = [torch.from_numpy(v).pin_memory() for v, _ in inputs[: args.warmup + args.steps]]
+    pin_b = torch.empty(g.n, dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    for k in range(total):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        pin_b.copy_(torch.from_numpy(inputs[k][1]))
+        t0 = time.perf_counter()
+        ok = s._lib.bdlu_refactor_solve(s._h, bd._p64(pin_v[k].numpy()), nnz, bd._p64(pin_b.numpy()), g.n, 1)
+        dt = (time.perf_counter() - t0) * 1000.0
+        assert ok == 0, s.last_error_message()
+        if k >= args.warmup:
+            e2e_ms.append(dt)
+    e2e = world * 1000.0 / statistics.mean(e2e_ms)
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    # Roofline of the dominant phase.
+    ph = {key: statistics.mean(p[key] for p in phases) for key in phases[0]}
+    dominant = max(("lu_small", "lu_large", "solve"), key=lambda key: ph[key])
+    peaks = measured_peaks()
+    dgemm = None
+    if dominant in ("lu_small", "lu_large"):
+        n8 = 8192
+        a = torch.randn(n8, n8, dtype=torch.float64, device=dev)
+        torch.matmul(a, a)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = 1e30
+        for _ in range(3):
+            e0.record()
+            torch.matmul(a, a)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        dgemm = 2.0 * n8 ** 3 / (best * 1e-3) / 1e12
+        del a
+    flops_large = first["factor_flops"]  # both dense classes; split below
+    roofline = None
+    if dominant == "solve":
+        traffic = 8 * first["dense_entries"] + 12 * first["nnz_offdiag"] + 8 * 4 * g.n
+        achieved = traffic / (ph["solve"] * 1e-3) / 1e9
+        peak = peaks.get("hbm_gbs", 6650.0)
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": None, "kernel": "solve sweep (k_solve_scalar/k_solve_dense levels)",
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"}
+    else:
+        achieved = flops_large / (ph["lu_small"] + ph["lu_large"]) / 1e9
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": dgemm, "unit": "TFLOP/s",
+                    "frac": achieved / dgemm if dgemm else None, "traffic": None,
+                    "kernel": "dense block LU (k_lu_small + k_panel/k_swap_trsm/k_gemm_update), FP64",
+                    "peak_source": "FP64 pipe: torch.matmul float64 8192^3 measured in this run "
+                                   "(MEASURED_PEAKS.json has no FP64 figure)"}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_port(g)
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": g.n, "nnz": nnz, "nrhs": 1, "nblocks": first["nblocks"],
+                   "nunits": first["nunits"], "max_block": first["max_unit"], "unit_levels": first["unit_levels"],
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed (256 MiB write) between timed steps, outside the step window",
+                   "analyze_s": analyze_s},
+        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8 * nnz + 8 * g.n, "d2h_bytes_per_step": 8 * g.n},
+        "phases_ms": ph,
+        "residual_inf_max": max(resid),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+        "gpu_launches": int(sum(launches)),
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

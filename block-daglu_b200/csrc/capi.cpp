@@ -1,0 +1,371 @@
+// C ABI (include/bdlu.h): the Solver state machine of blockdaglu/src/solver.cpp
+// (set_matrix :749-800, analyze :802-1182, factor :1184-1350, solve_in_place
+// :1352-1539, exports :1541-1725) over the GPU engine.  No exception crosses
+// the boundary; every failure maps to a status code and a message.
+#include <cuda_runtime_api.h>
+
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "analysis.h"
+#include "bdlu.h"
+#include "capi_internal.h"
+#include "engine.h"
+#include "plan.h"
+
+using bdlu::Status;
+
+namespace {
+
+int fail(bdlu_solver* h, int code, std::string msg) {
+  h->last_error = code;
+  h->last_message = std::move(msg);
+  return code;
+}
+
+void clear_error(bdlu_solver* h) {
+  h->last_error = BDLU_OK;
+  h->last_message.clear();
+}
+
+int refine_iters_for(const bdlu_solver* h) {
+  if (h->refine_iters >= 0) return h->refine_iters;
+  if (const char* e = bdlu::getenv_compat("USERALGO_REFINE_ITERS")) {
+    const int v = std::atoi(e);
+    if (v >= 0) return v;
+  }
+  return 0;
+}
+
+int pick_mode() {
+  // solver.cpp:824-841: unknown values fall back to AUTO.
+  if (const char* e = bdlu::getenv_compat("USERALGO_MODE")) {
+    std::string v(e);
+    for (auto& c : v) c = static_cast<char>(std::tolower(static_cast<unsigned char>(c)));
+    if (v == "klu") return BDLU_MODE_KLU;
+    if (v == "block") return BDLU_MODE_BLOCK;
+  }
+  return BDLU_MODE_AUTO;
+}
+
+// Runs validation + canonicalisation once (solver.cpp:806-819).
+int ensure_validated(bdlu_solver* h) {
+  if (h->validated) return BDLU_OK;
+  std::string msg;
+  const Status st = bdlu::canonicalize(h->in_rows.data(), h->in_cols.data(), h->in_vals.data(),
+                                       static_cast<int64_t>(h->in_rows.size()), h->dimension_hint, h->coo, msg);
+  if (st != Status::Ok) return fail(h, static_cast<int>(st), msg);
+  h->n = h->coo.n;
+  h->validated = true;
+  return BDLU_OK;
+}
+
+int do_factor(bdlu_solver* h, cudaStream_t stream) {
+  std::string err;
+  if (!h->engine->factor_async(h->engine->values_buffer(), stream, err))
+    return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+  if (!h->engine->factor_status(stream, err)) {
+    h->factored = false;
+    return fail(h, BDLU_FACTORIZATION_FAILED, err);
+  }
+  h->factored = true;
+  h->exported = false;
+  return BDLU_OK;
+}
+
+int upload_values(bdlu_solver* h, const double* vals, bool device, cudaStream_t stream) {
+  const size_t bytes = static_cast<size_t>(h->engine->nnz()) * sizeof(double);
+  const cudaError_t e = cudaMemcpyAsync(h->engine->values_buffer(), vals, bytes,
+                                        device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return fail(h, BDLU_BACKEND_UNAVAILABLE, std::string("value upload: ") + cudaGetErrorString(e));
+  return BDLU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+bdlu_solver* bdlu_create(void) {
+  try {
+    return new bdlu_solver();
+  } catch (...) {
+    return nullptr;
+  }
+}
+
+void bdlu_destroy(bdlu_solver* h) { delete h; }
+
+int bdlu_set_coo(bdlu_solver* h, const int32_t* rows, const int32_t* cols, const double* vals, int64_t nnz,
+                 int32_t dimension) {
+  if (!h) return BDLU_NOT_PREPARED;
+  clear_error(h);
+  if (dimension < -1) return fail(h, BDLU_INVALID_DIMENSION, "matrix dimension must be non-negative");
+  if (nnz < 0 || (nnz > 0 && (!rows || !cols || !vals))) return fail(h, BDLU_INVALID_INDEX, "invalid COO arrays");
+  try {
+    h->engine.reset();
+    h->in_rows.assign(rows, rows + nnz);
+    h->in_cols.assign(cols, cols + nnz);
+    h->in_vals.assign(vals, vals + nnz);
+    h->coo = bdlu::CanonicalCoo{};
+    h->dec = bdlu::Decomposition{};
+  } catch (const std::exception& e) {
+    return fail(h, BDLU_ANALYSIS_FAILED, e.what());
+  }
+  // Storage only (solver.cpp:771-774): validation is deferred to analyze.
+  h->dimension_hint = dimension;
+  h->n = dimension >= 0 ? dimension : -1;
+  h->prepared = true;
+  h->validated = false;
+  h->decomposed = false;
+  h->factored = false;
+  h->exported = false;
+  h->mode = BDLU_MODE_AUTO;
+  h->global_route = false;
+  return BDLU_OK;
+}
+
+int bdlu_analyze(bdlu_solver* h) {
+  if (!h) return BDLU_NOT_PREPARED;
+  clear_error(h);
+  if (!h->prepared) return fail(h, BDLU_NOT_PREPARED, "set_matrix must be called before analyze");
+  if (const int st = ensure_validated(h)) return st;
+  h->sig = bdlu::matrix_sig(h->n, h->coo);
+  h->sig2 = bdlu::matrix_sig2(h->n, h->coo);
+  h->value_sig = bdlu::matrix_value_sig(h->coo);
+  h->mode = pick_mode();
+  // The GPU engine runs the block route under AUTO; "klu" forces the global
+  // route, which here means one diagonal block with partial pivoting.
+  h->global_route = (h->mode == BDLU_MODE_KLU);
+  h->decomposed = false;
+  h->factored = false;
+  h->exported = false;
+  try {
+    bdlu::AnalysisOptions opt = bdlu::analysis_options_from_env();
+    opt.single_block = h->global_route;
+    h->dec = bdlu::build_decomposition(h->coo, opt);
+    if (h->analysis_only) {
+      h->engine.reset();
+      h->decomposed = true;
+      return BDLU_OK;
+    }
+    int dev_count = 0;
+    const cudaError_t ce = cudaGetDeviceCount(&dev_count);
+    if (ce != cudaSuccess || dev_count <= 0)
+      return fail(h, BDLU_BACKEND_UNAVAILABLE,
+                  std::string("no CUDA device available: ") + (ce != cudaSuccess ? cudaGetErrorString(ce) : "0 devices"));
+    const bdlu::Plan plan = bdlu::build_plan(h->coo, h->dec, bdlu::small_unit_max());
+    if (!h->engine) h->engine = std::make_unique<bdlu::Engine>();
+    std::string err;
+    if (!h->engine->upload(plan, h->dec, h->coo, err)) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+    // The engine keeps its own value buffer; load the analysed values.
+    if (const int st = upload_values(h, h->coo.val.data(), false, nullptr)) return st;
+  } catch (const std::bad_alloc&) {
+    return fail(h, BDLU_ANALYSIS_FAILED, "out of host memory during analysis");
+  } catch (const std::exception& e) {
+    return fail(h, BDLU_ANALYSIS_FAILED, e.what());
+  }
+  h->decomposed = true;
+  return BDLU_OK;
+}
+
+int bdlu_factor(bdlu_solver* h) {
+  if (!h) return BDLU_NOT_PREPARED;
+  clear_error(h);
+  if (!h->decomposed) return fail(h, BDLU_NOT_PREPARED, "analyze must succeed before factor");
+  if (!h->engine) return fail(h, BDLU_BACKEND_UNAVAILABLE, "analysis was run without a device (analysis_only)");
+  if (const int st = upload_values(h, h->coo.val.data(), false, nullptr)) return st;
+  return do_factor(h, nullptr);
+}
+
+int bdlu_refactor_values(bdlu_solver* h, const double* vals, int64_t nnz) {
+  if (!h) return BDLU_NOT_PREPARED;
+  clear_error(h);
+  if (!h->decomposed) return fail(h, BDLU_NOT_PREPARED, "analyze must succeed before refactor");
+  if (!h->engine) return fail(h, BDLU_BACKEND_UNAVAILABLE, "analysis was run without a device (analysis_only)");
+  if (!vals || nnz != h->coo.nnz()) return fail(h, BDLU_INVALID_INDEX, "value count does not match the analysed pattern");
+  for (int64_t k = 0; k < nnz; ++k)
+    if (!std::isfinite(vals[k])) return fail(h, BDLU_NON_FINITE_VALUE, "matrix contains NaN or infinity");
+  std::memcpy(h->coo.val.data(), vals, static_cast<size_t>(nnz) * sizeof(double));
+  if (const int st = upload_values(h, vals, false, nullptr)) return st;
+  return do_factor(h, nullptr);
+}
+
+int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nnz, void* stream) {
+  if (!h) return BDLU_NOT_PREPARED;
+  clear_error(h);
+  if (!h->decomposed) return fail(h, BDLU_NOT_PREPARED, "analyze must succeed before refactor");
+  if (!h->engine) return fail(h, BDLU_BACKEND_UNAVAILABLE, "analysis was run without a device (analysis_only)");
+  if (!d_vals || nnz != h->coo.nnz()) return fail(h, BDLU_INVALID_INDEX, "value count does not match the analysed pattern");
+  auto s = static_cast<cudaStream_t>(stream);
+  if (const int st = upload_values(h, d_vals, true, s)) return st;
+  std::string err;
+  if (!h->engine->factor_async(h->engine->values_buffer(), s, err)) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+  // Zero pivots are reported by the next synchronising call (bdlu_solve_status).
+  h->factored = true;
+  h->exported = false;
+  return BDLU_OK;
+}
+
+int bdlu_solve(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs) {
+  if (!h) return BDLU_NOT_PREPARED;
+  clear_error(h);
+  if (!h->factored) return fail(h, BDLU_NOT_PREPARED, "factor must succeed before solve");
+  if (!B || nrhs < 1 || ldb < h->n) return fail(h, BDLU_INVALID_RHS, "right-hand side size does not match matrix dimension");
+  for (int32_t k = 0; k < nrhs; ++k)
+    for (int32_t i = 0; i < h->n; ++i)
+      if (!std::isfinite(B[static_cast<size_t>(k) * ldb + i]))
+        return fail(h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
+  std::string err;
+  double* d_B = h->engine->rhs_buffer(nrhs, err);
+  if (!d_B) return fail(h, BDLU_SOLVE_FAILED, err);
+  cudaError_t e = cudaMemcpy2D(d_B, static_cast<size_t>(h->n) * sizeof(double), B, static_cast<size_t>(ldb) * sizeof(double),
+                               static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("rhs upload: ") + cudaGetErrorString(e));
+  const int iters = refine_iters_for(h);
+  if (!h->engine->solve_async(d_B, h->n, nrhs, iters, nullptr, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+  e = cudaMemcpy2D(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
+                   static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
+  bdlu::SolveResidual r{};
+  if (!h->engine->last_residual(nullptr, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+  const double denom = r.a_inf * r.x_inf + r.b_inf;
+  h->last_residual = denom > 0.0 ? r.resid_inf / denom : r.resid_inf;
+  h->last_refine = iters;
+  if (!std::isfinite(h->last_residual)) return fail(h, BDLU_SOLVE_FAILED, "block solve produced a non-finite solution");
+  return BDLU_OK;
+}
+
+int bdlu_solve_device(bdlu_solver* h, double* d_B, int32_t ldb, int32_t nrhs, void* stream) {
+  if (!h) return BDLU_NOT_PREPARED;
+  clear_error(h);
+  if (!h->factored) return fail(h, BDLU_NOT_PREPARED, "factor must succeed before solve");
+  if (!d_B || nrhs < 1 || ldb < h->n) return fail(h, BDLU_INVALID_RHS, "right-hand side size does not match matrix dimension");
+  std::string err;
+  const int iters = refine_iters_for(h);
+  if (!h->engine->solve_async(d_B, ldb, nrhs, iters, static_cast<cudaStream_t>(stream), err))
+    return fail(h, BDLU_SOLVE_FAILED, err);
+  h->last_refine = iters;
+  return BDLU_OK;
+}
+
+int bdlu_refactor_solve(bdlu_solver* h, const double* vals, int64_t nnz, double* B, int32_t ldb, int32_t nrhs) {
+  if (const int st = bdlu_refactor_values(h, vals, nnz)) return st;
+  return bdlu_solve(h, B, ldb, nrhs);
+}
+
+int bdlu_last_error(const bdlu_solver* h, char* buf, int64_t len) {
+  if (!h) return BDLU_NOT_PREPARED;
+  if (buf && len > 0) {
+    const size_t k = std::min<size_t>(static_cast<size_t>(len - 1), h->last_message.size());
+    std::memcpy(buf, h->last_message.data(), k);
+    buf[k] = '\0';
+  }
+  return h->last_error;
+}
+
+int32_t bdlu_n(const bdlu_solver* h) { return h ? h->n : 0; }
+
+const char* bdlu_selected_mode(const bdlu_solver* h) { return (h && h->global_route) ? "KLU" : "BLOCK"; }
+
+int64_t bdlu_canonical_pattern(const bdlu_solver* h, int32_t* rows, int32_t* cols) {
+  if (!h || !h->validated) return 0;
+  const int64_t nnz = h->coo.nnz();
+  if (rows) std::memcpy(rows, h->coo.row.data(), static_cast<size_t>(nnz) * sizeof(int32_t));
+  if (cols) std::memcpy(cols, h->coo.col.data(), static_cast<size_t>(nnz) * sizeof(int32_t));
+  return nnz;
+}
+
+int bdlu_get_stats(const bdlu_solver* h, bdlu_stats* out) {
+  if (!h || !out) return BDLU_NOT_PREPARED;
+  std::memset(out, 0, sizeof(*out));
+  out->n = h->n;
+  out->nnz = h->coo.nnz();
+  out->nblocks = h->dec.nblocks;
+  out->nblocks_raw = h->dec.nblocks_raw;
+  out->max_level = h->dec.max_level;
+  for (int32_t b = 0; b < h->dec.nblocks; ++b) out->max_block = std::max(out->max_block, h->dec.R[static_cast<size_t>(b) + 1] - h->dec.R[static_cast<size_t>(b)]);
+  out->nnz_offdiag = h->dec.off_ptr.empty() ? 0 : h->dec.off_ptr.back();
+  out->refine_iters = h->last_refine;
+  out->residual_inf = h->last_residual;
+  if (h->engine) {
+    auto* e = const_cast<bdlu::Engine*>(h->engine.get());
+    out->dense_entries = e->plan().dense_entries;
+    out->factor_flops = e->plan().factor_flops;
+    out->unit_levels = e->plan().umax_level + 1;
+    out->nunits = e->plan().nunits;
+    out->max_unit = e->plan().max_unit;
+    out->factor_launches = e->launches_factor_;
+    out->solve_launches = e->launches_solve_;
+    out->last_factor_ms = e->last_factor_ms();
+    out->last_solve_ms = e->last_solve_ms();
+  }
+  return BDLU_OK;
+}
+
+int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap) {
+  if (!h || !h->engine) return 0;
+  float f[bdlu::Engine::kPhases];
+  h->engine->phase_ms(f);
+  for (int32_t i = 0; i < cap && i < bdlu::Engine::kPhases; ++i) ms[i] = f[i];
+  return bdlu::Engine::kPhases;
+}
+
+int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
+  if (!h || !key) return BDLU_INVALID_DIMENSION;
+  const std::string k(key);
+  if (k == "refine_iters") {
+    h->refine_iters = static_cast<int32_t>(value);
+    return BDLU_OK;
+  }
+  if (k == "analysis_only") {
+    h->analysis_only = value != 0.0;
+    return BDLU_OK;
+  }
+  return BDLU_INVALID_DIMENSION;
+}
+
+int32_t bdlu_btf_order(int32_t n, const int32_t* Ap, const int32_t* Ai, int32_t* P, int32_t* Q, int32_t* R,
+                       int32_t* nmatch) {
+  try {
+    return bdlu::btf_order(n, Ap, Ai, P, Q, R, nmatch);
+  } catch (...) {
+    return -1;
+  }
+}
+
+int32_t bdlu_merge_block_boundaries(const int32_t* R, int32_t nR, int32_t n, int32_t merge_max, int32_t* Rout) {
+  try {
+    const std::vector<int32_t> in(R, R + nR);
+    const std::vector<int32_t> out = bdlu::merge_block_boundaries(in, n, merge_max);
+    if (Rout) std::memcpy(Rout, out.data(), std::min<size_t>(out.size(), static_cast<size_t>(nR)) * sizeof(int32_t));
+    return static_cast<int32_t>(out.size());
+  } catch (...) {
+    return -1;
+  }
+}
+
+int bdlu_get_decomposition(const bdlu_solver* h, int32_t* P, int32_t* Q, int32_t* R, int32_t* off_ptr, int32_t* off_col,
+                           int32_t* off_src, int32_t* level) {
+  if (!h || !h->decomposed) return BDLU_NOT_PREPARED;
+  const auto& d = h->dec;
+  auto cp = [](int32_t* dst, const std::vector<int32_t>& v) {
+    if (dst && !v.empty()) std::memcpy(dst, v.data(), v.size() * sizeof(int32_t));
+  };
+  cp(P, d.P);
+  cp(Q, d.Q);
+  cp(R, d.R);
+  cp(off_ptr, d.off_ptr);
+  cp(off_col, d.off_col);
+  cp(off_src, d.off_src);
+  cp(level, d.level);
+  return BDLU_OK;
+}
+
+}  // extern "C"

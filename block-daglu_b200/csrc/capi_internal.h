@@ -1,0 +1,54 @@
+// Internal state behind the opaque bdlu_solver handle (include/bdlu.h).
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "analysis.h"
+#include "bdlu.h"
+#include "engine.h"
+
+struct bdlu_solver {
+  // Stage flags (solver.h:86-90).
+  bool prepared = false;
+  bool validated = false;
+  bool decomposed = false;
+  bool factored = false;
+  int32_t dimension_hint = -1;
+  int32_t n = 0;
+  std::vector<int32_t> in_rows, in_cols;
+  std::vector<double> in_vals;
+  bdlu::CanonicalCoo coo;
+  uint64_t sig = 0, sig2 = 0, value_sig = 0;
+  int mode = BDLU_MODE_AUTO;
+  bool global_route = false;  // "KLU": one block, no BTF
+  bdlu::Decomposition dec;
+  std::unique_ptr<bdlu::Engine> engine;
+  // Options.
+  int32_t refine_iters = -1;  // -1: REFINE_ITERS env, else 0
+  bool analysis_only = false; // host analysis without device upload (inspection, CPU tests)
+  // Error state (solver.h:122-123).
+  int last_error = BDLU_OK;
+  std::string last_message;
+  // Stats of the last solve.
+  int32_t last_refine = 0;
+  double last_residual = 0.0;
+  // Export cache.
+  bool exported = false;
+  std::vector<int32_t> exP;          // row order of the exported factorisation
+  std::vector<int32_t> l_r, l_c, u_r, u_c;
+  std::vector<double> l_v, u_v;
+};
+
+
+inline int bdlu_fail(bdlu_solver* h, int code, std::string msg) {
+  h->last_error = code;
+  h->last_message = std::move(msg);
+  return code;
+}
+
+// Builds the export cache (P, L, U in the engine's factor order); returns a
+// status code and sets the handle's error on failure.
+int bdlu_build_export(bdlu_solver* h);

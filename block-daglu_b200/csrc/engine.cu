@@ -1,0 +1,802 @@
+// sm_100a kernels and device memory management for the numeric factor and
+// solve.  Units are raw BTF blocks (plan.h).  Kernels:
+//   k_gather          coupling values + scalar-unit diagonals from the
+//                     canonical value array (value-only refactor is a gather)
+//   k_lu_small        one CTA per dense unit, the unit in shared memory, fused
+//                     value scatter; unblocked partial-pivoting LU that
+//                     performs exactly the reference micro-kernel's operations
+//                     (ubtf_block_solver.cpp:1450-1498): same pivot choice,
+//                     same per-element operation order, no FMA contraction,
+//                     so factors are bit-identical
+//   k_scatter_large   value scatter into the arena slots of large units
+//   k_panel / k_swap_trsm / k_gemm_update
+//                     right-looking blocked LU (panel width kPanel) for large
+//                     units, batched over all units active at a step
+//   k_solve_scalar / k_solve_dense
+//                     level-scheduled block back-substitution with the
+//                     off-diagonal update fused in (ubtf_block_solver.cpp:
+//                     2260-2401): rhs = b - A_cpl x, then the unit's L/U solve
+//   k_unpermute       x[Q[i]] (+)= xperm[i]
+//   k_residual        r = b - A x over the canonical CSR, with inf-norms
+#include "engine.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+namespace bdlu {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kFailZeroPivot = 1;
+
+__device__ __forceinline__ void report_failure(int32_t* status, int32_t unit) {
+  if (atomicCAS(status, 0, kFailZeroPivot) == 0) status[1] = unit;
+}
+
+// (value, index) maximum with the reference's tie rule: the smallest index
+// among equal maxima, i.e. the first strict maximum of an ascending scan.
+__device__ __forceinline__ void pivot_combine(double& best, int& bi, double ob, int oi, int none) {
+  if (oi == none) return;
+  if (bi == none || ob > best || (ob == best && oi < bi)) {
+    best = ob;
+    bi = oi;
+  }
+}
+
+__device__ __forceinline__ void warp_pivot_reduce(double& best, int& bi, int none) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+    pivot_combine(best, bi, ob, oi, none);
+  }
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Value gather for coupling entries and scalar units.
+// ---------------------------------------------------------------------------
+__global__ void k_gather(DevPlan dp, const double* __restrict__ vals, int64_t ncpl) {
+  const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t q = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; q < ncpl; q += stride)
+    dp.cpl_val[q] = vals[dp.cpl_src[q]];
+  for (int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; r < dp.n; r += stride) {
+    const int32_t src = dp.sdiag_src[r];
+    if (src == -1) continue;  // row of a dense unit
+    const double v = (src >= 0) ? vals[src] : 0.0;
+    dp.sdiag[r] = v;
+    if (v == 0.0) report_failure(dp.status, static_cast<int32_t>(r));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dense LU of one unit in shared memory (column-major, leading dimension m).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double* __restrict__ vals,
+                                                        const int32_t* __restrict__ units) {
+  extern __shared__ double A[];
+  __shared__ double s_best[kThreads / 32];
+  __shared__ int s_bi[kThreads / 32];
+  __shared__ int s_piv;
+  __shared__ double s_pbest;
+  const int u = units[blockIdx.x];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < m * m; i += kThreads) A[i] = 0.0;
+  __syncthreads();
+  for (int64_t e = dp.dent_ptr[u] + tid; e < dp.dent_ptr[u + 1]; e += kThreads) A[dp.dent_pos[e]] = vals[dp.dent_src[e]];
+  __syncthreads();
+  int32_t* piv = dp.piv + s;
+  for (int k = 0; k < m; ++k) {
+    double* colk = A + static_cast<size_t>(k) * m;
+    // Pivot: each warp scans a strided share of rows k..m-1.
+    double best = 0.0;
+    int bi = m;
+    for (int i = k + tid; i < m; i += kThreads) {
+      const double a = fabs(colk[i]);
+      if (bi == m || a > best) {
+        best = a;
+        bi = i;
+      }
+    }
+    warp_pivot_reduce(best, bi, m);
+    if (lane == 0) {
+      s_best[warp] = best;
+      s_bi[warp] = bi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      best = (lane < kThreads / 32) ? s_best[lane] : 0.0;
+      bi = (lane < kThreads / 32) ? s_bi[lane] : m;
+      warp_pivot_reduce(best, bi, m);
+      if (lane == 0) {
+        s_piv = bi;
+        s_pbest = best;
+      }
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (s_pbest == 0.0) {
+      if (tid == 0) report_failure(dp.status, u);
+      return;
+    }
+    if (tid == 0) piv[k] = p;
+    if (p != k) {
+      for (int j = tid; j < m; j += kThreads) {
+        double* c = A + static_cast<size_t>(j) * m;
+        const double t = c[k];
+        c[k] = c[p];
+        c[p] = t;
+      }
+    }
+    __syncthreads();
+    const double akk = colk[k];
+    for (int i = k + 1 + tid; i < m; i += kThreads) colk[i] = __ddiv_rn(colk[i], akk);
+    __syncthreads();
+    const int r = m - k - 1;
+    for (int t = tid; t < r * r; t += kThreads) {
+      const int jj = t / r, ii = t - jj * r;
+      const int i = k + 1 + ii, j = k + 1 + jj;
+      double* c = A + static_cast<size_t>(j) * m;
+      c[i] = __dsub_rn(c[i], __dmul_rn(colk[i], c[k]));
+    }
+    __syncthreads();
+  }
+  double* out = dp.lu + dp.lu_off[u];
+  for (int i = tid; i < m * m; i += kThreads) out[i] = A[i];
+}
+
+// ---------------------------------------------------------------------------
+// Large units: blocked right-looking LU in the arena (global memory).
+// ---------------------------------------------------------------------------
+__global__ void k_scatter_large(DevPlan dp, const double* __restrict__ vals, const int32_t* __restrict__ units) {
+  const int u = units[blockIdx.y];
+  double* A = dp.lu + dp.lu_off[u];
+  for (int64_t e = dp.dent_ptr[u] + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < dp.dent_ptr[u + 1];
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    A[dp.dent_pos[e]] = vals[dp.dent_src[e]];
+}
+
+// Panel factorisation: one CTA per active unit, columns k0..k0+nb-1, rows
+// k0..m-1, partial pivoting with the same tie rule; row swaps inside the
+// panel only (the rest of each row is swapped by k_swap_trsm).
+__global__ void __launch_bounds__(kThreads) k_panel(DevPlan dp, int32_t k0, int32_t ubase) {
+  __shared__ double s_best[kThreads / 32];
+  __shared__ int s_bi[kThreads / 32];
+  __shared__ int s_piv;
+  __shared__ double s_pbest;
+  const int u = dp.step_unit[ubase + blockIdx.x];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kPanel, m - k0);
+  double* A = dp.lu + dp.lu_off[u];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int j = k0; j < k0 + nb; ++j) {
+    double* colj = A + static_cast<size_t>(j) * m;
+    double best = 0.0;
+    int bi = m;
+    for (int i = j + tid; i < m; i += kThreads) {
+      const double a = fabs(colj[i]);
+      if (bi == m || a > best) {
+        best = a;
+        bi = i;
+      }
+    }
+    warp_pivot_reduce(best, bi, m);
+    if (lane == 0) {
+      s_best[warp] = best;
+      s_bi[warp] = bi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      best = (lane < kThreads / 32) ? s_best[lane] : 0.0;
+      bi = (lane < kThreads / 32) ? s_bi[lane] : m;
+      warp_pivot_reduce(best, bi, m);
+      if (lane == 0) {
+        s_piv = bi;
+        s_pbest = best;
+      }
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (s_pbest == 0.0) {
+      if (tid == 0) report_failure(dp.status, u);
+      return;
+    }
+    if (tid == 0) dp.piv[s + j] = p;
+    if (p != j && tid < nb) {
+      double* c = A + static_cast<size_t>(k0 + tid) * m;
+      const double t = c[j];
+      c[j] = c[p];
+      c[p] = t;
+    }
+    __syncthreads();
+    const double ajj = colj[j];
+    for (int i = j + 1 + tid; i < m; i += kThreads) {
+      const double l = colj[i] / ajj;
+      colj[i] = l;
+      for (int jj = j + 1; jj < k0 + nb; ++jj) {
+        double* c = A + static_cast<size_t>(jj) * m;
+        c[i] = fma(-l, c[j], c[i]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Applies the panel's row swaps to every column outside the panel and solves
+// U12 = L11^{-1} A12 for the columns right of it.  One thread per column.
+__global__ void __launch_bounds__(kTrsmCols) k_swap_trsm(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
+  __shared__ double L11[kPanel * kPanel];
+  __shared__ int spiv[kPanel];
+  // Locate (unit, chunk) for this CTA.
+  int a = 0;
+  while (a + 1 < nact && dp.step_trsm_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
+  const int u = dp.step_unit[ubase + a];
+  const int chunk = blockIdx.x - dp.step_trsm_pref[ubase + a];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kPanel, m - k0);
+  double* A = dp.lu + dp.lu_off[u];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    const int q = t / nb, r = t - q * nb;  // L11(r, q)
+    L11[q * kPanel + r] = A[static_cast<size_t>(k0 + q) * m + k0 + r];
+  }
+  if (threadIdx.x < nb) spiv[threadIdx.x] = dp.piv[s + k0 + threadIdx.x];
+  __syncthreads();
+  const int j = chunk * kTrsmCols + threadIdx.x;
+  if (j >= m || (j >= k0 && j < k0 + nb)) return;
+  double* c = A + static_cast<size_t>(j) * m;
+  for (int r = 0; r < nb; ++r) {
+    const int p = spiv[r];
+    if (p != k0 + r) {
+      const double t = c[k0 + r];
+      c[k0 + r] = c[p];
+      c[p] = t;
+    }
+  }
+  if (j < k0 + nb) return;
+  double x[kPanel];
+#pragma unroll
+  for (int r = 0; r < kPanel; ++r) x[r] = (r < nb) ? c[k0 + r] : 0.0;
+#pragma unroll
+  for (int r = 1; r < kPanel; ++r) {
+    double v = x[r];
+#pragma unroll
+    for (int q = 0; q < r; ++q) v = fma(-L11[q * kPanel + r], x[q], v);
+    x[r] = v;
+  }
+#pragma unroll
+  for (int r = 0; r < kPanel; ++r)
+    if (r < nb) c[k0 + r] = x[r];
+}
+
+// Trailing update A22 -= L21 * U12, 64x64 output tile per CTA, 4x4 per thread.
+__global__ void __launch_bounds__(kThreads) k_gemm_update(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
+  __shared__ double Ls[kPanel][kGemmTile + 1];
+  __shared__ double Us[kPanel][kGemmTile + 1];
+  int a = 0;
+  while (a + 1 < nact && dp.step_gemm_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
+  const int u = dp.step_unit[ubase + a];
+  const int tile = blockIdx.x - dp.step_gemm_pref[ubase + a];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kPanel, m - k0);
+  const int base = k0 + nb;
+  const int rest = m - base;
+  const int nt = (rest + kGemmTile - 1) / kGemmTile;
+  const int ti = tile % nt, tj = tile / nt;
+  const int i0 = base + ti * kGemmTile, j0 = base + tj * kGemmTile;
+  double* A = dp.lu + dp.lu_off[u];
+  const int tid = threadIdx.x;
+  for (int t = tid; t < kPanel * kGemmTile; t += kThreads) {
+    const int q = t / kGemmTile, i = t - q * kGemmTile;
+    Ls[q][i] = (q < nb && i0 + i < m) ? A[static_cast<size_t>(k0 + q) * m + i0 + i] : 0.0;
+  }
+  for (int t = tid; t < kPanel * kGemmTile; t += kThreads) {
+    const int jj = t / kPanel, q = t - jj * kPanel;
+    Us[q][jj] = (q < nb && j0 + jj < m) ? A[static_cast<size_t>(j0 + jj) * m + k0 + q] : 0.0;
+  }
+  __syncthreads();
+  const int tx = tid & 15, ty = tid >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
+#pragma unroll 8
+  for (int q = 0; q < kPanel; ++q) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int x = 0; x < 4; ++x) av[x] = Ls[q][tx + 16 * x];
+#pragma unroll
+    for (int y = 0; y < 4; ++y) bv[y] = Us[q][ty + 16 * y];
+#pragma unroll
+    for (int x = 0; x < 4; ++x)
+#pragma unroll
+      for (int y = 0; y < 4; ++y) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
+  }
+#pragma unroll
+  for (int y = 0; y < 4; ++y) {
+    const int j = j0 + ty + 16 * y;
+    if (j >= m) continue;
+    double* c = A + static_cast<size_t>(j) * m;
+#pragma unroll
+    for (int x = 0; x < 4; ++x) {
+      const int i = i0 + tx + 16 * x;
+      if (i < m) c[i] -= acc[x][y];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Solve.  xp holds the solution in permuted order (n x nrhs, ld n).
+// ---------------------------------------------------------------------------
+__global__ void k_solve_scalar(DevPlan dp, const int32_t* __restrict__ rows, int32_t count,
+                               const double* __restrict__ rhs, int32_t ldr, double* __restrict__ xp,
+                               int32_t nrhs) {
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= count) return;
+  const int r = rows[w];
+  const int p0 = dp.cpl_ptr[r], p1 = dp.cpl_ptr[r + 1];
+  const int n = dp.n;
+  const double d = dp.sdiag[r];
+  const int src = dp.P[r];
+  for (int k = 0; k < nrhs; ++k) {
+    double acc = 0.0;
+    for (int q = p0 + lane; q < p1; q += 32) acc = fma(dp.cpl_val[q], xp[dp.cpl_col[q] + static_cast<size_t>(k) * n], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) xp[r + static_cast<size_t>(k) * n] = (rhs[src + static_cast<size_t>(k) * ldr] - acc) / d;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int32_t* __restrict__ units,
+                                                           const double* __restrict__ rhs, int32_t ldr,
+                                                           double* __restrict__ xp, int32_t nrhs) {
+  extern __shared__ double x[];
+  const int u = units[blockIdx.x];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int n = dp.n;
+  const double* LU = dp.lu + dp.lu_off[u];
+  const int32_t* piv = dp.piv + s;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int k = 0; k < nrhs; ++k) {
+    const double* xk = xp + static_cast<size_t>(k) * n;
+    for (int i = warp; i < m; i += kThreads / 32) {
+      const int r = s + i;
+      double acc = 0.0;
+      for (int q = dp.cpl_ptr[r] + lane; q < dp.cpl_ptr[r + 1]; q += 32) acc = fma(dp.cpl_val[q], xk[dp.cpl_col[q]], acc);
+      acc = warp_sum(acc);
+      if (lane == 0) x[i] = rhs[dp.P[r] + static_cast<size_t>(k) * ldr] - acc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      for (int i = 0; i < m; ++i) {
+        const int p = piv[i];
+        if (p != i) {
+          const double t = x[i];
+          x[i] = x[p];
+          x[p] = t;
+        }
+      }
+    }
+    __syncthreads();
+    // Forward solve with unit-lower L (column oriented).
+    for (int j = 0; j < m - 1; ++j) {
+      const double xj = x[j];
+      const double* lc = LU + static_cast<size_t>(j) * m;
+      for (int i = j + 1 + tid; i < m; i += kThreads) x[i] = fma(-lc[i], xj, x[i]);
+      __syncthreads();
+    }
+    // Backward solve with U.
+    for (int j = m - 1; j >= 0; --j) {
+      const double* uc = LU + static_cast<size_t>(j) * m;
+      const double xj = x[j] / uc[j];
+      for (int i = tid; i < j; i += kThreads) x[i] = fma(-uc[i], xj, x[i]);
+      __syncthreads();
+      if (tid == 0) x[j] = xj;
+      __syncthreads();
+    }
+    double* xo = xp + static_cast<size_t>(k) * n + s;
+    for (int i = tid; i < m; i += kThreads) xo[i] = x[i];
+    __syncthreads();
+  }
+}
+
+__global__ void k_unpermute(const int32_t* __restrict__ Q, int32_t n, const double* __restrict__ xp,
+                            double* __restrict__ X, int32_t ldx, int32_t nrhs, int add) {
+  const int64_t total = static_cast<int64_t>(n) * nrhs;
+  for (int64_t t = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; t < total;
+       t += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t k = t / n;
+    const int64_t i = t - k * n;
+    double* dst = X + Q[i] + k * ldx;
+    if (add) *dst += xp[t];
+    else *dst = xp[t];
+  }
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* a, double v) {
+  atomicMax(a, static_cast<unsigned long long>(__double_as_longlong(v)));
+}
+
+// R = B - A X (original coordinates), warp per row; norms[4k..4k+3] gather
+// |r|_inf, |b|_inf, |x|_inf, |A|_inf for column k.
+__global__ void k_residual(DevPlan dp, const double* __restrict__ vals, const double* __restrict__ X,
+                           int32_t ldx, const double* __restrict__ B, int32_t ldb, double* __restrict__ R,
+                           int32_t nrhs, unsigned long long* norms) {
+  const int lane = threadIdx.x & 31;
+  const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (r >= dp.n) return;
+  const int p0 = dp.csr_ptr[r], p1 = dp.csr_ptr[r + 1];
+  double arow = 0.0;
+  for (int q = p0 + lane; q < p1; q += 32) arow += fabs(vals[q]);
+  arow = warp_sum(arow);
+  for (int k = 0; k < nrhs; ++k) {
+    const double* xk = X + static_cast<size_t>(k) * ldx;
+    double acc = 0.0;
+    for (int q = p0 + lane; q < p1; q += 32) acc = fma(vals[q], xk[dp.csr_col[q]], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      const double b = B[r + static_cast<size_t>(k) * ldb];
+      const double res = b - acc;
+      if (R) R[r + static_cast<size_t>(k) * dp.n] = res;
+      unsigned long long* nk = norms + 4 * k;
+      atomic_max_nonneg(nk + 0, fabs(res));
+      atomic_max_nonneg(nk + 1, fabs(b));
+      atomic_max_nonneg(nk + 2, fabs(xk[r]));
+      atomic_max_nonneg(nk + 3, arow);
+    }
+  }
+}
+
+int grid_for(int64_t work, int threads, int cap) {
+  const int64_t g = (work + threads - 1) / threads;
+  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(g, cap)));
+}
+
+}  // namespace
+
+int32_t small_unit_max() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || optin <= 0)
+    optin = 227 * 1024;
+  // m*m doubles plus the kernel's static shared memory (~1 KB).
+  const int64_t budget = optin - 2048;
+  int32_t m = 1;
+  while (static_cast<int64_t>(m + 1) * (m + 1) * 8 <= budget) ++m;
+  return m;
+}
+
+Engine::Engine() {
+  for (auto& e : ev_) cudaEventCreate(&e);
+  for (auto& e : pev_) cudaEventCreate(&e);
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev);
+}
+
+Engine::~Engine() {
+  release();
+  for (auto& e : ev_)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : pev_)
+    if (e) cudaEventDestroy(e);
+}
+
+void Engine::release() {
+  for (void* p : allocs_) cudaFree(p);
+  allocs_.clear();
+  d_vals_ = nullptr;
+  d_status_ = nullptr;
+  d_b0_ = d_xp_ = d_r_ = d_rhs_ = nullptr;
+  d_norms_ = nullptr;
+  work_nrhs_ = 0;
+  dp_ = DevPlan{};
+}
+
+#define BDLU_CUDA(call)                                                      \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) {                                                 \
+      err = std::string(#call) + ": " + cudaGetErrorString(e_);              \
+      return false;                                                          \
+    }                                                                        \
+  } while (0)
+
+template <class T>
+static bool upload_vec(std::vector<void*>& allocs, const std::vector<T>& v, const T** out, std::string& err) {
+  void* p = nullptr;
+  const size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(T);
+  BDLU_CUDA(cudaMalloc(&p, bytes));
+  allocs.push_back(p);
+  if (!v.empty()) BDLU_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *out = static_cast<const T*>(p);
+  return true;
+}
+
+template <class T>
+static bool alloc_dev(std::vector<void*>& allocs, size_t count, T** out, std::string& err) {
+  void* p = nullptr;
+  BDLU_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
+  allocs.push_back(p);
+  *out = static_cast<T*>(p);
+  return true;
+}
+
+bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalCoo& a, std::string& err) {
+  release();
+  plan_ = plan;
+  DevPlan d{};
+  d.n = plan.n;
+  d.nunits = plan.nunits;
+  d.nnz = plan.nnz;
+  if (!upload_vec(allocs_, dec.P, &d.P, err)) return false;
+  if (!upload_vec(allocs_, dec.Q, &d.Q, err)) return false;
+  if (!upload_vec(allocs_, plan.ustart, &d.ustart, err)) return false;
+  if (!upload_vec(allocs_, plan.lu_off, &d.lu_off, err)) return false;
+  if (!upload_vec(allocs_, plan.dent_ptr, &d.dent_ptr, err)) return false;
+  if (!upload_vec(allocs_, plan.dent_pos, &d.dent_pos, err)) return false;
+  if (!upload_vec(allocs_, plan.dent_src, &d.dent_src, err)) return false;
+  if (!upload_vec(allocs_, plan.sdiag_src, &d.sdiag_src, err)) return false;
+  if (!upload_vec(allocs_, plan.cpl_ptr, &d.cpl_ptr, err)) return false;
+  if (!upload_vec(allocs_, plan.cpl_col, &d.cpl_col, err)) return false;
+  if (!upload_vec(allocs_, plan.cpl_src, &d.cpl_src, err)) return false;
+  if (!upload_vec(allocs_, plan.csr_ptr, &d.csr_ptr, err)) return false;
+  if (!upload_vec(allocs_, a.col, &d.csr_col, err)) return false;
+  if (!upload_vec(allocs_, plan.step_unit, &d.step_unit, err)) return false;
+  if (!upload_vec(allocs_, plan.step_trsm_pref, &d.step_trsm_pref, err)) return false;
+  if (!upload_vec(allocs_, plan.step_gemm_pref, &d.step_gemm_pref, err)) return false;
+  if (!alloc_dev(allocs_, static_cast<size_t>(plan.lu_size), &d.lu, err)) return false;
+  if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.piv, err)) return false;
+  if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.sdiag, err)) return false;
+  if (!alloc_dev(allocs_, plan.cpl_col.size(), &d.cpl_val, err)) return false;
+  if (!alloc_dev(allocs_, 2, &d.status, err)) return false;
+  if (!alloc_dev(allocs_, static_cast<size_t>(plan.nnz), &d_vals_, err)) return false;
+  d_status_ = d.status;
+  BDLU_CUDA(cudaMemset(d.status, 0, 2 * sizeof(int32_t)));
+  BDLU_CUDA(cudaMemset(d.piv, 0, static_cast<size_t>(plan.n) * sizeof(int32_t)));
+  dp_ = d;
+  smem_small_ = 0;
+  int32_t small_m = 0;
+  for (int32_t u : plan.small_units) small_m = std::max(small_m, plan.ustart[static_cast<size_t>(u) + 1] - plan.ustart[static_cast<size_t>(u)]);
+  smem_small_ = static_cast<size_t>(small_m) * small_m * sizeof(double);
+  smem_solve_ = static_cast<size_t>(std::max<int32_t>(plan.max_unit, 1)) * sizeof(double);
+  if (smem_solve_ > 200 * 1024) {
+    err = "largest diagonal block exceeds the solve kernel's shared-memory vector";
+    return false;
+  }
+  {
+    // The dynamic shared-memory limit is a per-function process-wide
+    // attribute; raise it once to the device maximum so handles of different
+    // sizes never lower each other's limit.
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+      int dev = 0, optin = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+      const int dyn = optin - 2048;
+      attr_err = cudaFuncSetAttribute(k_lu_small, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_solve_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+    });
+    BDLU_CUDA(attr_err);
+  }
+  // Kernel work lists.
+  const int32_t* small_list = nullptr;
+  const int32_t* large_list = nullptr;
+  const int32_t* lvl_scalar = nullptr;
+  const int32_t* lvl_dense = nullptr;
+  if (!upload_vec(allocs_, plan.small_units, &small_list, err)) return false;
+  if (!upload_vec(allocs_, plan.large_units, &large_list, err)) return false;
+  if (!upload_vec(allocs_, plan.lvl_scalar, &lvl_scalar, err)) return false;
+  if (!upload_vec(allocs_, plan.lvl_dense, &lvl_dense, err)) return false;
+  small_list_ = small_list;
+  large_list_ = large_list;
+  lvl_scalar_ = lvl_scalar;
+  lvl_dense_ = lvl_dense;
+  return true;
+}
+
+bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string& err) {
+  const Plan& p = plan_;
+  BDLU_CUDA(cudaMemsetAsync(d_status_, 0, 2 * sizeof(int32_t), stream));
+  BDLU_CUDA(cudaEventRecord(ev_[0], stream));
+  const int64_t ncpl = static_cast<int64_t>(p.cpl_col.size());
+  launches_factor_ = 1 + (p.small_units.empty() ? 0 : 1);
+  k_gather<<<grid_for(std::max<int64_t>(ncpl, p.n), kThreads, num_sms_ * 8), kThreads, 0, stream>>>(dp_, d_vals, ncpl);
+  BDLU_CUDA(cudaEventRecord(pev_[0], stream));
+  if (!p.small_units.empty())
+    k_lu_small<<<static_cast<int>(p.small_units.size()), kThreads, smem_small_, stream>>>(dp_, d_vals, small_list_);
+  BDLU_CUDA(cudaEventRecord(pev_[1], stream));
+  if (!p.large_units.empty()) {
+    BDLU_CUDA(cudaMemsetAsync(dp_.lu + p.lu_large_begin, 0,
+                              static_cast<size_t>(p.lu_large_end - p.lu_large_begin) * sizeof(double), stream));
+    k_scatter_large<<<dim3(64, static_cast<unsigned>(p.large_units.size())), kThreads, 0, stream>>>(dp_, d_vals, large_list_);
+    ++launches_factor_;
+    for (int32_t st = 0; st < p.nsteps; ++st) {
+      const int32_t ub = p.step_ptr[static_cast<size_t>(st)];
+      const int32_t na = p.step_ptr[static_cast<size_t>(st) + 1] - ub;
+      if (na <= 0) continue;
+      const int32_t k0 = st * kPanel;
+      k_panel<<<na, kThreads, 0, stream>>>(dp_, k0, ub);
+      k_swap_trsm<<<p.step_trsm_total[static_cast<size_t>(st)], kTrsmCols, 0, stream>>>(dp_, k0, ub, na);
+      launches_factor_ += 2;
+      if (p.step_gemm_total[static_cast<size_t>(st)] > 0) {
+        k_gemm_update<<<p.step_gemm_total[static_cast<size_t>(st)], kThreads, 0, stream>>>(dp_, k0, ub, na);
+        ++launches_factor_;
+      }
+    }
+  }
+  BDLU_CUDA(cudaGetLastError());
+  BDLU_CUDA(cudaEventRecord(ev_[1], stream));
+  factor_timed_ = true;
+  return true;
+}
+
+bool Engine::factor_status(cudaStream_t stream, std::string& err) {
+  int32_t st[2] = {0, 0};
+  BDLU_CUDA(cudaMemcpyAsync(st, d_status_, sizeof(st), cudaMemcpyDeviceToHost, stream));
+  BDLU_CUDA(cudaStreamSynchronize(stream));
+  if (st[0] != 0) {
+    err = "block factorization failed: zero pivot in diagonal block " + std::to_string(st[1]);
+    return false;
+  }
+  return true;
+}
+
+bool Engine::ensure_work(int32_t nrhs, std::string& err) {
+  if (nrhs <= work_nrhs_) return true;
+  const size_t nn = static_cast<size_t>(plan_.n) * static_cast<size_t>(nrhs);
+  for (void* q : {static_cast<void*>(d_b0_), static_cast<void*>(d_xp_), static_cast<void*>(d_r_),
+                  static_cast<void*>(d_rhs_), static_cast<void*>(d_norms_)}) {
+    if (!q) continue;
+    cudaFree(q);
+    allocs_.erase(std::remove(allocs_.begin(), allocs_.end(), q), allocs_.end());
+  }
+  if (!alloc_dev(allocs_, nn, &d_b0_, err)) return false;
+  if (!alloc_dev(allocs_, nn, &d_xp_, err)) return false;
+  if (!alloc_dev(allocs_, nn, &d_r_, err)) return false;
+  if (!alloc_dev(allocs_, nn, &d_rhs_, err)) return false;
+  if (!alloc_dev(allocs_, static_cast<size_t>(4 * nrhs), &d_norms_, err)) return false;
+  work_nrhs_ = nrhs;
+  return true;
+}
+
+double* Engine::rhs_buffer(int32_t nrhs, std::string& err) {
+  if (!ensure_work(nrhs, err)) return nullptr;
+  return d_rhs_;
+}
+
+void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, int32_t nrhs, cudaStream_t stream) {
+  const Plan& p = plan_;
+  const int32_t nl = p.umax_level + 1;
+  for (int32_t l = 0; l < nl; ++l) {
+    const int32_t s0 = p.lvl_scalar_ptr[static_cast<size_t>(l)], s1 = p.lvl_scalar_ptr[static_cast<size_t>(l) + 1];
+    const int32_t d0 = p.lvl_dense_ptr[static_cast<size_t>(l)], d1 = p.lvl_dense_ptr[static_cast<size_t>(l) + 1];
+    if (s1 > s0) {
+      ++launches_solve_;
+      const int warps_per_cta = kThreads / 32;
+      k_solve_scalar<<<(s1 - s0 + warps_per_cta - 1) / warps_per_cta, kThreads, 0, stream>>>(
+          dp_, lvl_scalar_ + s0, s1 - s0, rhs, ldr, xp, nrhs);
+    }
+    if (d1 > d0) ++launches_solve_;
+    if (d1 > d0)
+      k_solve_dense<<<d1 - d0, kThreads, smem_solve_, stream>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp, nrhs);
+  }
+}
+
+bool Engine::solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_iters, cudaStream_t stream,
+                         std::string& err) {
+  if (!ensure_work(nrhs, err)) return false;
+  const int32_t n = plan_.n;
+  BDLU_CUDA(cudaEventRecord(ev_[2], stream));
+  launches_solve_ = 3 + 3 * refine_iters;  // unpermute + residual (+ per step residual, unpermute) below
+  BDLU_CUDA(cudaMemcpy2DAsync(d_b0_, static_cast<size_t>(n) * sizeof(double), d_B,
+                              static_cast<size_t>(ldb) * sizeof(double), static_cast<size_t>(n) * sizeof(double),
+                              static_cast<size_t>(nrhs), cudaMemcpyDeviceToDevice, stream));
+  solve_core(d_b0_, n, d_xp_, nrhs, stream);
+  const int ug = grid_for(static_cast<int64_t>(n) * nrhs, kThreads, num_sms_ * 16);
+  k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 0);
+  BDLU_CUDA(cudaEventRecord(pev_[2], stream));
+  const int rg = grid_for(static_cast<int64_t>(n) * 32, kThreads, 1 << 30);
+  for (int32_t it = 0; it < refine_iters; ++it) {
+    BDLU_CUDA(cudaMemsetAsync(d_norms_, 0, static_cast<size_t>(4 * nrhs) * sizeof(unsigned long long), stream));
+    k_residual<<<rg, kThreads, 0, stream>>>(dp_, d_vals_, d_B, ldb, d_b0_, n, d_r_, nrhs, d_norms_);
+    solve_core(d_r_, n, d_xp_, nrhs, stream);
+    k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 1);
+  }
+  BDLU_CUDA(cudaMemsetAsync(d_norms_, 0, static_cast<size_t>(4 * nrhs) * sizeof(unsigned long long), stream));
+  k_residual<<<rg, kThreads, 0, stream>>>(dp_, d_vals_, d_B, ldb, d_b0_, n, nullptr, nrhs, d_norms_);
+  BDLU_CUDA(cudaGetLastError());
+  BDLU_CUDA(cudaEventRecord(ev_[3], stream));
+  last_nrhs_ = nrhs;
+  solve_timed_ = true;
+  return true;
+}
+
+bool Engine::last_residual(cudaStream_t stream, SolveResidual& out, std::string& err) {
+  out = SolveResidual{0, 0, 0, 0};
+  if (last_nrhs_ <= 0) return true;
+  std::vector<unsigned long long> h(static_cast<size_t>(4 * last_nrhs_));
+  BDLU_CUDA(cudaMemcpyAsync(h.data(), d_norms_, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+  BDLU_CUDA(cudaStreamSynchronize(stream));
+  double worst = -1.0;
+  for (int32_t k = 0; k < last_nrhs_; ++k) {
+    double v[4];
+    std::memcpy(v, &h[static_cast<size_t>(4 * k)], sizeof(v));
+    const double denom = v[3] * v[2] + v[1];
+    const double rel = denom > 0.0 ? v[0] / denom : v[0];
+    if (rel > worst) {
+      worst = rel;
+      out = SolveResidual{v[0], v[1], v[2], v[3]};
+    }
+  }
+  return true;
+}
+
+void Engine::phase_ms(float out[kPhases]) {
+  for (int i = 0; i < kPhases; ++i) out[i] = 0.0f;
+  if (factor_timed_ && cudaEventSynchronize(ev_[1]) == cudaSuccess) {
+    cudaEventElapsedTime(&out[0], ev_[0], pev_[0]);
+    cudaEventElapsedTime(&out[1], pev_[0], pev_[1]);
+    cudaEventElapsedTime(&out[2], pev_[1], ev_[1]);
+  }
+  if (solve_timed_ && cudaEventSynchronize(ev_[3]) == cudaSuccess) {
+    cudaEventElapsedTime(&out[3], ev_[2], pev_[2]);
+    cudaEventElapsedTime(&out[4], pev_[2], ev_[3]);
+  }
+}
+
+float Engine::last_factor_ms() {
+  float ms = 0.0f;
+  if (factor_timed_ && cudaEventSynchronize(ev_[1]) == cudaSuccess) cudaEventElapsedTime(&ms, ev_[0], ev_[1]);
+  return ms;
+}
+
+float Engine::last_solve_ms() {
+  float ms = 0.0f;
+  if (solve_timed_ && cudaEventSynchronize(ev_[3]) == cudaSuccess) cudaEventElapsedTime(&ms, ev_[2], ev_[3]);
+  return ms;
+}
+
+bool Engine::download_unit(int32_t u, std::vector<double>& lu, std::vector<int32_t>& piv, double& scalar,
+                           std::string& err) {
+  if (u < 0 || u >= plan_.nunits) {
+    err = "unit index out of range";
+    return false;
+  }
+  const int32_t s = plan_.ustart[static_cast<size_t>(u)];
+  const int32_t m = plan_.ustart[static_cast<size_t>(u) + 1] - s;
+  BDLU_CUDA(cudaDeviceSynchronize());
+  if (plan_.ukind[static_cast<size_t>(u)] == kUnitScalar) {
+    BDLU_CUDA(cudaMemcpy(&scalar, dp_.sdiag + s, sizeof(double), cudaMemcpyDeviceToHost));
+    lu.assign(1, scalar);
+    piv.assign(1, 0);
+    return true;
+  }
+  lu.resize(static_cast<size_t>(m) * m);
+  piv.resize(static_cast<size_t>(m));
+  BDLU_CUDA(cudaMemcpy(lu.data(), dp_.lu + plan_.lu_off[static_cast<size_t>(u)], lu.size() * sizeof(double),
+                       cudaMemcpyDeviceToHost));
+  BDLU_CUDA(cudaMemcpy(piv.data(), dp_.piv + s, piv.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  return true;
+}
+
+}  // namespace bdlu

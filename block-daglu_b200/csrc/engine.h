@@ -1,0 +1,131 @@
+// Device engine: per-pattern device plan, numeric factor and solve on the GPU.
+#pragma once
+
+#include <cuda_runtime_api.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "plan.h"
+
+namespace bdlu {
+
+// Device-side view of a plan (all pointers device memory owned by Engine).
+struct DevPlan {
+  int32_t n;
+  int32_t nunits;
+  int64_t nnz;
+  const int32_t* P;
+  const int32_t* Q;
+  const int32_t* ustart;
+  const int64_t* lu_off;
+  const int64_t* dent_ptr;
+  const int32_t* dent_pos;
+  const int32_t* dent_src;
+  const int32_t* sdiag_src;
+  const int32_t* cpl_ptr;
+  const int32_t* cpl_col;
+  const int32_t* cpl_src;
+  const int32_t* csr_ptr;
+  const int32_t* csr_col;
+  const int32_t* step_unit;
+  const int32_t* step_trsm_pref;
+  const int32_t* step_gemm_pref;
+  double* lu;
+  int32_t* piv;
+  double* sdiag;
+  double* cpl_val;
+  int32_t* status;  // [0] failure code (0 = ok), [1] failing unit
+};
+
+struct SolveResidual {
+  double resid_inf;   // |b - Ax|_inf
+  double b_inf;
+  double x_inf;
+  double a_inf;       // max row sum |A|
+};
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  // Uploads the pattern: plan tables, permutations, canonical column indices.
+  // Returns false and sets `err` on a CUDA error.
+  bool upload(const Plan& plan, const Decomposition& dec, const CanonicalCoo& a, std::string& err);
+
+  // Enqueues the numeric factor of every unit from canonical-order values
+  // already on the device (d_vals, nnz entries).
+  bool factor_async(const double* d_vals, cudaStream_t stream, std::string& err);
+  // Waits for the factor and reports a zero pivot as a failure.
+  bool factor_status(cudaStream_t stream, std::string& err);
+
+  // Enqueues X = A^{-1} B for nrhs columns (column-major, ld ldb, in place),
+  // followed by `refine_iters` FP64 refinement steps and the residual norms.
+  bool solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_iters, cudaStream_t stream,
+                   std::string& err);
+  // Residual norms of the last solve (synchronises the stream), worst column.
+  bool last_residual(cudaStream_t stream, SolveResidual& out, std::string& err);
+
+  double* values_buffer() { return d_vals_; }
+  // Device buffer of n * nrhs doubles for host-API right-hand sides.
+  double* rhs_buffer(int32_t nrhs, std::string& err);
+  int64_t nnz() const { return plan_.nnz; }
+  int32_t n() const { return plan_.n; }
+  const Plan& plan() const { return plan_; }
+  float last_factor_ms();
+  float last_solve_ms();
+  // Device time of the last factor's and solve's phases, in order: value
+  // gather, shared-memory LU, blocked LU of large units, first solve sweep,
+  // refinement + residual.  Synchronises on the recorded events.
+  static constexpr int kPhases = 5;
+  void phase_ms(float out[kPhases]);
+
+  // Copies a dense unit's LU (column-major m*m) and pivots to the host.
+  bool download_unit(int32_t u, std::vector<double>& lu, std::vector<int32_t>& piv, double& scalar,
+                     std::string& err);
+
+ private:
+  void release();
+  bool ensure_work(int32_t nrhs, std::string& err);
+  void solve_core(const double* rhs, int32_t ldr, double* xp, int32_t nrhs, cudaStream_t stream);
+
+  Plan plan_;
+  DevPlan dp_{};
+  std::vector<void*> allocs_;
+  double* d_vals_ = nullptr;
+  int32_t* d_status_ = nullptr;
+  // Solve work space, grown to the largest nrhs seen.
+  int32_t work_nrhs_ = 0;
+  double* d_b0_ = nullptr;
+  double* d_xp_ = nullptr;
+  double* d_r_ = nullptr;
+  double* d_rhs_ = nullptr;
+  unsigned long long* d_norms_ = nullptr;  // 4 per rhs
+  int32_t last_nrhs_ = 0;
+  cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
+  // Phase boundaries: factor start, after gather, after small LU, factor end
+  // (ev_[0..1] reuse), solve start, after first sweep, solve end.
+  cudaEvent_t pev_[8] = {};
+  bool factor_timed_ = false, solve_timed_ = false;
+  const int32_t* small_list_ = nullptr;
+  const int32_t* large_list_ = nullptr;
+  const int32_t* lvl_scalar_ = nullptr;
+  const int32_t* lvl_dense_ = nullptr;
+  size_t smem_small_ = 0;
+  size_t smem_solve_ = 0;
+  int num_sms_ = 148;
+
+ public:
+  // Kernel launches enqueued by the last factor / solve.
+  int32_t launches_factor_ = 0;
+  int32_t launches_solve_ = 0;
+};
+
+// Largest unit the shared-memory LU kernel takes on this device.
+int32_t small_unit_max();
+
+}  // namespace bdlu

@@ -1,0 +1,177 @@
+// Builds the per-pattern device plan (see plan.h).
+#include "plan.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace bdlu {
+
+static double lu_flops(int64_t m) {
+  // Partial-pivoting LU: (m-k-1) divisions and (m-k-1)^2 multiply-subtract
+  // pairs at step k.
+  double f = 0.0;
+  for (int64_t k = 0; k < m; ++k) {
+    const double r = static_cast<double>(m - k - 1);
+    f += r + 2.0 * r * r;
+  }
+  return f;
+}
+
+Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max) {
+  Plan p;
+  const int32_t n = d.n;
+  p.n = n;
+  p.nnz = a.nnz();
+  p.small_max = small_max;
+  p.ustart = d.R_raw;
+  p.nunits = static_cast<int32_t>(p.ustart.size()) - 1;
+  const int32_t nu = p.nunits;
+  p.unit_of.resize(static_cast<size_t>(n));
+  p.ukind.resize(static_cast<size_t>(nu));
+  p.lu_off.assign(static_cast<size_t>(nu), -1);
+  for (int32_t u = 0; u < nu; ++u) {
+    const int32_t s = p.ustart[static_cast<size_t>(u)], e = p.ustart[static_cast<size_t>(u) + 1];
+    const int32_t m = e - s;
+    for (int32_t r = s; r < e; ++r) p.unit_of[static_cast<size_t>(r)] = u;
+    p.ukind[static_cast<size_t>(u)] = (m == 1) ? kUnitScalar : (m <= small_max ? kUnitSmall : kUnitLarge);
+    p.max_unit = std::max(p.max_unit, m);
+  }
+  // Arena: small units first, then large units contiguously (so one memset
+  // clears all large slots).  Slots are padded to 32 doubles.
+  int64_t off = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) p.lu_large_begin = off;
+    for (int32_t u = 0; u < nu; ++u) {
+      const int32_t k = p.ukind[static_cast<size_t>(u)];
+      if ((pass == 0 && k != kUnitSmall) || (pass == 1 && k != kUnitLarge)) continue;
+      const int64_t m = p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)];
+      p.lu_off[static_cast<size_t>(u)] = off;
+      off += (m * m + 31) / 32 * 32;
+      p.dense_entries += m * m;
+      p.factor_flops += lu_flops(m);
+      (pass == 0 ? p.small_units : p.large_units).push_back(u);
+    }
+  }
+  p.lu_large_end = off;
+  p.lu_size = off;
+
+  // Split entries into unit-diagonal entries and coupling, canonical order.
+  const double drop = [&] {
+    const AnalysisOptions o = analysis_options_from_env();
+    return o.drop_abs_lt < 0.0 ? (n >= 50000 ? 1e-20 : 0.0) : o.drop_abs_lt;
+  }();
+  p.sdiag_src.assign(static_cast<size_t>(n), -1);
+  for (int32_t u = 0; u < nu; ++u)
+    if (p.ukind[static_cast<size_t>(u)] == kUnitScalar) p.sdiag_src[static_cast<size_t>(p.ustart[static_cast<size_t>(u)])] = -2;
+  std::vector<int64_t> dcnt(static_cast<size_t>(nu), 0);
+  std::vector<int32_t> ccnt(static_cast<size_t>(n), 0);
+  const size_t nnz = static_cast<size_t>(a.nnz());
+  for (size_t k = 0; k < nnz; ++k) {
+    if (drop > 0.0 && std::abs(a.val[k]) < drop) continue;
+    const int32_t rp = d.invP[static_cast<size_t>(a.row[k])], cp = d.invQ[static_cast<size_t>(a.col[k])];
+    const int32_t ur = p.unit_of[static_cast<size_t>(rp)], uc = p.unit_of[static_cast<size_t>(cp)];
+    if (ur == uc) {
+      if (p.ukind[static_cast<size_t>(ur)] == kUnitScalar) p.sdiag_src[static_cast<size_t>(rp)] = static_cast<int32_t>(k);
+      else dcnt[static_cast<size_t>(ur)]++;
+    } else {
+      ccnt[static_cast<size_t>(rp)]++;
+    }
+  }
+  p.dent_ptr.assign(static_cast<size_t>(nu) + 1, 0);
+  for (int32_t u = 0; u < nu; ++u) p.dent_ptr[static_cast<size_t>(u) + 1] = p.dent_ptr[static_cast<size_t>(u)] + dcnt[static_cast<size_t>(u)];
+  p.cpl_ptr.assign(static_cast<size_t>(n) + 1, 0);
+  for (int32_t r = 0; r < n; ++r) p.cpl_ptr[static_cast<size_t>(r) + 1] = p.cpl_ptr[static_cast<size_t>(r)] + ccnt[static_cast<size_t>(r)];
+  p.dent_pos.resize(static_cast<size_t>(p.dent_ptr[static_cast<size_t>(nu)]));
+  p.dent_src.resize(p.dent_pos.size());
+  p.cpl_col.resize(static_cast<size_t>(p.cpl_ptr[static_cast<size_t>(n)]));
+  p.cpl_src.resize(p.cpl_col.size());
+  std::vector<int64_t> dnext(p.dent_ptr.begin(), p.dent_ptr.end() - 1);
+  std::vector<int32_t> cnext(p.cpl_ptr.begin(), p.cpl_ptr.end() - 1);
+  for (size_t k = 0; k < nnz; ++k) {
+    if (drop > 0.0 && std::abs(a.val[k]) < drop) continue;
+    const int32_t rp = d.invP[static_cast<size_t>(a.row[k])], cp = d.invQ[static_cast<size_t>(a.col[k])];
+    const int32_t ur = p.unit_of[static_cast<size_t>(rp)], uc = p.unit_of[static_cast<size_t>(cp)];
+    if (ur == uc) {
+      if (p.ukind[static_cast<size_t>(ur)] == kUnitScalar) continue;
+      const int32_t s = p.ustart[static_cast<size_t>(ur)];
+      const int32_t m = p.ustart[static_cast<size_t>(ur) + 1] - s;
+      const int64_t q = dnext[static_cast<size_t>(ur)]++;
+      p.dent_pos[static_cast<size_t>(q)] = (cp - s) * m + (rp - s);
+      p.dent_src[static_cast<size_t>(q)] = static_cast<int32_t>(k);
+    } else {
+      const int32_t q = cnext[static_cast<size_t>(rp)]++;
+      p.cpl_col[static_cast<size_t>(q)] = cp;
+      p.cpl_src[static_cast<size_t>(q)] = static_cast<int32_t>(k);
+    }
+  }
+
+  // Unit DAG levels from the coupling (dependencies point to higher units).
+  p.ulevel.assign(static_cast<size_t>(nu), 0);
+  p.umax_level = 0;
+  for (int32_t u = nu - 1; u >= 0; --u) {
+    int32_t lev = 0;
+    for (int32_t r = p.ustart[static_cast<size_t>(u)]; r < p.ustart[static_cast<size_t>(u) + 1]; ++r)
+      for (int32_t q = p.cpl_ptr[static_cast<size_t>(r)]; q < p.cpl_ptr[static_cast<size_t>(r) + 1]; ++q)
+        lev = std::max(lev, p.ulevel[static_cast<size_t>(p.unit_of[static_cast<size_t>(p.cpl_col[static_cast<size_t>(q)])])] + 1);
+    p.ulevel[static_cast<size_t>(u)] = lev;
+    p.umax_level = std::max(p.umax_level, lev);
+  }
+  const int32_t nl = p.umax_level + 1;
+  p.lvl_scalar_ptr.assign(static_cast<size_t>(nl) + 1, 0);
+  p.lvl_dense_ptr.assign(static_cast<size_t>(nl) + 1, 0);
+  for (int32_t u = 0; u < nu; ++u) {
+    const int32_t l = p.ulevel[static_cast<size_t>(u)];
+    if (p.ukind[static_cast<size_t>(u)] == kUnitScalar) p.lvl_scalar_ptr[static_cast<size_t>(l) + 1]++;
+    else p.lvl_dense_ptr[static_cast<size_t>(l) + 1]++;
+  }
+  for (int32_t l = 0; l < nl; ++l) {
+    p.lvl_scalar_ptr[static_cast<size_t>(l) + 1] += p.lvl_scalar_ptr[static_cast<size_t>(l)];
+    p.lvl_dense_ptr[static_cast<size_t>(l) + 1] += p.lvl_dense_ptr[static_cast<size_t>(l)];
+  }
+  p.lvl_scalar.resize(static_cast<size_t>(p.lvl_scalar_ptr[static_cast<size_t>(nl)]));
+  p.lvl_dense.resize(static_cast<size_t>(p.lvl_dense_ptr[static_cast<size_t>(nl)]));
+  {
+    std::vector<int32_t> sn(p.lvl_scalar_ptr.begin(), p.lvl_scalar_ptr.end() - 1);
+    std::vector<int32_t> dn(p.lvl_dense_ptr.begin(), p.lvl_dense_ptr.end() - 1);
+    for (int32_t u = 0; u < nu; ++u) {
+      const int32_t l = p.ulevel[static_cast<size_t>(u)];
+      if (p.ukind[static_cast<size_t>(u)] == kUnitScalar)
+        p.lvl_scalar[static_cast<size_t>(sn[static_cast<size_t>(l)]++)] = p.ustart[static_cast<size_t>(u)];
+      else
+        p.lvl_dense[static_cast<size_t>(dn[static_cast<size_t>(l)]++)] = u;
+    }
+  }
+
+  // Blocked-LU step tables for large units.
+  int32_t max_large = 0;
+  for (int32_t u : p.large_units) max_large = std::max(max_large, p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)]);
+  p.nsteps = (max_large + kPanel - 1) / kPanel;
+  p.step_ptr.assign(static_cast<size_t>(p.nsteps) + 1, 0);
+  for (int32_t st = 0; st < p.nsteps; ++st) {
+    const int32_t k0 = st * kPanel;
+    int32_t tpre = 0, gpre = 0;
+    for (int32_t u : p.large_units) {
+      const int32_t m = p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)];
+      if (m <= k0) continue;
+      const int32_t nb = std::min(kPanel, m - k0);
+      const int32_t rest = m - k0 - nb;
+      p.step_unit.push_back(u);
+      p.step_trsm_pref.push_back(tpre);
+      p.step_gemm_pref.push_back(gpre);
+      tpre += (m + kTrsmCols - 1) / kTrsmCols;
+      const int32_t t = (rest + kGemmTile - 1) / kGemmTile;
+      gpre += t * t;
+    }
+    p.step_ptr[static_cast<size_t>(st) + 1] = static_cast<int32_t>(p.step_unit.size());
+    p.step_trsm_total.push_back(tpre);
+    p.step_gemm_total.push_back(gpre);
+  }
+
+  // Canonical CSR row pointer (original coordinates) for the residual.
+  p.csr_ptr.assign(static_cast<size_t>(n) + 1, 0);
+  for (size_t k = 0; k < nnz; ++k) p.csr_ptr[static_cast<size_t>(a.row[k]) + 1]++;
+  for (int32_t r = 0; r < n; ++r) p.csr_ptr[static_cast<size_t>(r) + 1] += p.csr_ptr[static_cast<size_t>(r)];
+  return p;
+}
+
+}  // namespace bdlu

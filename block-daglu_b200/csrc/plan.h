@@ -1,0 +1,79 @@
+// Device execution plan for one sparsity pattern.
+//
+// The reference factors and solves per merged block (ubtf_block_solver.cpp:
+// 1427-1826 and 2220-2555).  A merged block is a run of raw BTF blocks, and
+// its partial-pivoting LU is block-diagonal in those raw blocks: rows of a
+// later raw block hold structural zeros in an earlier raw block's columns, so
+// they are never chosen as pivots and only ever receive x - (+-0)*y updates.
+// The diagonal sub-blocks of the merged LU are therefore exactly the LUs of
+// the raw blocks, and the merged solve equals a solve over raw blocks.  The
+// device works on raw blocks ("units"): they are smaller (less factor work)
+// and their DAG is far shallower than the merged one, which the solve
+// schedule needs.  The merged partition and DAG are still computed exactly
+// (analysis.h) for the API and for parity.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "analysis.h"
+
+namespace bdlu {
+
+enum UnitKind : int32_t {
+  kUnitScalar = 0,  // 1x1 raw block: the LU is the diagonal entry
+  kUnitSmall = 1,   // dense LU in one CTA's shared memory
+  kUnitLarge = 2,   // dense blocked LU across CTAs
+};
+
+struct Plan {
+  int32_t n = 0;
+  int64_t nnz = 0;
+  int32_t nunits = 0;
+  int32_t small_max = 0;  // largest unit handled by the shared-memory kernel
+  std::vector<int32_t> ustart;   // nunits + 1
+  std::vector<int32_t> ukind;    // nunits
+  std::vector<int32_t> unit_of;  // n: unit of each permuted index
+  std::vector<int64_t> lu_off;   // nunits: column-major m*m arena slot, -1 for scalars
+  int64_t lu_size = 0;           // doubles
+  int64_t lu_large_begin = 0;    // arena range holding the large units
+  int64_t lu_large_end = 0;
+  // Diagonal-block entries of dense units: local column-major position and
+  // canonical source index.
+  std::vector<int64_t> dent_ptr;  // nunits + 1
+  std::vector<int32_t> dent_pos, dent_src;
+  // Scalar units: canonical source of the diagonal entry per permuted row
+  // (-1 for rows of dense units, -2 for a missing diagonal).
+  std::vector<int32_t> sdiag_src;
+  // Coupling CSR in permuted coordinates: every stored entry outside the
+  // unit diagonal blocks (all strictly upper at unit level).
+  std::vector<int32_t> cpl_ptr, cpl_col, cpl_src;
+  // Unit DAG levels (level 0 = no dependencies, solved first).
+  std::vector<int32_t> ulevel;
+  int32_t umax_level = 0;
+  std::vector<int32_t> lvl_scalar_ptr, lvl_scalar;  // permuted rows of scalar units, by level
+  std::vector<int32_t> lvl_dense_ptr, lvl_dense;    // dense unit ids, by level
+  std::vector<int32_t> small_units, large_units;
+  // Blocked LU steps for large units (panel width kPanel): per step, the
+  // active large units and per-unit CTA prefix sums for the swap/TRSM and
+  // GEMM-update kernels.
+  int32_t nsteps = 0;
+  std::vector<int32_t> step_ptr;        // nsteps + 1 into the arrays below
+  std::vector<int32_t> step_unit;       // active unit ids
+  std::vector<int32_t> step_trsm_pref;  // exclusive prefix of TRSM CTAs (per active unit, +1 total)
+  std::vector<int32_t> step_gemm_pref;  // exclusive prefix of GEMM tiles
+  std::vector<int32_t> step_trsm_total, step_gemm_total;  // per step
+  // Canonical CSR (original coordinates) for the residual.
+  std::vector<int32_t> csr_ptr;
+  double factor_flops = 0.0;
+  int64_t dense_entries = 0;
+  int32_t max_unit = 0;
+};
+
+constexpr int kPanel = 32;       // panel width of the blocked LU
+constexpr int kTrsmCols = 128;   // columns per CTA in the swap/TRSM kernel
+constexpr int kGemmTile = 64;    // square output tile of the update kernel
+
+Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max);
+
+}  // namespace bdlu

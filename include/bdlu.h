@@ -1,0 +1,196 @@
+/*
+ * bdlu.h - C ABI of the B200 numeric engine for BlockDAGLU's hot path.
+ *
+ * The reference exposes its numeric factor and solve through the C++ class
+ * blockdaglu::Solver (blockdaglu/include/blockdaglu/solver.h:43-126) and, for
+ * DLL callers, through CreateAlgorithm/DestroyAlgorithm
+ * (blockdaglu/src/exports.cpp:16-23).  This header is the plain-C boundary
+ * under an equivalent Solver: an opaque handle, plain pointers and sizes,
+ * integer status codes mirroring blockdaglu::SolverError, and no exceptions
+ * across the boundary.  The C++ class in include/blockdaglu/solver.h wraps it.
+ *
+ * Memory: the handle owns every device allocation.  Host-pointer arguments are
+ * read or written before the call returns.  Functions whose name ends in
+ * _device take device pointers and a CUDA stream (cudaStream_t passed as void*;
+ * NULL means the legacy default stream) and return once the work is enqueued.
+ *
+ * Threading: one handle must not be used from two threads at once.  Distinct
+ * handles may be used concurrently (solver.h:43-126 gives the same rule).
+ */
+#ifndef BDLU_H_
+#define BDLU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes, one for one with blockdaglu::SolverError (solver.h:19-31). */
+enum bdlu_status {
+  BDLU_OK = 0,
+  BDLU_NOT_PREPARED = 1,
+  BDLU_INVALID_DIMENSION = 2,
+  BDLU_INVALID_INDEX = 3,
+  BDLU_NON_FINITE_VALUE = 4,
+  BDLU_INVALID_RHS = 5,
+  BDLU_BACKEND_UNAVAILABLE = 6,
+  BDLU_ANALYSIS_FAILED = 7,
+  BDLU_FACTORIZATION_FAILED = 8,
+  BDLU_SOLVE_FAILED = 9,
+  BDLU_EXPORT_FAILED = 10
+};
+
+/* Route, as selected by analyze (solver.h:72-76 Mode). */
+enum bdlu_mode { BDLU_MODE_AUTO = 0, BDLU_MODE_KLU = 1, BDLU_MODE_BLOCK = 2 };
+
+typedef struct bdlu_solver bdlu_solver;
+
+/* Solver::Solver / ~Solver (solver.h:45-46). */
+bdlu_solver* bdlu_create(void);
+void bdlu_destroy(bdlu_solver* h);
+
+/* Solver::set_matrix(CooMatrix m, int32_t dimension) (solver.h:48-49,
+ * solver.cpp:749-800).  Storage only: the triplets are copied and nothing is
+ * validated until analyze.  dimension = -1 infers n from the largest index. */
+int bdlu_set_coo(bdlu_solver* h, const int32_t* rows, const int32_t* cols, const double* vals,
+                 int64_t nnz, int32_t dimension);
+
+/* Solver::analyze (solver.h:50, solver.cpp:802-1182): validation and
+ * canonicalisation, DM/BTF, block merge, UBTF split, block DAG and levels,
+ * upload of the per-pattern device structure. */
+int bdlu_analyze(bdlu_solver* h);
+
+/* Solver::factor (solver.h:51, solver.cpp:1184-1350): numeric factorisation of
+ * every diagonal block on the GPU. */
+int bdlu_factor(bdlu_solver* h);
+
+/* Value-only refactor (no counterpart API in the reference; there a value
+ * change is set_matrix + analyze + factor, solver.cpp:749-1350).  `vals` holds
+ * nnz values in canonical order: sorted by (row, col) with duplicates summed
+ * and exact zeros dropped, i.e. the order bdlu_canonical_pattern returns.  The
+ * pattern, permutations, blocks and pivot-free structure are reused. */
+int bdlu_refactor_values(bdlu_solver* h, const double* vals, int64_t nnz);
+int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nnz, void* stream);
+
+/* Solver::solve_in_place (solver.h:52, solver.cpp:1352-1539), generalised to
+ * nrhs right-hand sides stored column-major with leading dimension ldb >= n.
+ * B is overwritten by X. */
+int bdlu_solve(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs);
+int bdlu_solve_device(bdlu_solver* h, double* d_B, int32_t ldb, int32_t nrhs, void* stream);
+
+/* Refactor + solve in one call (the serving unit of work); values in
+ * canonical order, B column-major, overwritten by X. */
+int bdlu_refactor_solve(bdlu_solver* h, const double* vals, int64_t nnz, double* B, int32_t ldb,
+                        int32_t nrhs);
+
+/* Solver::last_error / last_error_message (solver.h:54-55).  Copies the
+ * message (NUL-terminated, truncated to len) and returns the status code. */
+int bdlu_last_error(const bdlu_solver* h, char* buf, int64_t len);
+
+/* Solver::n / selected_mode (solver.h:64-65): "KLU" or "BLOCK". */
+int32_t bdlu_n(const bdlu_solver* h);
+const char* bdlu_selected_mode(const bdlu_solver* h);
+
+/* Canonical pattern after analyze: nnz, and rows/cols if non-NULL. */
+int64_t bdlu_canonical_pattern(const bdlu_solver* h, int32_t* rows, int32_t* cols);
+
+/* Lazy exports, Solver::getP/getQ/getL/getU/get_rearranged_matrix
+ * (solver.h:58-62, solver.cpp:1665-1725).  COO triplets; call with cap = 0 to
+ * get the count, then again with buffers of that size.  Returns the entry
+ * count, or -(status) on failure.  The identity dense(rearranged) =
+ * dense(L) * dense(U) holds (apps/tests/main.cpp:170-195). */
+int64_t bdlu_export_p(bdlu_solver* h, int32_t* rows, int32_t* cols, double* vals, int64_t cap);
+int64_t bdlu_export_q(bdlu_solver* h, int32_t* rows, int32_t* cols, double* vals, int64_t cap);
+int64_t bdlu_export_l(bdlu_solver* h, int32_t* rows, int32_t* cols, double* vals, int64_t cap);
+int64_t bdlu_export_u(bdlu_solver* h, int32_t* rows, int32_t* cols, double* vals, int64_t cap);
+int64_t bdlu_export_rearranged(bdlu_solver* h, int32_t* rows, int32_t* cols, double* vals,
+                               int64_t cap);
+
+/* Per-result statistics (the reference prints these as USERALGO_PROFILE lines,
+ * solver.cpp:1510-1517). */
+typedef struct bdlu_stats {
+  int32_t n;
+  int32_t nblocks;
+  int32_t nblocks_raw;
+  int32_t max_block;
+  int32_t max_level;
+  int32_t refine_iters;      /* refinement steps taken by the last solve */
+  int32_t nunits;            /* raw BTF blocks: the device's factor/solve units */
+  int32_t unit_levels;       /* depth of the unit DAG: sequential steps of the solve */
+  int32_t max_unit;          /* largest raw BTF block */
+  int32_t factor_launches;   /* kernels launched by the last factor */
+  int32_t solve_launches;    /* kernels launched by the last solve */
+  int64_t nnz;
+  int64_t nnz_offdiag;
+  int64_t dense_entries;     /* sum of m^2 over dense-factored blocks */
+  double factor_flops;       /* algorithmic flops of one factor */
+  double residual_inf;       /* |Ax-b|_inf / (|A|_inf |x|_inf + |b|_inf), last solve, worst rhs */
+  double last_factor_ms;     /* device time of the last factor */
+  double last_solve_ms;      /* device time of the last solve */
+} bdlu_stats;
+int bdlu_get_stats(const bdlu_solver* h, bdlu_stats* out);
+
+/* Device time in ms of the phases of the last factor and solve, from CUDA
+ * events on the stream they ran on: [0] value gather, [1] shared-memory LU of
+ * small blocks, [2] blocked LU of large blocks, [3] first solve sweep
+ * (permute, level-scheduled block solve, unpermute), [4] refinement steps and
+ * residual.  Writes min(cap, 5) values; returns 5.  Synchronises. */
+int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
+
+/* Engine options.
+ *   "refine_iters": number of FP64 iterative-refinement steps (r = b - Ax,
+ *     solve, x += d) after each solve; default is the reference's REFINE_ITERS
+ *     environment value, else 0 (solver.cpp:1449-1465).
+ *   "analysis_only": 1 makes analyze stop after the host analysis (no device
+ *     upload); factor then reports BDLU_BACKEND_UNAVAILABLE.  For structure
+ *     inspection on machines without a GPU.
+ * Returns BDLU_OK, or BDLU_INVALID_DIMENSION for an unknown key. */
+int bdlu_set_option(bdlu_solver* h, const char* key, double value);
+
+/* ---- Host analysis, exposed for parity testing ----------------------------
+ * Same calling convention as SuiteSparse btf_order as bound by the reference
+ * (blockdaglu/src/btf_dynamic.h:19-28, called at ubtf_block_solver.cpp:661-670):
+ * returns nblocks; Q holds BTF_FLIP(-j-2) marks for unmatched columns. */
+int32_t bdlu_btf_order(int32_t n, const int32_t* Ap, const int32_t* Ai, int32_t* P, int32_t* Q,
+                       int32_t* R, int32_t* nmatch);
+
+/* merge_block_boundaries (ubtf_block_solver.cpp:393-476); returns new count
+ * of boundaries (nblocks'+1) written to Rout (capacity nR). */
+int32_t bdlu_merge_block_boundaries(const int32_t* R, int32_t nR, int32_t n, int32_t merge_max,
+                                    int32_t* Rout);
+
+/* Analysis products after analyze, for parity checks: copies whichever
+ * pointers are non-NULL.  Sizes: P,Q: n; R: nblocks+1; off_ptr: n+1;
+ * off_col/off_src: nnz_offdiag; level: nblocks. */
+int bdlu_get_decomposition(const bdlu_solver* h, int32_t* P, int32_t* Q, int32_t* R,
+                           int32_t* off_ptr, int32_t* off_col, int32_t* off_src, int32_t* level);
+
+/* Dense factor of block b after factor (for parity with the reference's dense
+ * micro-kernel, ubtf_block_solver.cpp:1450-1498): m*m values row-major and m
+ * LAPACK-style pivots.  Returns m, or -(status). */
+int32_t bdlu_get_block_lu(bdlu_solver* h, int32_t b, double* lu_rowmajor, int32_t* piv);
+
+/* ---- Seeded synthetic systems --------------------------------------------- */
+enum bdlu_synth_family { BDLU_SYNTH_BLOCK = 0, BDLU_SYNTH_CIRCUIT = 1, BDLU_SYNTH_PRECISION = 3 };
+typedef struct bdlu_synth bdlu_synth;
+/* family BLOCK: n rows, param = number of blocks (0: n/50).
+ * family CIRCUIT: n rows, param = number of Pareto blocks (0: 1000*n/200000).
+ * family PRECISION: n = number of large blocks, param = log10(kappa). */
+bdlu_synth* bdlu_synth_create(int32_t family, uint64_t seed, int32_t n, int32_t param, int32_t nrhs);
+void bdlu_synth_destroy(bdlu_synth* s);
+int32_t bdlu_synth_n(const bdlu_synth* s);
+int64_t bdlu_synth_nnz(const bdlu_synth* s);
+int32_t bdlu_synth_nrhs(const bdlu_synth* s);
+int32_t bdlu_synth_nblocks(const bdlu_synth* s);
+void bdlu_synth_copy(const bdlu_synth* s, int32_t* rows, int32_t* cols, double* vals, double* x_true,
+                     double* b);
+void bdlu_synth_block_sizes(const bdlu_synth* s, int32_t* sizes);
+void bdlu_synth_perturb(const bdlu_synth* s, uint64_t seed, double* vals_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BDLU_H_ */

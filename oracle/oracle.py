@@ -1,0 +1,196 @@
+"""ctypes access to the oracle (test infrastructure: only tests/, the smoke check
+and bench.py's cpu_baseline leg use it, always as the checker).
+
+liboracle.so is the C restatement in bdlu_oracle.c; canonicalize_small is a
+pure-Python restatement of validate_and_canonicalize_matrix
+(blockdaglu/src/solver.cpp:642-722) for small inputs.
+"""
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libbdlu_ref.so")
+_lib = None
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(os.path.join(HERE, "bdlu_oracle.c")):
+        build()
+    lib = ctypes.CDLL(LIB)
+    vp = ctypes.c_void_p
+    sig = {
+        "or_merge_block_boundaries": (ctypes.c_int32, [_i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p]),
+        "or_dense_lu": (ctypes.c_int, [_f64p, _i32p, ctypes.c_int32]),
+        "or_dense_solve": (ctypes.c_int, [_f64p, _i32p, ctypes.c_int32, _f64p]),
+        "or_split": (vp, [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _f64p, _i32p, _i32p, _i32p, ctypes.c_int32,
+                          ctypes.c_double]),
+        "or_free": (None, [vp]),
+        "or_levels": (None, [vp, _i32p, _i32p]),
+        "or_factor": (ctypes.c_int, [vp]),
+        "or_block_lu": (_f64p, [vp, ctypes.c_int32, ctypes.POINTER(_i32p), _i32p]),
+        "or_block_solve": (ctypes.c_int, [vp, _f64p]),
+        "or_solve_system": (ctypes.c_int, [vp, _f64p, ctypes.c_int]),
+        "or_metrics": (None, [ctypes.c_int32, ctypes.c_int64, _i32p, _i32p, _f64p, _f64p, _f64p, _f64p, _f64p]),
+        "or_failed_block": (ctypes.c_int32, [vp]),
+        "or_nblocks": (ctypes.c_int32, [vp]),
+        "or_offdiag_nnz": (ctypes.c_int32, [vp]),
+        "or_get_offdiag": (None, [vp, _i32p, _i32p, _f64p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _p32(a):
+    return a.ctypes.data_as(_i32p) if a is not None else None
+
+
+def _p64(a):
+    return a.ctypes.data_as(_f64p) if a is not None else None
+
+
+def merge_block_boundaries(R, n, merge_max=64):
+    lib = load()
+    r = np.ascontiguousarray(R, np.int32)
+    out = np.empty(len(r) + 2, np.int32)
+    k = lib.or_merge_block_boundaries(_p32(r), len(r), int(n), int(merge_max), _p32(out))
+    return out[:k].copy()
+
+
+def dense_lu(a):
+    """Reference micro-kernel on a row-major copy; returns (ok, lu, piv)."""
+    lib = load()
+    m = a.shape[0]
+    lu = np.ascontiguousarray(a, np.float64).copy()
+    piv = np.zeros(m, np.int32)
+    ok = lib.or_dense_lu(_p64(lu), _p32(piv), m)
+    return bool(ok), lu, piv
+
+
+def metrics(rows, cols, vals, x, b, x_true=None, n=None):
+    """(inf-norm relative residual, l2 relative residual, l2 relative error)."""
+    lib = load()
+    r = np.ascontiguousarray(rows, np.int32)
+    c = np.ascontiguousarray(cols, np.int32)
+    v = np.ascontiguousarray(vals, np.float64)
+    xx = np.ascontiguousarray(x, np.float64)
+    bb = np.ascontiguousarray(b, np.float64)
+    xt = np.ascontiguousarray(x_true, np.float64) if x_true is not None else None
+    out = np.zeros(3)
+    lib.or_metrics(int(n if n is not None else len(xx)), len(r), _p32(r), _p32(c), _p64(v), _p64(xx), _p64(bb), _p64(xt),
+                   _p64(out))
+    return float(out[0]), float(out[1]), float(out[2])
+
+
+class System:
+    """The reference's block route on a canonical COO under given (P, Q, merged R)."""
+
+    def __init__(self, n, rows, cols, vals, P, Q, R, drop=None):
+        self._lib = load()
+        self.n = int(n)
+        self._keep = [np.ascontiguousarray(a, t) for a, t in
+                      ((rows, np.int32), (cols, np.int32), (vals, np.float64), (P, np.int32), (Q, np.int32), (R, np.int32))]
+        r, c, v, p, q, rr = self._keep
+        if drop is None:
+            drop = 1e-20 if n >= 50000 else 0.0
+        self._s = self._lib.or_split(self.n, len(r), _p32(r), _p32(c), _p64(v), _p32(p), _p32(q), _p32(rr), len(rr) - 1,
+                                     float(drop))
+        if not self._s:
+            raise ValueError("permutation is not UBTF (found lower-block entries)")
+        self.nblocks = len(rr) - 1
+
+    def __del__(self):
+        s, self._s = getattr(self, "_s", None), None
+        if s:
+            self._lib.or_free(s)
+
+    def factor(self):
+        return bool(self._lib.or_factor(self._s))
+
+    def failed_block(self):
+        return self._lib.or_failed_block(self._s)
+
+    def levels(self):
+        lev = np.zeros(self.nblocks, np.int32)
+        mx = np.zeros(1, np.int32)
+        self._lib.or_levels(self._s, _p32(lev), _p32(mx))
+        return lev, int(mx[0])
+
+    def offdiag(self):
+        nnz = self._lib.or_offdiag_nnz(self._s)
+        ptr = np.empty(self.n + 1, np.int32)
+        col = np.empty(nnz, np.int32)
+        val = np.empty(nnz, np.float64)
+        self._lib.or_get_offdiag(self._s, _p32(ptr), _p32(col), _p64(val))
+        return ptr, col, val
+
+    def block_lu(self, b):
+        piv = _i32p()
+        m = ctypes.c_int32()
+        ptr = self._lib.or_block_lu(self._s, int(b), ctypes.byref(piv), ctypes.byref(m))
+        mm = m.value
+        lu = np.ctypeslib.as_array(ptr, shape=(mm * mm,)).reshape(mm, mm).copy() if mm else np.zeros((0, 0))
+        pv = np.ctypeslib.as_array(piv, shape=(mm,)).copy() if mm else np.zeros(0, np.int32)
+        return lu, pv
+
+    def solve(self, b, refine_iters=0):
+        x = np.ascontiguousarray(b, np.float64).copy()
+        taken = self._lib.or_solve_system(self._s, _p64(x), int(refine_iters))
+        if taken < 0:
+            raise RuntimeError("oracle block solve failed")
+        return x
+
+
+# Error codes of blockdaglu::SolverError used below.
+INVALID_DIMENSION, INVALID_INDEX, NON_FINITE = 2, 3, 4
+
+
+def canonicalize_small(coo, dimension_hint=-1):
+    """solver.cpp:642-722 for small inputs: returns (code, n, canonical list).
+
+    Duplicate sums use math.fsum (correctly rounded); the reference sums in
+    long double, which agrees on every input used by the tests."""
+    if dimension_hint < -1:
+        return INVALID_DIMENSION, 0, []
+    max_index = -1
+    for r, c, v in coo:
+        if r < 0 or c < 0:
+            return INVALID_INDEX, 0, []
+        if not math.isfinite(v):
+            return NON_FINITE, 0, []
+        if dimension_hint >= 0 and (r >= dimension_hint or c >= dimension_hint):
+            return INVALID_INDEX, 0, []
+        max_index = max(max_index, r, c)
+    n = dimension_hint if dimension_hint >= 0 else max_index + 1
+    if n <= 0:
+        return INVALID_DIMENSION, 0, []
+    groups = {}
+    for r, c, v in coo:
+        groups.setdefault((r, c), []).append(v)
+    out = []
+    for key in sorted(groups):
+        v = math.fsum(groups[key])
+        if not math.isfinite(v):
+            return NON_FINITE, 0, []
+        if v != 0.0:
+            out.append((key[0], key[1], v))
+    return 0, n, out
