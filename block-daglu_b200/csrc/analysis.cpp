@@ -13,7 +13,10 @@
 namespace bdlu {
 
 const char* getenv_compat(const char* name) {
-  // env.h:15-25: USERALGO_X is looked up as BLOCKDAGLU_X first.
+  // env.h:15-25 documents that USERALGO_X is looked up as BLOCKDAGLU_X first.
+  // (The reference's own helper compares 8 characters of the 9-character
+  // prefix and ends up querying "BLOCKDAGLU__X"; the documented names are
+  // honoured here.)
   if (!name) return nullptr;
   static const char kOld[] = "USERALGO_";
   if (std::strncmp(name, kOld, 9) == 0) {
