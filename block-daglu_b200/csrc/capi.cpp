@@ -235,6 +235,11 @@ int bdlu_solve(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs) {
   if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
   bdlu::SolveResidual r{};
   if (!h->engine->last_residual(nullptr, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+  // A zero pivot met by an earlier device-side refactor surfaces here.
+  if (!h->engine->factor_status(nullptr, err)) {
+    h->factored = false;
+    return fail(h, BDLU_FACTORIZATION_FAILED, err);
+  }
   const double denom = r.a_inf * r.x_inf + r.b_inf;
   h->last_residual = denom > 0.0 ? r.resid_inf / denom : r.resid_inf;
   h->last_refine = iters;
