@@ -149,6 +149,31 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  * Returns BDLU_OK, or BDLU_INVALID_DIMENSION for an unknown key. */
 int bdlu_set_option(bdlu_solver* h, const char* key, double value);
 
+/* ---- Dense batch solve without allocation -----------------------------------
+ * No counterpart in the reference.  For callers that must not allocate
+ * device memory where they solve (an allocator or memory budget closed after
+ * start-up, real-time loops that cannot absorb cudaMalloc's latency and
+ * implicit synchronisation, code called back inside another framework's step):
+ * solves A_i X_i = B_i for `batch` dense m x m matrices with the engine's
+ * dense-block partial-pivoting LU, using only the caller's buffers and a
+ * static device scratch built into the library (about 8.3 MiB, held on every
+ * GPU that loads the library until exit).  No cudaMalloc, cudaFree or other
+ * allocating call is made.
+ *   d_A: batch matrices, each m*m column-major, contiguous (not modified).
+ *   d_B, d_X: batch blocks of m x nrhs, column-major (ld m), contiguous; X may
+ *   be the same buffer as B.
+ * Limits: m <= 128, batch*m*m <= 1048576, batch*m <= 65536; larger sizes
+ * return BDLU_INVALID_DIMENSION with a message.  A singular matrix returns
+ * BDLU_FACTORIZATION_FAILED (X is then unspecified).  Uses the calling
+ * thread's current device; the call waits for `stream` before returning.
+ * The first call on a device resolves the scratch's address and sets a kernel
+ * attribute; make that first call before any stream capture.  Every call on a
+ * device shares the one scratch, so calls whose work overlaps on the GPU (other
+ * streams, other host threads) race and must be serialised by the caller.
+ * msg (may be NULL) receives an error message of at most msg_len bytes. */
+int bdlu_dense_batch_solve_noalloc(const double* d_A, int32_t m, int32_t batch, const double* d_B,
+                                   double* d_X, int32_t nrhs, void* stream, char* msg, int64_t msg_len);
+
 /* ---- Host analysis, exposed for parity testing ----------------------------
  * Same calling convention as SuiteSparse btf_order as bound by the reference
  * (blockdaglu/src/btf_dynamic.h:19-28, called at ubtf_block_solver.cpp:661-670):
