@@ -8,10 +8,8 @@
 //                     (ubtf_block_solver.cpp:1450-1498): same pivot choice,
 //                     same per-element operation order, no FMA contraction,
 //                     so factors are bit-identical
-//   k_scatter_large   value scatter into the arena slots of large units
-//   k_panel / k_swap_trsm / k_gemm_update
-//                     right-looking blocked LU (panel width kPanel) for large
-//                     units, batched over all units active at a step
+//   k_scatter_large   value scatter into the arena slots of large units (the
+//                     blocked LU and large-unit solves are in large.cu)
 //   k_solve_scalar / k_solve_dense
 //                     level-scheduled block back-substitution with the
 //                     off-diagonal update fused in (ubtf_block_solver.cpp:
@@ -19,6 +17,9 @@
 //   k_unpermute       x[Q[i]] (+)= xperm[i]
 //   k_residual        r = b - A x over the canonical CSR, with inf-norms
 #include "engine.h"
+
+#include "device_util.cuh"
+#include "large.h"
 
 #include <cuda_runtime.h>
 
@@ -31,37 +32,6 @@ namespace bdlu {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kFailZeroPivot = 1;
-
-__device__ __forceinline__ void report_failure(int32_t* status, int32_t unit) {
-  if (atomicCAS(status, 0, kFailZeroPivot) == 0) status[1] = unit;
-}
-
-// (value, index) maximum with the reference's tie rule: the smallest index
-// among equal maxima, i.e. the first strict maximum of an ascending scan.
-__device__ __forceinline__ void pivot_combine(double& best, int& bi, double ob, int oi, int none) {
-  if (oi == none) return;
-  if (bi == none || ob > best || (ob == best && oi < bi)) {
-    best = ob;
-    bi = oi;
-  }
-}
-
-__device__ __forceinline__ void warp_pivot_reduce(double& best, int& bi, int none) {
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) {
-    const double ob = __shfl_xor_sync(0xffffffffu, best, off);
-    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-    pivot_combine(best, bi, ob, oi, none);
-  }
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-  return v;
-}
-
 // ---------------------------------------------------------------------------
 // Value gather for coupling entries and scalar units.
 // ---------------------------------------------------------------------------
@@ -158,7 +128,7 @@ __global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double*
 }
 
 // ---------------------------------------------------------------------------
-// Large units: blocked right-looking LU in the arena (global memory).
+// Large units: value scatter into their (row-major) arena slots.
 // ---------------------------------------------------------------------------
 __global__ void k_scatter_large(DevPlan dp, const double* __restrict__ vals, const int32_t* __restrict__ units) {
   const int u = units[blockIdx.y];
@@ -166,178 +136,6 @@ __global__ void k_scatter_large(DevPlan dp, const double* __restrict__ vals, con
   for (int64_t e = dp.dent_ptr[u] + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < dp.dent_ptr[u + 1];
        e += static_cast<int64_t>(gridDim.x) * blockDim.x)
     A[dp.dent_pos[e]] = vals[dp.dent_src[e]];
-}
-
-// Panel factorisation: one CTA per active unit, columns k0..k0+nb-1, rows
-// k0..m-1, partial pivoting with the same tie rule; row swaps inside the
-// panel only (the rest of each row is swapped by k_swap_trsm).
-__global__ void __launch_bounds__(kThreads) k_panel(DevPlan dp, int32_t k0, int32_t ubase) {
-  __shared__ double s_best[kThreads / 32];
-  __shared__ int s_bi[kThreads / 32];
-  __shared__ int s_piv;
-  __shared__ double s_pbest;
-  const int u = dp.step_unit[ubase + blockIdx.x];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const int nb = min(kPanel, m - k0);
-  double* A = dp.lu + dp.lu_off[u];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int j = k0; j < k0 + nb; ++j) {
-    double* colj = A + static_cast<size_t>(j) * m;
-    double best = 0.0;
-    int bi = m;
-    for (int i = j + tid; i < m; i += kThreads) {
-      const double a = fabs(colj[i]);
-      if (bi == m || a > best) {
-        best = a;
-        bi = i;
-      }
-    }
-    warp_pivot_reduce(best, bi, m);
-    if (lane == 0) {
-      s_best[warp] = best;
-      s_bi[warp] = bi;
-    }
-    __syncthreads();
-    if (warp == 0) {
-      best = (lane < kThreads / 32) ? s_best[lane] : 0.0;
-      bi = (lane < kThreads / 32) ? s_bi[lane] : m;
-      warp_pivot_reduce(best, bi, m);
-      if (lane == 0) {
-        s_piv = bi;
-        s_pbest = best;
-      }
-    }
-    __syncthreads();
-    const int p = s_piv;
-    if (s_pbest == 0.0) {
-      if (tid == 0) report_failure(dp.status, u);
-      return;
-    }
-    if (tid == 0) dp.piv[s + j] = p;
-    if (p != j && tid < nb) {
-      double* c = A + static_cast<size_t>(k0 + tid) * m;
-      const double t = c[j];
-      c[j] = c[p];
-      c[p] = t;
-    }
-    __syncthreads();
-    const double ajj = colj[j];
-    for (int i = j + 1 + tid; i < m; i += kThreads) {
-      const double l = colj[i] / ajj;
-      colj[i] = l;
-      for (int jj = j + 1; jj < k0 + nb; ++jj) {
-        double* c = A + static_cast<size_t>(jj) * m;
-        c[i] = fma(-l, c[j], c[i]);
-      }
-    }
-    __syncthreads();
-  }
-}
-
-// Applies the panel's row swaps to every column outside the panel and solves
-// U12 = L11^{-1} A12 for the columns right of it.  One thread per column.
-__global__ void __launch_bounds__(kTrsmCols) k_swap_trsm(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
-  __shared__ double L11[kPanel * kPanel];
-  __shared__ int spiv[kPanel];
-  // Locate (unit, chunk) for this CTA.
-  int a = 0;
-  while (a + 1 < nact && dp.step_trsm_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
-  const int u = dp.step_unit[ubase + a];
-  const int chunk = blockIdx.x - dp.step_trsm_pref[ubase + a];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const int nb = min(kPanel, m - k0);
-  double* A = dp.lu + dp.lu_off[u];
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    const int q = t / nb, r = t - q * nb;  // L11(r, q)
-    L11[q * kPanel + r] = A[static_cast<size_t>(k0 + q) * m + k0 + r];
-  }
-  if (threadIdx.x < nb) spiv[threadIdx.x] = dp.piv[s + k0 + threadIdx.x];
-  __syncthreads();
-  const int j = chunk * kTrsmCols + threadIdx.x;
-  if (j >= m || (j >= k0 && j < k0 + nb)) return;
-  double* c = A + static_cast<size_t>(j) * m;
-  for (int r = 0; r < nb; ++r) {
-    const int p = spiv[r];
-    if (p != k0 + r) {
-      const double t = c[k0 + r];
-      c[k0 + r] = c[p];
-      c[p] = t;
-    }
-  }
-  if (j < k0 + nb) return;
-  double x[kPanel];
-#pragma unroll
-  for (int r = 0; r < kPanel; ++r) x[r] = (r < nb) ? c[k0 + r] : 0.0;
-#pragma unroll
-  for (int r = 1; r < kPanel; ++r) {
-    double v = x[r];
-#pragma unroll
-    for (int q = 0; q < r; ++q) v = fma(-L11[q * kPanel + r], x[q], v);
-    x[r] = v;
-  }
-#pragma unroll
-  for (int r = 0; r < kPanel; ++r)
-    if (r < nb) c[k0 + r] = x[r];
-}
-
-// Trailing update A22 -= L21 * U12, 64x64 output tile per CTA, 4x4 per thread.
-__global__ void __launch_bounds__(kThreads) k_gemm_update(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
-  __shared__ double Ls[kPanel][kGemmTile + 1];
-  __shared__ double Us[kPanel][kGemmTile + 1];
-  int a = 0;
-  while (a + 1 < nact && dp.step_gemm_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
-  const int u = dp.step_unit[ubase + a];
-  const int tile = blockIdx.x - dp.step_gemm_pref[ubase + a];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const int nb = min(kPanel, m - k0);
-  const int base = k0 + nb;
-  const int rest = m - base;
-  const int nt = (rest + kGemmTile - 1) / kGemmTile;
-  const int ti = tile % nt, tj = tile / nt;
-  const int i0 = base + ti * kGemmTile, j0 = base + tj * kGemmTile;
-  double* A = dp.lu + dp.lu_off[u];
-  const int tid = threadIdx.x;
-  for (int t = tid; t < kPanel * kGemmTile; t += kThreads) {
-    const int q = t / kGemmTile, i = t - q * kGemmTile;
-    Ls[q][i] = (q < nb && i0 + i < m) ? A[static_cast<size_t>(k0 + q) * m + i0 + i] : 0.0;
-  }
-  for (int t = tid; t < kPanel * kGemmTile; t += kThreads) {
-    const int jj = t / kPanel, q = t - jj * kPanel;
-    Us[q][jj] = (q < nb && j0 + jj < m) ? A[static_cast<size_t>(j0 + jj) * m + k0 + q] : 0.0;
-  }
-  __syncthreads();
-  const int tx = tid & 15, ty = tid >> 4;
-  double acc[4][4];
-#pragma unroll
-  for (int x = 0; x < 4; ++x)
-#pragma unroll
-    for (int y = 0; y < 4; ++y) acc[x][y] = 0.0;
-#pragma unroll 8
-  for (int q = 0; q < kPanel; ++q) {
-    double av[4], bv[4];
-#pragma unroll
-    for (int x = 0; x < 4; ++x) av[x] = Ls[q][tx + 16 * x];
-#pragma unroll
-    for (int y = 0; y < 4; ++y) bv[y] = Us[q][ty + 16 * y];
-#pragma unroll
-    for (int x = 0; x < 4; ++x)
-#pragma unroll
-      for (int y = 0; y < 4; ++y) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
-  }
-#pragma unroll
-  for (int y = 0; y < 4; ++y) {
-    const int j = j0 + ty + 16 * y;
-    if (j >= m) continue;
-    double* c = A + static_cast<size_t>(j) * m;
-#pragma unroll
-    for (int x = 0; x < 4; ++x) {
-      const int i = i0 + tx + 16 * x;
-      if (i < m) c[i] -= acc[x][y];
-    }
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -564,6 +362,7 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   if (!upload_vec(allocs_, plan.step_gemm_pref, &d.step_gemm_pref, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.lu_size), &d.lu, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.piv, err)) return false;
+  if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.lperm, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.sdiag, err)) return false;
   if (!alloc_dev(allocs_, plan.cpl_col.size(), &d.cpl_val, err)) return false;
   if (!alloc_dev(allocs_, 2, &d.status, err)) return false;
@@ -576,11 +375,7 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   int32_t small_m = 0;
   for (int32_t u : plan.small_units) small_m = std::max(small_m, plan.ustart[static_cast<size_t>(u) + 1] - plan.ustart[static_cast<size_t>(u)]);
   smem_small_ = static_cast<size_t>(small_m) * small_m * sizeof(double);
-  smem_solve_ = static_cast<size_t>(std::max<int32_t>(plan.max_unit, 1)) * sizeof(double);
-  if (smem_solve_ > 200 * 1024) {
-    err = "largest diagonal block exceeds the solve kernel's shared-memory vector";
-    return false;
-  }
+  smem_solve_ = static_cast<size_t>(std::max<int32_t>(small_m, 1)) * sizeof(double);
   {
     // The dynamic shared-memory limit is a per-function process-wide
     // attribute; raise it once to the device maximum so handles of different
@@ -607,6 +402,9 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   if (!upload_vec(allocs_, plan.large_units, &large_list, err)) return false;
   if (!upload_vec(allocs_, plan.lvl_scalar, &lvl_scalar, err)) return false;
   if (!upload_vec(allocs_, plan.lvl_dense, &lvl_dense, err)) return false;
+  const int32_t* lvl_large = nullptr;
+  if (!upload_vec(allocs_, plan.lvl_large, &lvl_large, err)) return false;
+  lvl_large_ = lvl_large;
   small_list_ = small_list;
   large_list_ = large_list;
   lvl_scalar_ = lvl_scalar;
@@ -630,19 +428,7 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
                               static_cast<size_t>(p.lu_large_end - p.lu_large_begin) * sizeof(double), stream));
     k_scatter_large<<<dim3(64, static_cast<unsigned>(p.large_units.size())), kThreads, 0, stream>>>(dp_, d_vals, large_list_);
     ++launches_factor_;
-    for (int32_t st = 0; st < p.nsteps; ++st) {
-      const int32_t ub = p.step_ptr[static_cast<size_t>(st)];
-      const int32_t na = p.step_ptr[static_cast<size_t>(st) + 1] - ub;
-      if (na <= 0) continue;
-      const int32_t k0 = st * kPanel;
-      k_panel<<<na, kThreads, 0, stream>>>(dp_, k0, ub);
-      k_swap_trsm<<<p.step_trsm_total[static_cast<size_t>(st)], kTrsmCols, 0, stream>>>(dp_, k0, ub, na);
-      launches_factor_ += 2;
-      if (p.step_gemm_total[static_cast<size_t>(st)] > 0) {
-        k_gemm_update<<<p.step_gemm_total[static_cast<size_t>(st)], kThreads, 0, stream>>>(dp_, k0, ub, na);
-        ++launches_factor_;
-      }
-    }
+    BDLU_CUDA(large_factor(dp_, p, large_list_, stream, &launches_factor_));
   }
   BDLU_CUDA(cudaGetLastError());
   BDLU_CUDA(cudaEventRecord(ev_[1], stream));
@@ -699,6 +485,10 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, int32_t nrhs
     if (d1 > d0) ++launches_solve_;
     if (d1 > d0)
       k_solve_dense<<<d1 - d0, kThreads, smem_solve_, stream>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp, nrhs);
+    const int32_t g0 = p.lvl_large_ptr[static_cast<size_t>(l)], g1 = p.lvl_large_ptr[static_cast<size_t>(l) + 1];
+    if (g1 > g0)
+      large_solve_level(dp_, p, lvl_large_ + g0, p.lvl_large.data() + g0, g1 - g0, rhs, ldr, xp, nrhs, stream,
+                        &launches_solve_);
   }
 }
 
@@ -795,6 +585,13 @@ bool Engine::download_unit(int32_t u, std::vector<double>& lu, std::vector<int32
   piv.resize(static_cast<size_t>(m));
   BDLU_CUDA(cudaMemcpy(lu.data(), dp_.lu + plan_.lu_off[static_cast<size_t>(u)], lu.size() * sizeof(double),
                        cudaMemcpyDeviceToHost));
+  if (plan_.ukind[static_cast<size_t>(u)] == kUnitLarge) {
+    // Large units are stored row-major; hand out column-major like the rest.
+    std::vector<double> t(lu.size());
+    for (int32_t i = 0; i < m; ++i)
+      for (int32_t j = 0; j < m; ++j) t[static_cast<size_t>(j) * m + i] = lu[static_cast<size_t>(i) * m + j];
+    lu.swap(t);
+  }
   BDLU_CUDA(cudaMemcpy(piv.data(), dp_.piv + s, piv.size() * sizeof(int32_t), cudaMemcpyDeviceToHost));
   return true;
 }

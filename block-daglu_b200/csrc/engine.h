@@ -34,6 +34,7 @@ struct DevPlan {
   const int32_t* step_gemm_pref;
   double* lu;
   int32_t* piv;
+  int32_t* lperm;  // final row order of each large unit (local indices)
   double* sdiag;
   double* cpl_val;
   int32_t* status;  // [0] failure code (0 = ok), [1] failing unit
@@ -115,6 +116,7 @@ class Engine {
   const int32_t* large_list_ = nullptr;
   const int32_t* lvl_scalar_ = nullptr;
   const int32_t* lvl_dense_ = nullptr;
+  const int32_t* lvl_large_ = nullptr;
   size_t smem_small_ = 0;
   size_t smem_solve_ = 0;
   int num_sms_ = 148;

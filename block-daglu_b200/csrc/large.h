@@ -1,0 +1,26 @@
+// Large units: blocked LU and block-triangular solves (large.cu).
+#pragma once
+
+#include <cuda_runtime_api.h>
+
+#include <cstdint>
+
+#include "engine.h"
+#include "plan.h"
+
+namespace bdlu {
+
+cudaError_t large_setup();
+
+// Enqueues the blocked LU of every large unit (slots already hold the unit
+// values, row-major) and the final row orders.
+cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, cudaStream_t stream,
+                         int32_t* launches);
+
+// Enqueues the solve of the large units of one level (d_units / h_units: the
+// level's list, single-CTA units first).  xp is the permuted solution.
+cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, const int32_t* d_units, const int32_t* h_units,
+                              int32_t count, const double* rhs, int32_t ldr, double* xp, int32_t nrhs,
+                              cudaStream_t stream, int32_t* launches);
+
+}  // namespace bdlu

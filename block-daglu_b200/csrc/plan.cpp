@@ -96,7 +96,10 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
       const int32_t s = p.ustart[static_cast<size_t>(ur)];
       const int32_t m = p.ustart[static_cast<size_t>(ur) + 1] - s;
       const int64_t q = dnext[static_cast<size_t>(ur)]++;
-      p.dent_pos[static_cast<size_t>(q)] = (cp - s) * m + (rp - s);
+      // Small units are column-major, large units row-major.
+      p.dent_pos[static_cast<size_t>(q)] = (p.ukind[static_cast<size_t>(ur)] == kUnitLarge)
+                                               ? (rp - s) * m + (cp - s)
+                                               : (cp - s) * m + (rp - s);
       p.dent_src[static_cast<size_t>(q)] = static_cast<int32_t>(k);
     } else {
       const int32_t q = cnext[static_cast<size_t>(rp)]++;
@@ -119,26 +122,39 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
   const int32_t nl = p.umax_level + 1;
   p.lvl_scalar_ptr.assign(static_cast<size_t>(nl) + 1, 0);
   p.lvl_dense_ptr.assign(static_cast<size_t>(nl) + 1, 0);
+  p.lvl_large_ptr.assign(static_cast<size_t>(nl) + 1, 0);
   for (int32_t u = 0; u < nu; ++u) {
     const int32_t l = p.ulevel[static_cast<size_t>(u)];
-    if (p.ukind[static_cast<size_t>(u)] == kUnitScalar) p.lvl_scalar_ptr[static_cast<size_t>(l) + 1]++;
-    else p.lvl_dense_ptr[static_cast<size_t>(l) + 1]++;
+    const int32_t k = p.ukind[static_cast<size_t>(u)];
+    if (k == kUnitScalar) p.lvl_scalar_ptr[static_cast<size_t>(l) + 1]++;
+    else if (k == kUnitSmall) p.lvl_dense_ptr[static_cast<size_t>(l) + 1]++;
+    else p.lvl_large_ptr[static_cast<size_t>(l) + 1]++;
   }
   for (int32_t l = 0; l < nl; ++l) {
     p.lvl_scalar_ptr[static_cast<size_t>(l) + 1] += p.lvl_scalar_ptr[static_cast<size_t>(l)];
     p.lvl_dense_ptr[static_cast<size_t>(l) + 1] += p.lvl_dense_ptr[static_cast<size_t>(l)];
+    p.lvl_large_ptr[static_cast<size_t>(l) + 1] += p.lvl_large_ptr[static_cast<size_t>(l)];
   }
   p.lvl_scalar.resize(static_cast<size_t>(p.lvl_scalar_ptr[static_cast<size_t>(nl)]));
   p.lvl_dense.resize(static_cast<size_t>(p.lvl_dense_ptr[static_cast<size_t>(nl)]));
+  p.lvl_large.resize(static_cast<size_t>(p.lvl_large_ptr[static_cast<size_t>(nl)]));
   {
     std::vector<int32_t> sn(p.lvl_scalar_ptr.begin(), p.lvl_scalar_ptr.end() - 1);
     std::vector<int32_t> dn(p.lvl_dense_ptr.begin(), p.lvl_dense_ptr.end() - 1);
-    for (int32_t u = 0; u < nu; ++u) {
-      const int32_t l = p.ulevel[static_cast<size_t>(u)];
-      if (p.ukind[static_cast<size_t>(u)] == kUnitScalar)
-        p.lvl_scalar[static_cast<size_t>(sn[static_cast<size_t>(l)]++)] = p.ustart[static_cast<size_t>(u)];
-      else
-        p.lvl_dense[static_cast<size_t>(dn[static_cast<size_t>(l)]++)] = u;
+    std::vector<int32_t> ln(p.lvl_large_ptr.begin(), p.lvl_large_ptr.end() - 1);
+    // Large units: those solved by one CTA first within each level.
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int32_t u = 0; u < nu; ++u) {
+        const int32_t l = p.ulevel[static_cast<size_t>(u)];
+        const int32_t k = p.ukind[static_cast<size_t>(u)];
+        const int32_t m = p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)];
+        if (pass == 0 && k == kUnitScalar)
+          p.lvl_scalar[static_cast<size_t>(sn[static_cast<size_t>(l)]++)] = p.ustart[static_cast<size_t>(u)];
+        else if (pass == 0 && k == kUnitSmall)
+          p.lvl_dense[static_cast<size_t>(dn[static_cast<size_t>(l)]++)] = u;
+        else if (k == kUnitLarge && (pass == 0) == (m <= kLargeSingleMax))
+          p.lvl_large[static_cast<size_t>(ln[static_cast<size_t>(l)]++)] = u;
+      }
     }
   }
 
@@ -149,10 +165,11 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
   p.step_ptr.assign(static_cast<size_t>(p.nsteps) + 1, 0);
   for (int32_t st = 0; st < p.nsteps; ++st) {
     const int32_t k0 = st * kPanel;
-    int32_t tpre = 0, gpre = 0;
+    int32_t tpre = 0, gpre = 0, rows = 0;
     for (int32_t u : p.large_units) {
       const int32_t m = p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)];
       if (m <= k0) continue;
+      rows = std::max(rows, m - k0);
       const int32_t nb = std::min(kPanel, m - k0);
       const int32_t rest = m - k0 - nb;
       p.step_unit.push_back(u);
@@ -165,6 +182,7 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
     p.step_ptr[static_cast<size_t>(st) + 1] = static_cast<int32_t>(p.step_unit.size());
     p.step_trsm_total.push_back(tpre);
     p.step_gemm_total.push_back(gpre);
+    p.step_max_rows.push_back(rows);
   }
 
   // Canonical CSR row pointer (original coordinates) for the residual.

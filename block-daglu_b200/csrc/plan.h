@@ -34,7 +34,8 @@ struct Plan {
   std::vector<int32_t> ustart;   // nunits + 1
   std::vector<int32_t> ukind;    // nunits
   std::vector<int32_t> unit_of;  // n: unit of each permuted index
-  std::vector<int64_t> lu_off;   // nunits: column-major m*m arena slot, -1 for scalars
+  std::vector<int64_t> lu_off;   // nunits: m*m arena slot (column-major for small units,
+                                 // row-major for large units), -1 for scalars
   int64_t lu_size = 0;           // doubles
   int64_t lu_large_begin = 0;    // arena range holding the large units
   int64_t lu_large_end = 0;
@@ -52,7 +53,8 @@ struct Plan {
   std::vector<int32_t> ulevel;
   int32_t umax_level = 0;
   std::vector<int32_t> lvl_scalar_ptr, lvl_scalar;  // permuted rows of scalar units, by level
-  std::vector<int32_t> lvl_dense_ptr, lvl_dense;    // dense unit ids, by level
+  std::vector<int32_t> lvl_dense_ptr, lvl_dense;    // small dense unit ids, by level
+  std::vector<int32_t> lvl_large_ptr, lvl_large;    // large unit ids by level, single-CTA solves first
   std::vector<int32_t> small_units, large_units;
   // Blocked LU steps for large units (panel width kPanel): per step, the
   // active large units and per-unit CTA prefix sums for the swap/TRSM and
@@ -63,6 +65,7 @@ struct Plan {
   std::vector<int32_t> step_trsm_pref;  // exclusive prefix of TRSM CTAs (per active unit, +1 total)
   std::vector<int32_t> step_gemm_pref;  // exclusive prefix of GEMM tiles
   std::vector<int32_t> step_trsm_total, step_gemm_total;  // per step
+  std::vector<int32_t> step_max_rows;                     // per step: largest m - k0
   // Canonical CSR (original coordinates) for the residual.
   std::vector<int32_t> csr_ptr;
   double factor_flops = 0.0;
@@ -70,9 +73,10 @@ struct Plan {
   int32_t max_unit = 0;
 };
 
-constexpr int kPanel = 32;       // panel width of the blocked LU
-constexpr int kTrsmCols = 128;   // columns per CTA in the swap/TRSM kernel
-constexpr int kGemmTile = 64;    // square output tile of the update kernel
+constexpr int kPanel = 32;          // panel width of the blocked LU
+constexpr int kTrsmCols = 128;      // columns per CTA in the swap/TRSM kernel
+constexpr int kGemmTile = 128;      // square output tile of the update kernel
+constexpr int kLargeSingleMax = 1024;  // large units solved by a single CTA
 
 Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max);
 

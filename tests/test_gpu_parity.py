@@ -250,3 +250,16 @@ def test_circuit_small_matches_oracle():
             lu, piv = s.block_lu(b)
             lu_ref, piv_ref = ref.block_lu(b)
             assert np.array_equal(piv, piv_ref) and np.array_equal(lu, lu_ref), b
+
+
+def test_global_route_tall_unit_fallback_panel(monkeypatch):
+    # MODE=klu on 7000 rows: one unit taller than a thread-block cluster holds,
+    # factored by the single-CTA global-memory panel and solved tile by tile.
+    monkeypatch.setenv("BLOCKDAGLU_MODE", "klu")
+    g = bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(0, 11), 7000, 140)
+    s = bd.Solver()
+    assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze() and s.factor(), s.last_error_message()
+    assert s.stats()["max_unit"] == 7000
+    x = g.b[:, 0].copy()
+    assert s.solve_in_place(x)
+    assert _inf_resid(g, g.vals, x, g.b[:, 0]) <= RESID_TOL
