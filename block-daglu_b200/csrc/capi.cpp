@@ -23,6 +23,12 @@
 using bdlu::Status;
 
 namespace {
+// Normwise residual above which a refactor that reused the pivot order is
+// redone with partial pivoting by the host-buffer solve.
+constexpr double kReuseResidualLimit = 1e-12;
+}  // namespace
+
+namespace {
 
 int fail(bdlu_solver* h, int code, std::string msg) {
   h->last_error = code;
@@ -67,17 +73,27 @@ int ensure_validated(bdlu_solver* h) {
   return BDLU_OK;
 }
 
-int do_factor(bdlu_solver* h, cudaStream_t stream) {
+// Factor from the engine's value buffer.  reuse: large blocks keep the pivot
+// order of the last full factorisation (value-only refactor); a zero pivot
+// met that way falls back to a factorisation with pivoting.
+int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   std::string err;
-  if (!h->engine->factor_async(h->engine->values_buffer(), stream, err))
-    return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
-  if (!h->engine->factor_status(stream, err)) {
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const bool r = reuse && attempt == 0;
+    if (!h->engine->factor_async(h->engine->values_buffer(), stream, err, r))
+      return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+    const int st = h->engine->factor_status(stream, err);
+    if (st == 0) {
+      h->factored = true;
+      h->exported = false;
+      return BDLU_OK;
+    }
+    if (st == 2 && r) continue;
     h->factored = false;
-    return fail(h, BDLU_FACTORIZATION_FAILED, err);
+    return fail(h, st < 0 ? BDLU_BACKEND_UNAVAILABLE : BDLU_FACTORIZATION_FAILED, err);
   }
-  h->factored = true;
-  h->exported = false;
-  return BDLU_OK;
+  h->factored = false;
+  return fail(h, BDLU_FACTORIZATION_FAILED, err);
 }
 
 int upload_values(bdlu_solver* h, const double* vals, bool device, cudaStream_t stream) {
@@ -181,7 +197,7 @@ int bdlu_factor(bdlu_solver* h) {
   if (!h->decomposed) return fail(h, BDLU_NOT_PREPARED, "analyze must succeed before factor");
   if (!h->engine) return fail(h, BDLU_BACKEND_UNAVAILABLE, "analysis was run without a device (analysis_only)");
   if (const int st = upload_values(h, h->coo.val.data(), false, nullptr)) return st;
-  return do_factor(h, nullptr);
+  return do_factor(h, nullptr, false);
 }
 
 int bdlu_refactor_values(bdlu_solver* h, const double* vals, int64_t nnz) {
@@ -194,7 +210,7 @@ int bdlu_refactor_values(bdlu_solver* h, const double* vals, int64_t nnz) {
     if (!std::isfinite(vals[k])) return fail(h, BDLU_NON_FINITE_VALUE, "matrix contains NaN or infinity");
   std::memcpy(h->coo.val.data(), vals, static_cast<size_t>(nnz) * sizeof(double));
   if (const int st = upload_values(h, vals, false, nullptr)) return st;
-  return do_factor(h, nullptr);
+  return do_factor(h, nullptr, h->reuse_pivots);
 }
 
 int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nnz, void* stream) {
@@ -206,7 +222,8 @@ int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nn
   auto s = static_cast<cudaStream_t>(stream);
   if (const int st = upload_values(h, d_vals, true, s)) return st;
   std::string err;
-  if (!h->engine->factor_async(h->engine->values_buffer(), s, err)) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+  if (!h->engine->factor_async(h->engine->values_buffer(), s, err, h->reuse_pivots))
+    return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
   // Zero pivots are reported by the next synchronising call (bdlu_solve_status).
   h->factored = true;
   h->exported = false;
@@ -235,13 +252,31 @@ int bdlu_solve(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs) {
   if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
   bdlu::SolveResidual r{};
   if (!h->engine->last_residual(nullptr, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-  // A zero pivot met by an earlier device-side refactor surfaces here.
-  if (!h->engine->factor_status(nullptr, err)) {
+  auto relres = [](const bdlu::SolveResidual& q) {
+    const double denom = q.a_inf * q.x_inf + q.b_inf;
+    return denom > 0.0 ? q.resid_inf / denom : q.resid_inf;
+  };
+  h->last_residual = relres(r);
+  // A zero pivot met by an earlier device-side refactor surfaces here.  A
+  // refactor that reused the pivot order of large blocks is redone with
+  // pivoting when it hit a zero pivot or when the residual leaves the bound.
+  const int fst = h->engine->factor_status(nullptr, err);
+  const bool redo = h->engine->last_factor_reused() &&
+                    (fst == 2 || !(h->last_residual <= kReuseResidualLimit));
+  if (fst == 1 || fst < 0 || (fst == 2 && !redo)) {
     h->factored = false;
-    return fail(h, BDLU_FACTORIZATION_FAILED, err);
+    return fail(h, fst < 0 ? BDLU_BACKEND_UNAVAILABLE : BDLU_FACTORIZATION_FAILED, err);
   }
-  const double denom = r.a_inf * r.x_inf + r.b_inf;
-  h->last_residual = denom > 0.0 ? r.resid_inf / denom : r.resid_inf;
+  if (redo) {
+    if (const int st = do_factor(h, nullptr, false)) return st;
+    if (!h->engine->restore_rhs(d_B, h->n, nrhs, nullptr, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+    if (!h->engine->solve_async(d_B, h->n, nrhs, iters, nullptr, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+    e = cudaMemcpy2D(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
+                     static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
+    if (!h->engine->last_residual(nullptr, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+    h->last_residual = relres(r);
+  }
   h->last_refine = iters;
   if (!std::isfinite(h->last_residual)) return fail(h, BDLU_SOLVE_FAILED, "block solve produced a non-finite solution");
   return BDLU_OK;
@@ -327,6 +362,10 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
   const std::string k(key);
   if (k == "refine_iters") {
     h->refine_iters = static_cast<int32_t>(value);
+    return BDLU_OK;
+  }
+  if (k == "refactor_pivoting") {
+    h->reuse_pivots = value == 0.0;
     return BDLU_OK;
   }
   if (k == "analysis_only") {

@@ -29,6 +29,7 @@ struct bdlu_solver {
   // Options.
   int32_t refine_iters = -1;  // -1: REFINE_ITERS env, else 0
   bool analysis_only = false; // host analysis without device upload (inspection, CPU tests)
+  bool reuse_pivots = true;   // value-only refactors keep the pivot order of large blocks
   // Error state (solver.h:122-123).
   int last_error = BDLU_OK;
   std::string last_message;

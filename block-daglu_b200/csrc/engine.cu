@@ -339,6 +339,8 @@ static bool alloc_dev(std::vector<void*>& allocs, size_t count, T** out, std::st
 
 bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalCoo& a, std::string& err) {
   release();
+  have_pivots_ = false;
+  last_reuse_ = false;
   plan_ = plan;
   DevPlan d{};
   d.n = plan.n;
@@ -363,6 +365,7 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.lu_size), &d.lu, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.piv, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.lperm, err)) return false;
+  if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.liperm, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.sdiag, err)) return false;
   if (!alloc_dev(allocs_, plan.cpl_col.size(), &d.cpl_val, err)) return false;
   if (!alloc_dev(allocs_, 2, &d.status, err)) return false;
@@ -412,8 +415,10 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   return true;
 }
 
-bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string& err) {
+bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string& err, bool reuse_pivots) {
   const Plan& p = plan_;
+  const bool reuse = reuse_pivots && have_pivots_ && !p.large_units.empty();
+  last_reuse_ = reuse;
   BDLU_CUDA(cudaMemsetAsync(d_status_, 0, 2 * sizeof(int32_t), stream));
   BDLU_CUDA(cudaEventRecord(ev_[0], stream));
   const int64_t ncpl = static_cast<int64_t>(p.cpl_col.size());
@@ -426,9 +431,14 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   if (!p.large_units.empty()) {
     BDLU_CUDA(cudaMemsetAsync(dp_.lu + p.lu_large_begin, 0,
                               static_cast<size_t>(p.lu_large_end - p.lu_large_begin) * sizeof(double), stream));
-    k_scatter_large<<<dim3(64, static_cast<unsigned>(p.large_units.size())), kThreads, 0, stream>>>(dp_, d_vals, large_list_);
+    if (reuse) {
+      BDLU_CUDA(large_scatter_reuse(dp_, p, d_vals, large_list_, stream));
+    } else {
+      k_scatter_large<<<dim3(64, static_cast<unsigned>(p.large_units.size())), kThreads, 0, stream>>>(dp_, d_vals,
+                                                                                                   large_list_);
+    }
     ++launches_factor_;
-    BDLU_CUDA(large_factor(dp_, p, large_list_, stream, &launches_factor_));
+    BDLU_CUDA(large_factor(dp_, p, large_list_, reuse, stream, &launches_factor_));
   }
   BDLU_CUDA(cudaGetLastError());
   BDLU_CUDA(cudaEventRecord(ev_[1], stream));
@@ -436,15 +446,24 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   return true;
 }
 
-bool Engine::factor_status(cudaStream_t stream, std::string& err) {
+int Engine::factor_status(cudaStream_t stream, std::string& err) {
   int32_t st[2] = {0, 0};
-  BDLU_CUDA(cudaMemcpyAsync(st, d_status_, sizeof(st), cudaMemcpyDeviceToHost, stream));
-  BDLU_CUDA(cudaStreamSynchronize(stream));
-  if (st[0] != 0) {
-    err = "block factorization failed: zero pivot in diagonal block " + std::to_string(st[1]);
-    return false;
+  cudaError_t e = cudaMemcpyAsync(st, d_status_, sizeof(st), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) {
+    err = std::string("factor status: ") + cudaGetErrorString(e);
+    return -1;
   }
-  return true;
+  if (st[0] == 1) {
+    err = "block factorization failed: zero pivot in diagonal block " + std::to_string(st[1]);
+    return 1;
+  }
+  if (st[0] == 2) {
+    err = "reused pivot order met a zero pivot in diagonal block " + std::to_string(st[1]);
+    return 2;
+  }
+  if (!last_reuse_) have_pivots_ = true;
+  return 0;
 }
 
 bool Engine::ensure_work(int32_t nrhs, std::string& err) {
@@ -518,6 +537,14 @@ bool Engine::solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_
   BDLU_CUDA(cudaEventRecord(ev_[3], stream));
   last_nrhs_ = nrhs;
   solve_timed_ = true;
+  return true;
+}
+
+bool Engine::restore_rhs(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream, std::string& err) {
+  const int32_t n = plan_.n;
+  BDLU_CUDA(cudaMemcpy2DAsync(d_B, static_cast<size_t>(ldb) * sizeof(double), d_b0_, static_cast<size_t>(n) * sizeof(double),
+                              static_cast<size_t>(n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToDevice,
+                              stream));
   return true;
 }
 

@@ -34,7 +34,8 @@ struct DevPlan {
   const int32_t* step_gemm_pref;
   double* lu;
   int32_t* piv;
-  int32_t* lperm;  // final row order of each large unit (local indices)
+  int32_t* lperm;   // final row order of each large unit (local indices)
+  int32_t* liperm;  // its inverse
   double* sdiag;
   double* cpl_val;
   int32_t* status;  // [0] failure code (0 = ok), [1] failing unit
@@ -59,15 +60,22 @@ class Engine {
   bool upload(const Plan& plan, const Decomposition& dec, const CanonicalCoo& a, std::string& err);
 
   // Enqueues the numeric factor of every unit from canonical-order values
-  // already on the device (d_vals, nnz entries).
-  bool factor_async(const double* d_vals, cudaStream_t stream, std::string& err);
-  // Waits for the factor and reports a zero pivot as a failure.
-  bool factor_status(cudaStream_t stream, std::string& err);
+  // already on the device (d_vals, nnz entries).  reuse_pivots: large units
+  // keep the row order of the last full factorisation (no pivot search);
+  // ignored until one full factorisation has succeeded.
+  bool factor_async(const double* d_vals, cudaStream_t stream, std::string& err, bool reuse_pivots = false);
+  // Waits for the factor.  Returns 0 (ok), 1 (zero pivot: the matrix is
+  // singular) or 2 (a reused pivot order met a zero pivot: factor again with
+  // pivoting); -1 on a CUDA error.
+  int factor_status(cudaStream_t stream, std::string& err);
+  bool last_factor_reused() const { return last_reuse_; }
 
   // Enqueues X = A^{-1} B for nrhs columns (column-major, ld ldb, in place),
   // followed by `refine_iters` FP64 refinement steps and the residual norms.
   bool solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_iters, cudaStream_t stream,
                    std::string& err);
+  // Copies the right-hand sides saved by the last solve_async back into d_B.
+  bool restore_rhs(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream, std::string& err);
   // Residual norms of the last solve (synchronises the stream), worst column.
   bool last_residual(cudaStream_t stream, SolveResidual& out, std::string& err);
 
@@ -120,6 +128,8 @@ class Engine {
   size_t smem_small_ = 0;
   size_t smem_solve_ = 0;
   int num_sms_ = 148;
+  bool have_pivots_ = false;  // a full factorisation of this pattern succeeded
+  bool last_reuse_ = false;
 
  public:
   // Kernel launches enqueued by the last factor / solve.

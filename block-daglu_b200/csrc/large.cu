@@ -24,7 +24,15 @@
 //                     U12 = L11^{-1} A12, one thread per column (coalesced)
 //   k_gemm_rm         A22 -= L21 * U12, FP64, 128 x 128 output tile per CTA,
 //                     8 x 8 accumulators per thread
-//   k_large_perm      final row order of each unit from its pivot sequence
+//   k_large_perm      final row order of each unit (and its inverse) from its
+//                     pivot sequence
+// Refactor with the stored pivot order (value-only refactor; the pivot order
+// of KLU's klu_refactor is reused the same way):
+//   k_scatter_large_perm  values scattered with rows already permuted
+//   k_diag_nopiv      nb x nb diagonal block, no pivot search; a zero or
+//                     non-finite pivot flags the unit for full pivoting
+//   k_trsm_l          L21 = A21 U11^{-1}, one warp per row
+//   k_swap_trsm_rm (no swaps) and k_gemm_rm as above
 // Solve (per level holding large units):
 //   k_large_rhs       rhs of every row in pivot order: b - A_cpl x, gathered
 //                     through the unit's final row order
@@ -53,22 +61,52 @@ namespace {
 constexpr int kPT = 512;                  // panel kernel threads
 constexpr int kPStride = kPanel + 1;      // shared-memory row stride of the panel (doubles)
 constexpr int kClusterMaxCtas = 8;        // portable cluster size
-constexpr int kPanelRowsMax = 800;        // panel rows one CTA holds (800 * 33 * 8 = 211,200 B)
+constexpr int kPanelRowsMax = 640;        // panel rows one CTA holds (one per thread)
 constexpr int kGT = 128;                  // GEMM output tile
 constexpr int kGThreads = 256;
 constexpr int kTile = 64;                 // solve tile
 constexpr int kSolveThreads = 256;
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kPT) k_panel_cluster(DevPlan dp, int32_t k0, int32_t ubase, int32_t csize) {
+// Panel factorisation in a thread-block cluster.  Each thread of a CTA holds
+// one panel row in registers (the column loop is unrolled, so register indices
+// are static).  Row swaps are logical: a thread carries the current position
+// of its row, and a swap of positions jj and p exchanges the two position
+// registers; rows are written to their final positions at the end.  Per
+// column: every warp finds its pivot candidate (largest |a|, ties to the
+// smallest position: the reference's first strict maximum) and stages that
+// row in shared memory; after one CTA barrier warp 0 pushes the CTA's
+// candidate row, value and position to every CTA of the cluster (DSMEM);
+// after one cluster barrier every warp combines the cluster's candidates
+// lane-parallel, and each thread applies the rank-1 update to its row.
+// Candidate buffers alternate by column parity, so one CTA and one cluster
+// barrier per column suffice.  Multipliers use the reciprocal of the pivot, as
+// LAPACK's dgetf2 does.
+constexpr int kPanelThreads = 640;
+constexpr int kPanelWarps = kPanelThreads / 32;
+
+// Warp arg-max over (value >= 0, position): the largest value, ties to the
+// smallest position.  Lanes with valid == false do not take part.  Returns the
+// winning lane (or -1 when no lane is valid); best/bpos hold the winner.
+__device__ __forceinline__ int warp_argmax(double val, int pos, bool valid, double& best, int& bpos) {
+  double mx = valid ? val : -1.0;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  const bool tie = valid && val == mx;
+  const int mn = __reduce_min_sync(0xffffffffu, tie ? pos : 0x7fffffff);
+  const unsigned who = __ballot_sync(0xffffffffu, tie && pos == mn);
+  best = mx;
+  bpos = mn;
+  return who ? __ffs(who) - 1 : -1;
+}
+
+__global__ void __launch_bounds__(kPanelThreads, 1) k_panel_cluster(DevPlan dp, int32_t k0, int32_t ubase,
+                                                                    int32_t csize) {
   cg::cluster_group cl = cg::this_cluster();
-  extern __shared__ double P[];
   __shared__ double cand[2][kClusterMaxCtas][kPanel + 2];
-  __shared__ double jbuf[2][kPanel];
-  __shared__ double s_best[kPT / 32];
-  __shared__ int s_bi[kPT / 32];
-  __shared__ double s_cbest;
-  __shared__ int s_cbi;
+  __shared__ double wrow[kPanelWarps][kPanel];
+  __shared__ double wbest[kPanelWarps];
+  __shared__ int wpos[kPanelWarps];
   const int rank = static_cast<int>(cl.block_rank());
   const int u = dp.step_unit[ubase + blockIdx.x / csize];
   const int s = dp.ustart[u];
@@ -80,93 +118,72 @@ __global__ void __launch_bounds__(kPT) k_panel_cluster(DevPlan dp, int32_t k0, i
   const int r0 = k0 + rank * chunk;
   const int r1 = min(m, r0 + chunk);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // Load my rows of the panel.
-  for (int t = tid; t < (r1 > r0 ? (r1 - r0) : 0) * kPanel; t += kPT) {
-    const int i = t / kPanel, c = t - i * kPanel;
-    P[i * kPStride + c] = (c < nb) ? A[static_cast<size_t>(r0 + i) * m + k0 + c] : 0.0;
-  }
-  __syncthreads();
-  for (int j = 0; j < nb; ++j) {
+  const bool has = r0 + tid < r1;
+  int pos = has ? r0 + tid : m;             // current position of this thread's row
+  double v[kPanel];
+#pragma unroll
+  for (int c = 0; c < kPanel; ++c) v[c] = (has && c < nb) ? A[static_cast<size_t>(r0 + tid) * m + k0 + c] : 0.0;
+#pragma unroll
+  for (int j = 0; j < kPanel; ++j) {
+    if (j >= nb) break;
     const int jj = k0 + j;
     const int par = j & 1;
-    // Local candidate among rows >= jj.
-    double best = 0.0;
-    int bi = m;
-    for (int i = max(r0, jj) + tid; i < r1; i += kPT) {
-      const double a = fabs(P[(i - r0) * kPStride + j]);
-      if (bi == m || a > best) {
-        best = a;
-        bi = i;
+    {
+      double best;
+      int bpos;
+      const int wl = warp_argmax(fabs(v[j]), pos, has && pos >= jj, best, bpos);
+      if (wl == lane) {
+#pragma unroll
+        for (int c = 0; c < kPanel; ++c) wrow[warp][c] = v[c];
       }
-    }
-    warp_pivot_reduce(best, bi, m);
-    if (lane == 0) {
-      s_best[warp] = best;
-      s_bi[warp] = bi;
+      if (lane == 0) {
+        wbest[warp] = best;
+        wpos[warp] = (wl >= 0) ? bpos : m;
+      }
     }
     __syncthreads();
     if (warp == 0) {
-      best = (lane < kPT / 32) ? s_best[lane] : 0.0;
-      bi = (lane < kPT / 32) ? s_bi[lane] : m;
-      warp_pivot_reduce(best, bi, m);
-      if (lane == 0) {
-        s_cbest = best;
-        s_cbi = bi;
+      const bool ok = lane < kPanelWarps && wpos[lane] != m;
+      double best;
+      int bpos;
+      const int ww = warp_argmax(ok ? wbest[lane] : 0.0, ok ? wpos[lane] : m, ok, best, bpos);
+      const double val = (ww >= 0) ? wrow[ww][lane] : 0.0;
+      for (int q = 0; q < csize; ++q) {
+        double* dst = cl.map_shared_rank(&cand[par][rank][0], q);
+        dst[lane] = val;
+        if (lane == 0) {
+          dst[kPanel] = (ww >= 0) ? best : -1.0;
+          dst[kPanel + 1] = static_cast<double>((ww >= 0) ? bpos : m);
+        }
       }
-    }
-    __syncthreads();
-    // Push the candidate (row, value, index) to every CTA of the cluster;
-    // the owner of row jj pushes that row as well.
-    const int oj = (jj - k0) / chunk;
-    if (warp < csize) {
-      const int q = warp;
-      double* dst = cl.map_shared_rank(&cand[par][rank][0], q);
-      const int cbi = s_cbi;
-      if (lane < kPanel) dst[lane] = (cbi != m) ? P[(cbi - r0) * kPStride + lane] : 0.0;
-      if (lane == 0) {
-        dst[kPanel] = s_cbest;
-        dst[kPanel + 1] = static_cast<double>(cbi);
-      }
-    } else if (rank == oj && warp >= kClusterMaxCtas && warp < kClusterMaxCtas + csize) {
-      const int q = warp - kClusterMaxCtas;
-      double* dst = cl.map_shared_rank(&jbuf[par][0], q);
-      if (lane < kPanel) dst[lane] = P[(jj - r0) * kPStride + lane];
     }
     cl.sync();
-    // Every CTA combines the candidates in rank order: the same pivot.
-    best = cand[par][0][kPanel];
-    bi = static_cast<int>(cand[par][0][kPanel + 1]);
-    int owner = 0;
-    for (int q = 1; q < csize; ++q) {
-      const double ob = cand[par][q][kPanel];
-      const int oi = static_cast<int>(cand[par][q][kPanel + 1]);
-      const int before = bi;
-      pivot_combine(best, bi, ob, oi, m);
-      if (bi != before) owner = q;
-    }
-    if (bi == m || best == 0.0) {
+    double gbest;
+    int gpos;
+    const bool cok = lane < csize && cand[par][lane][kPanel] >= 0.0;
+    const int owner = warp_argmax(cok ? cand[par][lane][kPanel] : 0.0,
+                                  cok ? static_cast<int>(cand[par][lane][kPanel + 1]) : m, cok, gbest, gpos);
+    if (owner < 0 || gbest == 0.0) {
       if (rank == 0 && tid == 0) report_failure(dp.status, u);
       cl.sync();
       return;
     }
-    const int p = bi;
-    const double* U = cand[par][owner];
-    if (rank == 0 && tid == 0) dp.piv[s + jj] = p;
-    if (rank == oj && tid < nb) P[(jj - r0) * kPStride + tid] = U[tid];
-    if (rank == owner && p != jj && tid < nb) P[(p - r0) * kPStride + tid] = jbuf[par][tid];
-    __syncthreads();
-    const double d = U[j];
-    for (int i = max(r0, jj + 1) + tid; i < r1; i += kPT) {
-      double* row = P + (i - r0) * kPStride;
-      const double l = row[j] / d;
-      row[j] = l;
-      for (int c = j + 1; c < nb; ++c) row[c] = fma(-l, U[c], row[c]);
+    if (rank == 0 && tid == 0) dp.piv[s + jj] = gpos;
+    // Logical swap of positions jj and gpos; the row now at jj is final.
+    if (pos == jj) pos = gpos;
+    else if (pos == gpos) pos = jj;
+    if (has && pos > jj) {
+      const double* U = cand[par][owner];
+      const double l = v[j] * (1.0 / U[j]);
+#pragma unroll
+      for (int c = j + 1; c < kPanel; ++c) v[c] = fma(-l, U[c], v[c]);
+      v[j] = l;
     }
-    __syncthreads();
   }
-  for (int t = tid; t < (r1 > r0 ? (r1 - r0) : 0) * nb; t += kPT) {
-    const int i = t / nb, c = t - i * nb;
-    A[static_cast<size_t>(r0 + i) * m + k0 + c] = P[i * kPStride + c];
+  if (has) {
+#pragma unroll
+    for (int c = 0; c < kPanel; ++c)
+      if (c < nb) A[static_cast<size_t>(pos) * m + k0 + c] = v[c];
   }
   cl.sync();
 }
@@ -238,10 +255,15 @@ __global__ void __launch_bounds__(kPT) k_panel_global(DevPlan dp, int32_t k0, in
 }
 
 // Row swaps of the panel applied to all other columns, then U12 for the
-// columns right of the panel.  One thread per column.
-__global__ void __launch_bounds__(kTrsmCols) k_swap_trsm_rm(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
+// columns right of the panel.  One thread per column.  The nb sequential swaps
+// touch at most 2*nb rows; their net permutation is formed once per CTA in
+// shared memory, so each thread loads every touched value before it stores.
+__global__ void __launch_bounds__(kTrsmCols) k_swap_trsm_rm(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
+                                                             int32_t swaps) {
   __shared__ double L11[kPanel][kPanel + 1];
-  __shared__ int spiv[kPanel];
+  __shared__ int rows[2 * kPanel];  // touched rows: k0..k0+nb-1 first, then the others
+  __shared__ int src[2 * kPanel];   // new value of rows[q] = old value of rows[src[q]]
+  __shared__ int s_cnt;
   int a = 0;
   while (a + 1 < nact && dp.step_trsm_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
   const int u = dp.step_unit[ubase + a];
@@ -254,24 +276,53 @@ __global__ void __launch_bounds__(kTrsmCols) k_swap_trsm_rm(DevPlan dp, int32_t 
     const int r = t / nb, q = t - r * nb;
     L11[r][q] = A[static_cast<size_t>(k0 + r) * m + k0 + q];
   }
-  if (threadIdx.x < nb) spiv[threadIdx.x] = dp.piv[s + k0 + threadIdx.x];
+  if (threadIdx.x == 0) {
+    int cnt = nb;
+    for (int r = 0; r < nb; ++r) {
+      rows[r] = k0 + r;
+      src[r] = r;
+    }
+    // Simulate the swaps on positions: pos_of[row] via linear search (<= 64).
+    for (int r = 0; r < nb && swaps; ++r) {
+      const int p = dp.piv[s + k0 + r];
+      if (p == k0 + r) continue;
+      int qp = -1;
+      for (int q = nb; q < cnt; ++q)
+        if (rows[q] == p) qp = q;
+      if (p < k0 + nb) qp = p - k0;
+      if (qp < 0) {
+        qp = cnt++;
+        rows[qp] = p;
+        src[qp] = qp;
+      }
+      const int t = src[r];
+      src[r] = src[qp];
+      src[qp] = t;
+    }
+    s_cnt = cnt;
+  }
   __syncthreads();
   const int j = chunk * kTrsmCols + threadIdx.x;
   if (j >= m || (j >= k0 && j < k0 + nb)) return;
-  for (int r = 0; r < nb; ++r) {
-    const int p = spiv[r];
-    if (p != k0 + r) {
-      double* x = A + static_cast<size_t>(k0 + r) * m + j;
-      double* y = A + static_cast<size_t>(p) * m + j;
-      const double t = *x;
-      *x = *y;
-      *y = t;
-    }
-  }
-  if (j < k0 + nb) return;
+  if (!swaps && j < k0) return;
+  const int cnt = s_cnt;
+  // Gather every touched row's new value (all loads first), then store.
+  double nv[2 * kPanel];
+#pragma unroll
+  for (int q = 0; q < 2 * kPanel; ++q)
+    if (q < cnt) nv[q] = A[static_cast<size_t>(rows[src[q]]) * m + j];
+#pragma unroll
+  for (int q = kPanel; q < 2 * kPanel; ++q)
+    if (q < cnt) A[static_cast<size_t>(rows[q]) * m + j] = nv[q];
   double x[kPanel];
 #pragma unroll
-  for (int r = 0; r < kPanel; ++r) x[r] = (r < nb) ? A[static_cast<size_t>(k0 + r) * m + j] : 0.0;
+  for (int r = 0; r < kPanel; ++r) x[r] = (r < nb) ? nv[r] : 0.0;
+  if (j < k0 + nb) {
+#pragma unroll
+    for (int r = 0; r < kPanel; ++r)
+      if (r < nb) A[static_cast<size_t>(k0 + r) * m + j] = x[r];
+    return;
+  }
 #pragma unroll
   for (int r = 1; r < kPanel; ++r) {
     double v = x[r];
@@ -284,12 +335,16 @@ __global__ void __launch_bounds__(kTrsmCols) k_swap_trsm_rm(DevPlan dp, int32_t 
     if (r < nb) A[static_cast<size_t>(k0 + r) * m + j] = x[r];
 }
 
-// A22 -= L21 * U12 on row-major storage; the panel depth is staged in two
-// halves of kKC columns.
-constexpr int kKC = 16;
+// A22 -= L21 * U12 on row-major storage, the whole panel depth staged in
+// shared memory.  All loads of the C tile precede its stores (a store may
+// alias a later load, which would serialise the round trips).
+constexpr int kAStride = kPanel + 1;   // As[i][q]
+constexpr int kBStride = kGT + 4;      // Bs[q][j]
+constexpr size_t kGemmSmem = (static_cast<size_t>(kGT) * kAStride + static_cast<size_t>(kPanel) * kBStride) * sizeof(double);
 __global__ void __launch_bounds__(kGThreads, 1) k_gemm_rm(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
-  __shared__ double As[kKC][kGT + 1];
-  __shared__ double Bs[kKC][kGT];
+  extern __shared__ double gsm[];
+  double* As = gsm;
+  double* Bs = gsm + kGT * kAStride;
   int a = 0;
   while (a + 1 < nact && dp.step_gemm_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
   const int u = dp.step_unit[ubase + a];
@@ -305,34 +360,41 @@ __global__ void __launch_bounds__(kGThreads, 1) k_gemm_rm(DevPlan dp, int32_t k0
   double* A = dp.lu + dp.lu_off[u];
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
+  for (int t = tid; t < kGT * kPanel; t += kGThreads) {
+    const int i = t / kPanel, q = t - i * kPanel;
+    As[i * kAStride + q] = (q < nb && i0 + i < m) ? A[static_cast<size_t>(i0 + i) * m + k0 + q] : 0.0;
+  }
+  for (int t = tid; t < kPanel * kGT; t += kGThreads) {
+    const int q = t / kGT, jj = t - q * kGT;
+    Bs[q * kBStride + jj] = (q < nb && j0 + jj < m) ? A[static_cast<size_t>(k0 + q) * m + j0 + jj] : 0.0;
+  }
+  __syncthreads();
   double acc[8][8];
 #pragma unroll
   for (int x = 0; x < 8; ++x)
 #pragma unroll
     for (int y = 0; y < 8; ++y) acc[x][y] = 0.0;
-  for (int h = 0; h < kPanel; h += kKC) {
-    for (int t = tid; t < kGT * kKC; t += kGThreads) {
-      const int i = t / kKC, q = t - i * kKC;
-      As[q][i] = (h + q < nb && i0 + i < m) ? A[static_cast<size_t>(i0 + i) * m + k0 + h + q] : 0.0;
-    }
-    for (int t = tid; t < kKC * kGT; t += kGThreads) {
-      const int q = t / kGT, jj = t - q * kGT;
-      Bs[q][jj] = (h + q < nb && j0 + jj < m) ? A[static_cast<size_t>(k0 + h + q) * m + j0 + jj] : 0.0;
-    }
-    __syncthreads();
 #pragma unroll 4
-    for (int q = 0; q < kKC; ++q) {
-      double av[8], bv[8];
+  for (int q = 0; q < kPanel; ++q) {
+    double av[8], bv[8];
 #pragma unroll
-      for (int x = 0; x < 8; ++x) av[x] = As[q][ty + 16 * x];
+    for (int x = 0; x < 8; ++x) av[x] = As[(ty + 16 * x) * kAStride + q];
 #pragma unroll
-      for (int y = 0; y < 8; ++y) bv[y] = Bs[q][tx + 16 * y];
+    for (int y = 0; y < 8; ++y) bv[y] = Bs[q * kBStride + tx + 16 * y];
 #pragma unroll
-      for (int x = 0; x < 8; ++x)
+    for (int x = 0; x < 8; ++x)
 #pragma unroll
-        for (int y = 0; y < 8; ++y) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
+      for (int y = 0; y < 8; ++y) acc[x][y] = fma(av[x], bv[y], acc[x][y]);
+  }
+#pragma unroll
+  for (int x = 0; x < 8; ++x) {
+    const int i = i0 + ty + 16 * x;
+    const double* row = A + static_cast<size_t>(min(i, m - 1)) * m;
+#pragma unroll
+    for (int y = 0; y < 8; ++y) {
+      const int j = j0 + tx + 16 * y;
+      acc[x][y] = (i < m && j < m) ? row[j] - acc[x][y] : 0.0;
     }
-    __syncthreads();
   }
 #pragma unroll
   for (int x = 0; x < 8; ++x) {
@@ -342,27 +404,129 @@ __global__ void __launch_bounds__(kGThreads, 1) k_gemm_rm(DevPlan dp, int32_t k0
 #pragma unroll
     for (int y = 0; y < 8; ++y) {
       const int j = j0 + tx + 16 * y;
-      if (j < m) row[j] -= acc[x][y];
+      if (j < m) row[j] = acc[x][y];
     }
   }
 }
 
-// Final row order of each large unit: row k of its factor is local row perm[k].
-__global__ void k_large_perm(DevPlan dp, const int32_t* __restrict__ units, int32_t count) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= count) return;
-  const int u = units[t];
+// Final row order of each large unit and its inverse: row k of the factor is
+// local row perm[k], local row r sits at iperm[r].  The sequential swaps run
+// on a shared-memory copy (one CTA per unit).
+__global__ void k_large_perm(DevPlan dp, const int32_t* __restrict__ units) {
+  extern __shared__ int32_t ord[];
+  const int u = units[blockIdx.x];
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
-  int32_t* perm = dp.lperm + s;
-  for (int k = 0; k < m; ++k) perm[k] = k;
-  for (int k = 0; k < m; ++k) {
-    const int p = dp.piv[s + k];
-    if (p != k) {
-      const int32_t tmp = perm[k];
-      perm[k] = perm[p];
-      perm[p] = tmp;
+  for (int k = threadIdx.x; k < m; k += blockDim.x) ord[k] = k;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < m; ++k) {
+      const int p = dp.piv[s + k];
+      if (p != k) {
+        const int32_t tmp = ord[k];
+        ord[k] = ord[p];
+        ord[p] = tmp;
+      }
     }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < m; k += blockDim.x) {
+    dp.lperm[s + k] = ord[k];
+    dp.liperm[s + ord[k]] = k;
+  }
+}
+
+// Value scatter of large units into their slots with rows already in the
+// stored pivot order (refactor with the previous pivot sequence).
+__global__ void k_scatter_large_perm(DevPlan dp, const double* __restrict__ vals, const int32_t* __restrict__ units) {
+  const int u = units[blockIdx.y];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  double* A = dp.lu + dp.lu_off[u];
+  for (int64_t e = dp.dent_ptr[u] + blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; e < dp.dent_ptr[u + 1];
+       e += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int pos = dp.dent_pos[e];
+    const int r = pos / m, c = pos - (pos / m) * m;
+    A[static_cast<size_t>(dp.liperm[s + r]) * m + c] = vals[dp.dent_src[e]];
+  }
+}
+
+// Diagonal block of a step without pivot search (rows already in pivot
+// order): unblocked LU of the nb x nb block in shared memory.  A zero or
+// non-finite pivot marks the unit for a factorisation with pivoting
+// (status 2).
+__global__ void __launch_bounds__(256) k_diag_nopiv(DevPlan dp, int32_t k0, int32_t ubase) {
+  __shared__ double D[kPanel][kPanel + 1];
+  __shared__ int s_bad;
+  const int u = dp.step_unit[ubase + blockIdx.x];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kPanel, m - k0);
+  double* A = dp.lu + dp.lu_off[u];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    const int r = t / nb, c = t - r * nb;
+    D[r][c] = A[static_cast<size_t>(k0 + r) * m + k0 + c];
+  }
+  if (threadIdx.x == 0) s_bad = 0;
+  __syncthreads();
+  for (int k = 0; k < nb; ++k) {
+    const double d = D[k][k];
+    if (!(fabs(d) > 0.0) || !isfinite(d)) {
+      if (threadIdx.x == 0) s_bad = 1;
+      break;
+    }
+    const double dinv = 1.0 / d;
+    const int r = threadIdx.x / kPanel, c = threadIdx.x - (threadIdx.x / kPanel) * kPanel;
+    // 256 threads: 8 rows x 32 columns per pass.
+    for (int i = k + 1 + r; i < nb; i += 8) {
+      const double l = D[i][k] * dinv;
+      if (c > k && c < nb) D[i][c] = fma(-l, D[k][c], D[i][c]);
+      __syncwarp();
+      if (c == k) D[i][k] = l;
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  if (s_bad) {
+    if (threadIdx.x == 0 && atomicCAS(dp.status, 0, 2) == 0) dp.status[1] = u;
+    return;
+  }
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    const int r = t / nb, c = t - r * nb;
+    A[static_cast<size_t>(k0 + r) * m + k0 + c] = D[r][c];
+  }
+}
+
+// L21 = A21 * U11^{-1} for the rows below the diagonal block, one warp per
+// row: lane c holds column c of the row.
+constexpr int kTrslRowsPerCta = 16;
+__global__ void __launch_bounds__(512) k_trsm_l(DevPlan dp, int32_t k0, int32_t ubase) {
+  __shared__ double Ut[kPanel][kPanel + 1];
+  __shared__ double rinv[kPanel];
+  const int u = dp.step_unit[ubase + blockIdx.y];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kPanel, m - k0);
+  const int base = k0 + nb;
+  const int row0 = base + blockIdx.x * kTrslRowsPerCta * 2;
+  if (row0 >= m) return;
+  double* A = dp.lu + dp.lu_off[u];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
+    const int r = t / nb, c = t - r * nb;
+    Ut[r][c] = A[static_cast<size_t>(k0 + r) * m + k0 + c];
+  }
+  if (threadIdx.x < nb) rinv[threadIdx.x] = 1.0 / A[static_cast<size_t>(k0 + threadIdx.x) * m + k0 + threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int i = row0 + warp; i < min(m, row0 + kTrslRowsPerCta * 2); i += 16) {
+    double* row = A + static_cast<size_t>(i) * m + k0;
+    double x = (lane < nb) ? row[lane] : 0.0;
+    for (int q = 0; q < nb; ++q) {
+      const double lq = __shfl_sync(0xffffffffu, x, q) * rinv[q];
+      if (lane > q) x = fma(-lq, Ut[q][lane], x);
+      else if (lane == q) x = lq;
+    }
+    if (lane < nb) row[lane] = x;
   }
 }
 
@@ -536,7 +700,9 @@ cudaError_t large_setup() {
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    err = cudaFuncSetAttribute(k_panel_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 8 * 1024);
+    err = cudaFuncSetAttribute(k_gemm_rm, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kGemmSmem));
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_large_perm, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 4 * 1024);
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_large_single, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (kTile * kTile + kLargeSingleMax) * static_cast<int>(sizeof(double)));
@@ -544,8 +710,8 @@ cudaError_t large_setup() {
   return err;
 }
 
-cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, cudaStream_t stream,
-                         int32_t* launches) {
+cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, bool reuse,
+                         cudaStream_t stream, int32_t* launches) {
   cudaError_t e = large_setup();
   if (e != cudaSuccess) return e;
   for (int32_t st = 0; st < p.nsteps; ++st) {
@@ -554,13 +720,32 @@ cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_larg
     if (na <= 0) continue;
     const int32_t k0 = st * kPanel;
     const int32_t rows = p.step_max_rows[static_cast<size_t>(st)];
+    if (reuse) {
+      // Rows are already in the stored pivot order: diagonal block, L21,
+      // U12 and the update, all without pivot search.
+      k_diag_nopiv<<<na, 256, 0, stream>>>(dp, k0, ub);
+      const int rows_below = rows - std::min(kPanel, rows);
+      if (rows_below > 0) {
+        const unsigned gx = static_cast<unsigned>((rows_below + 2 * kTrslRowsPerCta - 1) / (2 * kTrslRowsPerCta));
+        k_trsm_l<<<dim3(gx, static_cast<unsigned>(na)), 512, 0, stream>>>(dp, k0, ub);
+        ++*launches;
+      }
+      k_swap_trsm_rm<<<p.step_trsm_total[static_cast<size_t>(st)], kTrsmCols, 0, stream>>>(dp, k0, ub, na, 0);
+      *launches += 2;
+      if (p.step_gemm_total[static_cast<size_t>(st)] > 0) {
+        k_gemm_rm<<<p.step_gemm_total[static_cast<size_t>(st)], kGThreads, kGemmSmem, stream>>>(dp, k0, ub, na);
+        ++*launches;
+      }
+      continue;
+    }
     const int csize = cluster_size_for(rows);
     if (csize <= kClusterMaxCtas) {
       const int chunk = (rows + csize - 1) / csize;
+      (void)chunk;
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3(static_cast<unsigned>(na * csize));
-      cfg.blockDim = dim3(kPT);
-      cfg.dynamicSmemBytes = static_cast<size_t>(chunk) * kPStride * sizeof(double);
+      cfg.blockDim = dim3(kPanelThreads);
+      cfg.dynamicSmemBytes = 0;
       cfg.stream = stream;
       cudaLaunchAttribute attr[1];
       attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -574,18 +759,27 @@ cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_larg
     } else {
       k_panel_global<<<na, kPT, 0, stream>>>(dp, k0, ub);
     }
-    k_swap_trsm_rm<<<p.step_trsm_total[static_cast<size_t>(st)], kTrsmCols, 0, stream>>>(dp, k0, ub, na);
+    k_swap_trsm_rm<<<p.step_trsm_total[static_cast<size_t>(st)], kTrsmCols, 0, stream>>>(dp, k0, ub, na, 1);
     *launches += 2;
     if (p.step_gemm_total[static_cast<size_t>(st)] > 0) {
-      k_gemm_rm<<<p.step_gemm_total[static_cast<size_t>(st)], kGThreads, 0, stream>>>(dp, k0, ub, na);
+      k_gemm_rm<<<p.step_gemm_total[static_cast<size_t>(st)], kGThreads, kGemmSmem, stream>>>(dp, k0, ub, na);
       ++*launches;
     }
   }
   const int nl = static_cast<int>(p.large_units.size());
-  if (nl > 0) {
-    k_large_perm<<<(nl + 127) / 128, 128, 0, stream>>>(dp, d_large_units, nl);
+  if (nl > 0 && !reuse) {
+    int32_t mmax = 0;
+    for (int32_t u : p.large_units) mmax = std::max(mmax, p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)]);
+    k_large_perm<<<nl, 256, static_cast<size_t>(mmax) * sizeof(int32_t), stream>>>(dp, d_large_units);
     ++*launches;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t large_scatter_reuse(const DevPlan& dp, const Plan& p, const double* d_vals, const int32_t* d_large_units,
+                                cudaStream_t stream) {
+  if (p.large_units.empty()) return cudaSuccess;
+  k_scatter_large_perm<<<dim3(64, static_cast<unsigned>(p.large_units.size())), 256, 0, stream>>>(dp, d_vals, d_large_units);
   return cudaGetLastError();
 }
 

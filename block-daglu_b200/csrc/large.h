@@ -13,9 +13,17 @@ namespace bdlu {
 cudaError_t large_setup();
 
 // Enqueues the blocked LU of every large unit (slots already hold the unit
-// values, row-major) and the final row orders.
-cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, cudaStream_t stream,
-                         int32_t* launches);
+// values, row-major).  reuse = false: partial pivoting, then the final row
+// orders (lperm/liperm).  reuse = true: the slots were filled by
+// large_scatter_reuse in the stored row order and no pivot search is made; a
+// zero or non-finite pivot sets status code 2.
+cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, bool reuse,
+                         cudaStream_t stream, int32_t* launches);
+
+// Scatters the values of all large units into their (zeroed) slots with the
+// rows in the stored pivot order.
+cudaError_t large_scatter_reuse(const DevPlan& dp, const Plan& p, const double* d_vals, const int32_t* d_large_units,
+                                cudaStream_t stream);
 
 // Enqueues the solve of the large units of one level (d_units / h_units: the
 // level's list, single-CTA units first).  xp is the permuted solution.

@@ -143,6 +143,11 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  *   "refine_iters": number of FP64 iterative-refinement steps (r = b - Ax,
  *     solve, x += d) after each solve; default is the reference's REFINE_ITERS
  *     environment value, else 0 (solver.cpp:1449-1465).
+ *   "refactor_pivoting": 0 (default) lets a value-only refactor keep the pivot
+ *     order of the last full factorisation for blocks factored across CTAs
+ *     (KLU's klu_refactor reuses the pivot order the same way); a zero pivot,
+ *     or a host-buffer solve whose residual exceeds 1e-12, triggers a
+ *     factorisation with partial pivoting.  1 pivots on every refactor.
  *   "analysis_only": 1 makes analyze stop after the host analysis (no device
  *     upload); factor then reports BDLU_BACKEND_UNAVAILABLE.  For structure
  *     inspection on machines without a GPU.

@@ -263,3 +263,44 @@ def test_global_route_tall_unit_fallback_panel(monkeypatch):
     x = g.b[:, 0].copy()
     assert s.solve_in_place(x)
     assert _inf_resid(g, g.vals, x, g.b[:, 0]) <= RESID_TOL
+
+
+def test_refactor_reusing_pivot_order_matches_pivoting_refactor(monkeypatch):
+    # MODE=klu: one 2000-row block factored across CTAs.  A value-only refactor
+    # keeps the block's pivot order (klu_refactor semantics); the result must
+    # agree with a refactor that pivots again.
+    monkeypatch.setenv("BLOCKDAGLU_MODE", "klu")
+    g = bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(0, 21), 2000, 40)
+    s1, s2 = bd.Solver(), bd.Solver()
+    for s, piv in ((s1, 0), (s2, 1)):
+        assert s.set_option("refactor_pivoting", piv)
+        assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze() and s.factor(), s.last_error_message()
+    for k in range(3):
+        v = g.perturbed(300 + k)
+        b = multiply(list(zip(g.rows, g.cols, v)), g.n, g.x_true[:, 0])
+        xs = []
+        for s in (s1, s2):
+            assert s.refactor_values(v), s.last_error_message()
+            x = b.copy()
+            assert s.solve_in_place(x), s.last_error_message()
+            assert _inf_resid(g, v, x, b) <= RESID_TOL
+            xs.append(x)
+        assert close_vec(xs[0], xs[1], 1e-8)
+
+
+def test_refactor_reused_zero_pivot_falls_back_to_pivoting(monkeypatch):
+    monkeypatch.setenv("BLOCKDAGLU_MODE", "klu")
+    g = bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(0, 22), 400, 1)
+    s = bd.Solver()
+    assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze() and s.factor(), s.last_error_message()
+    first_row = s.getP()[0][1]      # original row chosen as the first pivot
+    v = g.vals.copy()
+    hit = np.nonzero((g.rows == first_row) & (g.cols == 0))[0]
+    assert len(hit) == 1
+    v[hit[0]] = 0.0                 # the reused first pivot is now exactly zero
+    assert s.refactor_values(v), s.last_error_message()
+    assert s.getP()[0][1] != first_row
+    b = multiply(list(zip(g.rows, g.cols, v)), g.n, g.x_true[:, 0])
+    x = b.copy()
+    assert s.solve_in_place(x)
+    assert _inf_resid(g, v, x, b) <= RESID_TOL
