@@ -160,10 +160,27 @@ __global__ void k_solve_scalar(DevPlan dp, const int32_t* __restrict__ rows, int
   }
 }
 
+// Small dense units (column-major LU): the right-hand sides of up to
+// kSolveRhsChunk columns are formed together; each triangle is staged in
+// shared memory (packed by columns), and each warp sweeps one right-hand side
+// with the column's values in registers (kSlots per lane), broadcasting each
+// finished unknown with a shuffle, so a sweep step costs no CTA barrier.
+constexpr int kSolveRhsChunk = 16;
+constexpr int kSlots = 6;  // rows per lane: units up to 192 rows
+static_assert(32 * kSlots >= 169, "register slots must cover the shared-memory LU limit");
+
+__device__ __forceinline__ double slot_get(const double (&a)[kSlots], int k) {
+  double v = a[0];
+#pragma unroll
+  for (int t = 1; t < kSlots; ++t)
+    if (k == t) v = a[t];
+  return v;
+}
+
 __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int32_t* __restrict__ units,
                                                            const double* __restrict__ rhs, int32_t ldr,
                                                            double* __restrict__ xp, int32_t nrhs) {
-  extern __shared__ double x[];
+  extern __shared__ double sm[];
   const int u = units[blockIdx.x];
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
@@ -171,45 +188,91 @@ __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int3
   const double* LU = dp.lu + dp.lu_off[u];
   const int32_t* piv = dp.piv + s;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int k = 0; k < nrhs; ++k) {
-    const double* xk = xp + static_cast<size_t>(k) * n;
-    for (int i = warp; i < m; i += kThreads / 32) {
+  constexpr int kWarps = kThreads / 32;
+  double* T = sm;                              // packed triangle, m*(m+1)/2
+  double* X = sm + (m * (m + 1)) / 2;          // X[i * kSolveRhsChunk + c]
+  for (int k0 = 0; k0 < nrhs; k0 += kSolveRhsChunk) {
+    const int nc = min(kSolveRhsChunk, nrhs - k0);
+    for (int i = warp; i < m; i += kWarps) {
       const int r = s + i;
-      double acc = 0.0;
-      for (int q = dp.cpl_ptr[r] + lane; q < dp.cpl_ptr[r + 1]; q += 32) acc = fma(dp.cpl_val[q], xk[dp.cpl_col[q]], acc);
-      acc = warp_sum(acc);
-      if (lane == 0) x[i] = rhs[dp.P[r] + static_cast<size_t>(k) * ldr] - acc;
+      const int p0 = dp.cpl_ptr[r], p1 = dp.cpl_ptr[r + 1];
+      for (int c = 0; c < nc; ++c) {
+        const double* xk = xp + static_cast<size_t>(k0 + c) * n;
+        double acc = 0.0;
+        for (int q = p0 + lane; q < p1; q += 32) acc = fma(dp.cpl_val[q], xk[dp.cpl_col[q]], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) X[i * kSolveRhsChunk + c] = rhs[dp.P[r] + static_cast<size_t>(k0 + c) * ldr] - acc;
+      }
+    }
+    // Strictly lower part of L, packed by columns: column j at j*(m-1) - j*(j-1)/2.
+    for (int j = warp; j < m - 1; j += kWarps) {
+      const int off = j * (m - 1) - (j * (j - 1)) / 2;
+      for (int i = j + 1 + lane; i < m; i += 32) T[off + i - j - 1] = LU[static_cast<size_t>(j) * m + i];
     }
     __syncthreads();
-    if (tid == 0) {
+    if (tid < nc) {
       for (int i = 0; i < m; ++i) {
         const int p = piv[i];
         if (p != i) {
-          const double t = x[i];
-          x[i] = x[p];
-          x[p] = t;
+          const double t = X[i * kSolveRhsChunk + tid];
+          X[i * kSolveRhsChunk + tid] = X[p * kSolveRhsChunk + tid];
+          X[p * kSolveRhsChunk + tid] = t;
         }
       }
     }
     __syncthreads();
-    // Forward solve with unit-lower L (column oriented).
-    for (int j = 0; j < m - 1; ++j) {
-      const double xj = x[j];
-      const double* lc = LU + static_cast<size_t>(j) * m;
-      for (int i = j + 1 + tid; i < m; i += kThreads) x[i] = fma(-lc[i], xj, x[i]);
-      __syncthreads();
+    for (int c = warp; c < nc; c += kWarps) {
+      double a[kSlots];
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        const int i = lane + 32 * k;
+        a[k] = (i < m) ? X[i * kSolveRhsChunk + c] : 0.0;
+      }
+      for (int j = 0; j < m - 1; ++j) {
+        const double xr = __shfl_sync(0xffffffffu, slot_get(a, j >> 5), j & 31);
+        const int base = j * (m - 1) - (j * (j - 1)) / 2 - j - 1;
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) {
+          const int i = lane + 32 * k;
+          if (i > j && i < m) a[k] = fma(-T[base + i], xr, a[k]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        const int i = lane + 32 * k;
+        if (i < m) X[i * kSolveRhsChunk + c] = a[k];
+      }
     }
-    // Backward solve with U.
-    for (int j = m - 1; j >= 0; --j) {
-      const double* uc = LU + static_cast<size_t>(j) * m;
-      const double xj = x[j] / uc[j];
-      for (int i = tid; i < j; i += kThreads) x[i] = fma(-uc[i], xj, x[i]);
-      __syncthreads();
-      if (tid == 0) x[j] = xj;
-      __syncthreads();
+    __syncthreads();
+    // Upper part of U with the diagonal, packed by columns: column j at j*(j+1)/2.
+    for (int j = warp; j < m; j += kWarps) {
+      const int off = (j * (j + 1)) / 2;
+      for (int i = lane; i <= j; i += 32) T[off + i] = LU[static_cast<size_t>(j) * m + i];
     }
-    double* xo = xp + static_cast<size_t>(k) * n + s;
-    for (int i = tid; i < m; i += kThreads) xo[i] = x[i];
+    __syncthreads();
+    for (int c = warp; c < nc; c += kWarps) {
+      double a[kSlots];
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        const int i = lane + 32 * k;
+        a[k] = (i < m) ? X[i * kSolveRhsChunk + c] : 0.0;
+      }
+      for (int j = m - 1; j >= 0; --j) {
+        const int off = (j * (j + 1)) / 2;
+        const double xr = __shfl_sync(0xffffffffu, slot_get(a, j >> 5), j & 31) / T[off + j];
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) {
+          const int i = lane + 32 * k;
+          if (i == j) a[k] = xr;
+          else if (i < j) a[k] = fma(-T[off + i], xr, a[k]);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kSlots; ++k) {
+        const int i = lane + 32 * k;
+        if (i < m) xp[static_cast<size_t>(k0 + c) * n + s + i] = a[k];
+      }
+    }
     __syncthreads();
   }
 }
@@ -282,6 +345,7 @@ int32_t small_unit_max() {
 }
 
 Engine::Engine() {
+  cudaStreamCreateWithFlags(&cap_stream_, cudaStreamNonBlocking);
   for (auto& e : ev_) cudaEventCreate(&e);
   for (auto& e : pev_) cudaEventCreate(&e);
   int dev = 0;
@@ -291,13 +355,24 @@ Engine::Engine() {
 
 Engine::~Engine() {
   release();
+  if (cap_stream_) cudaStreamDestroy(cap_stream_);
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
   for (auto& e : pev_)
     if (e) cudaEventDestroy(e);
 }
 
+void Engine::drop_graphs() {
+  if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
+  if (reuse_exec_) cudaGraphExecDestroy(reuse_exec_);
+  solve_exec_ = nullptr;
+  reuse_exec_ = nullptr;
+  solve_exec_nrhs_ = 0;
+  solve_exec_b0_ = nullptr;
+}
+
 void Engine::release() {
+  drop_graphs();
   for (void* p : allocs_) cudaFree(p);
   allocs_.clear();
   d_vals_ = nullptr;
@@ -378,7 +453,8 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   int32_t small_m = 0;
   for (int32_t u : plan.small_units) small_m = std::max(small_m, plan.ustart[static_cast<size_t>(u) + 1] - plan.ustart[static_cast<size_t>(u)]);
   smem_small_ = static_cast<size_t>(small_m) * small_m * sizeof(double);
-  smem_solve_ = static_cast<size_t>(std::max<int32_t>(small_m, 1)) * sizeof(double);
+  smem_solve_ = (static_cast<size_t>(small_m) * (small_m + 1) / 2 + static_cast<size_t>(small_m) * kSolveRhsChunk) *
+                sizeof(double);
   {
     // The dynamic shared-memory limit is a per-function process-wide
     // attribute; raise it once to the device maximum so handles of different
@@ -396,6 +472,8 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
     });
     BDLU_CUDA(attr_err);
   }
+  // Kernel attributes are set before any stream capture can start.
+  BDLU_CUDA(large_setup());
   // Kernel work lists.
   const int32_t* small_list = nullptr;
   const int32_t* large_list = nullptr;
@@ -428,7 +506,30 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   if (!p.small_units.empty())
     k_lu_small<<<static_cast<int>(p.small_units.size()), kThreads, smem_small_, stream>>>(dp_, d_vals, small_list_);
   BDLU_CUDA(cudaEventRecord(pev_[1], stream));
-  if (!p.large_units.empty()) {
+  if (!p.large_units.empty() && reuse) {
+    if (!reuse_exec_ || d_vals != d_vals_) {
+      if (d_vals != d_vals_) {
+        err = "refactor with the stored pivot order reads the engine's value buffer";
+        return false;
+      }
+      BDLU_CUDA(cudaStreamBeginCapture(cap_stream_, cudaStreamCaptureModeThreadLocal));
+      int32_t n_launch = 0;
+      cudaMemsetAsync(dp_.lu + p.lu_large_begin, 0,
+                      static_cast<size_t>(p.lu_large_end - p.lu_large_begin) * sizeof(double), cap_stream_);
+      cudaError_t ce = large_scatter_reuse(dp_, p, d_vals, large_list_, cap_stream_);
+      if (ce == cudaSuccess) ce = large_factor(dp_, p, large_list_, true, cap_stream_, &n_launch);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ee = cudaStreamEndCapture(cap_stream_, &g);
+      BDLU_CUDA(ce);
+      BDLU_CUDA(ee);
+      const cudaError_t ie = cudaGraphInstantiate(&reuse_exec_, g, 0);
+      cudaGraphDestroy(g);
+      BDLU_CUDA(ie);
+      reuse_launches_ = n_launch + 1;
+    }
+    BDLU_CUDA(cudaGraphLaunch(reuse_exec_, stream));
+    launches_factor_ += reuse_launches_;
+  } else if (!p.large_units.empty()) {
     BDLU_CUDA(cudaMemsetAsync(dp_.lu + p.lu_large_begin, 0,
                               static_cast<size_t>(p.lu_large_end - p.lu_large_begin) * sizeof(double), stream));
     if (reuse) {
@@ -520,7 +621,24 @@ bool Engine::solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_
   BDLU_CUDA(cudaMemcpy2DAsync(d_b0_, static_cast<size_t>(n) * sizeof(double), d_B,
                               static_cast<size_t>(ldb) * sizeof(double), static_cast<size_t>(n) * sizeof(double),
                               static_cast<size_t>(nrhs), cudaMemcpyDeviceToDevice, stream));
-  solve_core(d_b0_, n, d_xp_, nrhs, stream);
+  if (!solve_exec_ || solve_exec_nrhs_ != nrhs || solve_exec_b0_ != d_b0_) {
+    if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
+    solve_exec_ = nullptr;
+    const int32_t saved = launches_solve_;
+    BDLU_CUDA(cudaStreamBeginCapture(cap_stream_, cudaStreamCaptureModeThreadLocal));
+    solve_core(d_b0_, n, d_xp_, nrhs, cap_stream_);
+    cudaGraph_t g = nullptr;
+    BDLU_CUDA(cudaStreamEndCapture(cap_stream_, &g));
+    const cudaError_t ie = cudaGraphInstantiate(&solve_exec_, g, 0);
+    cudaGraphDestroy(g);
+    BDLU_CUDA(ie);
+    solve_core_launches_ = launches_solve_ - saved;
+    launches_solve_ = saved;
+    solve_exec_nrhs_ = nrhs;
+    solve_exec_b0_ = d_b0_;
+  }
+  BDLU_CUDA(cudaGraphLaunch(solve_exec_, stream));
+  launches_solve_ += solve_core_launches_;
   const int ug = grid_for(static_cast<int64_t>(n) * nrhs, kThreads, num_sms_ * 16);
   k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 0);
   BDLU_CUDA(cudaEventRecord(pev_[2], stream));

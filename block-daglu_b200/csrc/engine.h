@@ -128,6 +128,18 @@ class Engine {
   size_t smem_small_ = 0;
   size_t smem_solve_ = 0;
   int num_sms_ = 148;
+  // CUDA graphs of the launch sequences that repeat unchanged: the solve
+  // sweep (per nrhs and work buffers) and the refactor of large units with
+  // the stored pivot order.  Captured on cap_stream_, launched on the
+  // caller's stream.
+  cudaStream_t cap_stream_ = nullptr;
+  cudaGraphExec_t solve_exec_ = nullptr;
+  int32_t solve_exec_nrhs_ = 0;
+  const double* solve_exec_b0_ = nullptr;
+  cudaGraphExec_t reuse_exec_ = nullptr;
+  int32_t reuse_launches_ = 0;
+  int32_t solve_core_launches_ = 0;
+  void drop_graphs();
   bool have_pivots_ = false;  // a full factorisation of this pattern succeeded
   bool last_reuse_ = false;
 

@@ -65,6 +65,7 @@ constexpr int kPanelRowsMax = 640;        // panel rows one CTA holds (one per t
 constexpr int kGT = 128;                  // GEMM output tile
 constexpr int kGThreads = 256;
 constexpr int kTile = 64;                 // solve tile
+constexpr int kTS = kTile + 1;            // shared-memory row stride of a staged tile
 constexpr int kSolveThreads = 256;
 
 // ---------------------------------------------------------------------------
@@ -553,33 +554,56 @@ __global__ void __launch_bounds__(kSolveThreads) k_large_rhs(DevPlan dp, const i
   }
 }
 
-// 64 x 64 triangle of tile `t0` (rows/cols t0..t0+w) solved in place on x.
-// Warp-level, the tile staged in shared memory.  lower: unit-lower forward;
-// else upper backward with division by the diagonal.
+// acc_r = sum_q row_r[q] * x[q] over q in [q0, q1) for 4 rows at once (more
+// loads in flight per warp); rows past `rows` contribute nothing.
+__device__ __forceinline__ void gemv4(const double* LU, int m, int i0, int rows, int q0, int q1, const double* x,
+                                      int lane, double acc[4]) {
+  acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
+  const double* r0 = LU + static_cast<size_t>(i0) * m;
+#pragma unroll 4
+  for (int q = q0 + lane; q < q1; q += 32) {
+    const double xq = x[q];
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+      if (t < rows) acc[t] = fma(__ldg(r0 + static_cast<size_t>(t) * m + q), xq, acc[t]);
+  }
+#pragma unroll
+  for (int t = 0; t < 4; ++t) acc[t] = warp_sum(acc[t]);
+}
+
+// 64 x 64 triangle of tile `t0` (rows/cols t0..t0+w) solved in place on x
+// (shared or global memory).  The tile is staged in shared memory; warp 0
+// keeps the 64 unknowns in registers (two per lane) and broadcasts each
+// finished one with a shuffle.  lower: unit-lower forward sweep; else upper
+// backward sweep with division by the diagonal.
 __device__ void tile_triangle(const double* LU, int m, int t0, int w, double* x, double* Ts, bool lower) {
   for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
     const int i = t / w, c = t - i * w;
-    Ts[i * kTile + c] = LU[static_cast<size_t>(t0 + i) * m + t0 + c];
+    Ts[i * kTS + c] = LU[static_cast<size_t>(t0 + i) * m + t0 + c];
   }
   __syncthreads();
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
+    double a = (lane < w) ? x[t0 + lane] : 0.0;
+    double b = (lane + 32 < w) ? x[t0 + 32 + lane] : 0.0;
     if (lower) {
       for (int r = 0; r < w; ++r) {
-        const double xr = x[t0 + r];
-        __syncwarp();
-        for (int i = r + 1 + lane; i < w; i += 32) x[t0 + i] = fma(-Ts[i * kTile + r], xr, x[t0 + i]);
-        __syncwarp();
+        const double xr = __shfl_sync(0xffffffffu, r < 32 ? a : b, r & 31);
+        if (lane > r && lane < w) a = fma(-Ts[lane * kTS + r], xr, a);
+        if (lane + 32 > r && lane + 32 < w) b = fma(-Ts[(lane + 32) * kTS + r], xr, b);
       }
     } else {
       for (int r = w - 1; r >= 0; --r) {
-        const double xr = x[t0 + r] / Ts[r * kTile + r];
-        __syncwarp();
-        if (lane == 0) x[t0 + r] = xr;
-        for (int i = lane; i < r; i += 32) x[t0 + i] = fma(-Ts[i * kTile + r], xr, x[t0 + i]);
-        __syncwarp();
+        const double d = Ts[r * kTS + r];
+        const double xr = __shfl_sync(0xffffffffu, r < 32 ? a : b, r & 31) / d;
+        if (lane == r) a = xr;
+        if (lane + 32 == r) b = xr;
+        if (lane < r) a = fma(-Ts[lane * kTS + r], xr, a);
+        if (lane + 32 < r) b = fma(-Ts[(lane + 32) * kTS + r], xr, b);
       }
     }
+    if (lane < w) x[t0 + lane] = a;
+    if (lane + 32 < w) x[t0 + 32 + lane] = b;
   }
   __syncthreads();
 }
@@ -588,8 +612,8 @@ __device__ void tile_triangle(const double* LU, int m, int t0, int w, double* x,
 __global__ void __launch_bounds__(kSolveThreads) k_large_single(DevPlan dp, const int32_t* __restrict__ units,
                                                                 double* __restrict__ xp, int32_t nrhs) {
   extern __shared__ double sm[];
-  double* Ts = sm;                  // kTile * kTile
-  double* x = sm + kTile * kTile;   // m
+  double* Ts = sm;                // kTile * kTS
+  double* x = sm + kTile * kTS;   // m
   const int u = units[blockIdx.x];
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
@@ -603,24 +627,22 @@ __global__ void __launch_bounds__(kSolveThreads) k_large_single(DevPlan dp, cons
     __syncthreads();
     for (int I = 0; I < nt; ++I) {
       const int t0 = I * kTile, w = min(kTile, m - t0);
-      for (int i = t0 + warp; i < t0 + w; i += nw) {
-        const double* row = LU + static_cast<size_t>(i) * m;
-        double acc = 0.0;
-        for (int q = lane; q < t0; q += 32) acc = fma(row[q], x[q], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) x[i] -= acc;
+      for (int i = t0 + 4 * warp; i < t0 + w; i += 4 * nw) {
+        double acc[4];
+        const int rows = min(4, t0 + w - i);
+        gemv4(LU, m, i, rows, 0, t0, x, lane, acc);
+        if (lane < rows) x[i + lane] -= (lane == 0) ? acc[0] : (lane == 1) ? acc[1] : (lane == 2) ? acc[2] : acc[3];
       }
       __syncthreads();
       tile_triangle(LU, m, t0, w, x, Ts, true);
     }
     for (int I = nt - 1; I >= 0; --I) {
       const int t0 = I * kTile, w = min(kTile, m - t0);
-      for (int i = t0 + warp; i < t0 + w; i += nw) {
-        const double* row = LU + static_cast<size_t>(i) * m;
-        double acc = 0.0;
-        for (int q = t0 + w + lane; q < m; q += 32) acc = fma(row[q], x[q], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) x[i] -= acc;
+      for (int i = t0 + 4 * warp; i < t0 + w; i += 4 * nw) {
+        double acc[4];
+        const int rows = min(4, t0 + w - i);
+        gemv4(LU, m, i, rows, t0 + w, m, x, lane, acc);
+        if (lane < rows) x[i + lane] -= (lane == 0) ? acc[0] : (lane == 1) ? acc[1] : (lane == 2) ? acc[2] : acc[3];
       }
       __syncthreads();
       tile_triangle(LU, m, t0, w, x, Ts, false);
@@ -634,7 +656,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_large_single(DevPlan dp, cons
 // J + 1 then solves its triangle.  J = -1 solves tile 0 only.
 __global__ void __launch_bounds__(kSolveThreads) k_trsv_fwd_rm(DevPlan dp, int32_t u, int32_t J,
                                                                double* __restrict__ xp, int32_t nrhs) {
-  __shared__ double Ts[kTile * kTile];
+  __shared__ double Ts[kTile * kTS];
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
   const double* LU = dp.lu + dp.lu_off[u];
@@ -645,12 +667,11 @@ __global__ void __launch_bounds__(kSolveThreads) k_trsv_fwd_rm(DevPlan dp, int32
   for (int c = 0; c < nrhs; ++c) {
     double* x = xp + static_cast<size_t>(c) * dp.n + s;
     if (J >= 0) {
-      for (int i = t0 + warp; i < t0 + w; i += kSolveThreads / 32) {
-        const double* row = LU + static_cast<size_t>(i) * m + j0;
-        double acc = 0.0;
-        for (int q = lane; q < kTile; q += 32) acc = fma(row[q], x[j0 + q], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) x[i] -= acc;
+      for (int i = t0 + 4 * warp; i < t0 + w; i += 4 * (kSolveThreads / 32)) {
+        double acc[4];
+        const int rows = min(4, t0 + w - i);
+        gemv4(LU, m, i, rows, j0, j0 + kTile, x, lane, acc);
+        if (lane < rows) x[i + lane] -= (lane == 0) ? acc[0] : (lane == 1) ? acc[1] : (lane == 2) ? acc[2] : acc[3];
       }
       __syncthreads();
     }
@@ -662,7 +683,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_trsv_fwd_rm(DevPlan dp, int32
 // J - 1 then solves its triangle.  J = nt solves the last tile only.
 __global__ void __launch_bounds__(kSolveThreads) k_trsv_bwd_rm(DevPlan dp, int32_t u, int32_t J, int32_t nt,
                                                                double* __restrict__ xp, int32_t nrhs) {
-  __shared__ double Ts[kTile * kTile];
+  __shared__ double Ts[kTile * kTS];
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
   const double* LU = dp.lu + dp.lu_off[u];
@@ -673,12 +694,11 @@ __global__ void __launch_bounds__(kSolveThreads) k_trsv_bwd_rm(DevPlan dp, int32
   for (int c = 0; c < nrhs; ++c) {
     double* x = xp + static_cast<size_t>(c) * dp.n + s;
     if (J < nt) {
-      for (int i = t0 + warp; i < t0 + w; i += kSolveThreads / 32) {
-        const double* row = LU + static_cast<size_t>(i) * m + j0;
-        double acc = 0.0;
-        for (int q = lane; q < jw; q += 32) acc = fma(row[q], x[j0 + q], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) x[i] -= acc;
+      for (int i = t0 + 4 * warp; i < t0 + w; i += 4 * (kSolveThreads / 32)) {
+        double acc[4];
+        const int rows = min(4, t0 + w - i);
+        gemv4(LU, m, i, rows, j0, j0 + jw, x, lane, acc);
+        if (lane < rows) x[i + lane] -= (lane == 0) ? acc[0] : (lane == 1) ? acc[1] : (lane == 2) ? acc[2] : acc[3];
       }
       __syncthreads();
     }
@@ -705,7 +725,7 @@ cudaError_t large_setup() {
       err = cudaFuncSetAttribute(k_large_perm, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 4 * 1024);
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_large_single, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (kTile * kTile + kLargeSingleMax) * static_cast<int>(sizeof(double)));
+                                 (kTile * kTS + kLargeSingleMax) * static_cast<int>(sizeof(double)));
   });
   return err;
 }
@@ -806,7 +826,7 @@ cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, const int32_t* d
   }
   if (nsingle > 0) {
     // d_units is ordered with the single-CTA units first (see plan.cpp).
-    k_large_single<<<nsingle, kSolveThreads, (kTile * kTile + kLargeSingleMax) * sizeof(double), stream>>>(
+    k_large_single<<<nsingle, kSolveThreads, (kTile * kTS + kLargeSingleMax) * sizeof(double), stream>>>(
         dp, d_units, xp, nrhs);
     ++*launches;
   }
