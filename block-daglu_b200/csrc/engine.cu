@@ -125,6 +125,23 @@ __global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double*
   }
   double* out = dp.lu + dp.lu_off[u];
   for (int i = tid; i < m * m; i += kThreads) out[i] = A[i];
+  // Final row order (row k of the factor is local row lperm[k]) for the solve.
+  __syncthreads();
+  int32_t* ord = reinterpret_cast<int32_t*>(A);
+  for (int k = tid; k < m; k += kThreads) ord[k] = k;
+  __syncthreads();
+  if (tid == 0) {
+    for (int k = 0; k < m; ++k) {
+      const int p = piv[k];
+      if (p != k) {
+        const int32_t t = ord[k];
+        ord[k] = ord[p];
+        ord[p] = t;
+      }
+    }
+  }
+  __syncthreads();
+  for (int k = tid; k < m; k += kThreads) dp.lperm[s + k] = ord[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -160,120 +177,97 @@ __global__ void k_solve_scalar(DevPlan dp, const int32_t* __restrict__ rows, int
   }
 }
 
-// Small dense units (column-major LU): the right-hand sides of up to
-// kSolveRhsChunk columns are formed together; each triangle is staged in
-// shared memory (packed by columns), and each warp sweeps one right-hand side
-// with the column's values in registers (kSlots per lane), broadcasting each
-// finished unknown with a shuffle, so a sweep step costs no CTA barrier.
-constexpr int kSolveRhsChunk = 16;
+// Small dense units (column-major LU, final row order in dp.lperm).  The
+// unit's m x m factor is copied to shared memory as it lies in the arena;
+// each warp then takes one right-hand side: it forms the pivoted rhs of its
+// rows directly in registers (kSlots rows per lane, b - A_cpl x gathered
+// through the row order), sweeps L and U with the column's values kept in
+// registers and each finished unknown broadcast by a shuffle, and writes x.
+// The backward sweep multiplies by the reciprocal of the pivot, which keeps
+// the division off the dependent chain.
 constexpr int kSlots = 6;  // rows per lane: units up to 192 rows
-static_assert(32 * kSlots >= 169, "register slots must cover the shared-memory LU limit");
-
-__device__ __forceinline__ double slot_get(const double (&a)[kSlots], int k) {
-  double v = a[0];
-#pragma unroll
-  for (int t = 1; t < kSlots; ++t)
-    if (k == t) v = a[t];
-  return v;
-}
+static_assert(32 * kSlots >= 170, "register slots must cover the shared-memory LU limit");
 
 __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int32_t* __restrict__ units,
                                                            const double* __restrict__ rhs, int32_t ldr,
                                                            double* __restrict__ xp, int32_t nrhs) {
-  extern __shared__ double sm[];
+  extern __shared__ double T[];
   const int u = units[blockIdx.x];
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
   const int n = dp.n;
-  const double* LU = dp.lu + dp.lu_off[u];
-  const int32_t* piv = dp.piv + s;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int kWarps = kThreads / 32;
-  double* T = sm;                              // packed triangle, m*(m+1)/2
-  double* X = sm + (m * (m + 1)) / 2;          // X[i * kSolveRhsChunk + c]
-  for (int k0 = 0; k0 < nrhs; k0 += kSolveRhsChunk) {
-    const int nc = min(kSolveRhsChunk, nrhs - k0);
-    for (int i = warp; i < m; i += kWarps) {
-      const int r = s + i;
-      const int p0 = dp.cpl_ptr[r], p1 = dp.cpl_ptr[r + 1];
-      for (int c = 0; c < nc; ++c) {
-        const double* xk = xp + static_cast<size_t>(k0 + c) * n;
+  const int nmine = (nrhs - warp + kWarps - 1) / kWarps;  // right-hand sides of this warp
+  double a[kSlots];
+  int rows[kSlots];
+#pragma unroll
+  for (int k = 0; k < kSlots; ++k) {
+    const int i = lane + 32 * k;
+    rows[k] = (i < m) ? s + dp.lperm[s + i] : -1;
+  }
+  auto form = [&](int c) {
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+      a[k] = 0.0;
+      const int r = rows[k];
+      if (r >= 0) {
+        const double* xk = xp + static_cast<size_t>(c) * n;
         double acc = 0.0;
-        for (int q = p0 + lane; q < p1; q += 32) acc = fma(dp.cpl_val[q], xk[dp.cpl_col[q]], acc);
-        acc = warp_sum(acc);
-        if (lane == 0) X[i * kSolveRhsChunk + c] = rhs[dp.P[r] + static_cast<size_t>(k0 + c) * ldr] - acc;
+        const int p1 = dp.cpl_ptr[r + 1];
+#pragma unroll 4
+        for (int q = dp.cpl_ptr[r]; q < p1; ++q) acc = fma(__ldg(dp.cpl_val + q), xk[__ldg(dp.cpl_col + q)], acc);
+        a[k] = rhs[dp.P[r] + static_cast<size_t>(c) * ldr] - acc;
       }
     }
-    // Strictly lower part of L, packed by columns: column j at j*(m-1) - j*(j-1)/2.
-    for (int j = warp; j < m - 1; j += kWarps) {
-      const int off = j * (m - 1) - (j * (j - 1)) / 2;
-      for (int i = j + 1 + lane; i < m; i += 32) T[off + i - j - 1] = LU[static_cast<size_t>(j) * m + i];
-    }
-    __syncthreads();
-    if (tid < nc) {
-      for (int i = 0; i < m; ++i) {
-        const int p = piv[i];
-        if (p != i) {
-          const double t = X[i * kSolveRhsChunk + tid];
-          X[i * kSolveRhsChunk + tid] = X[p * kSolveRhsChunk + tid];
-          X[p * kSolveRhsChunk + tid] = t;
-        }
-      }
-    }
-    __syncthreads();
-    for (int c = warp; c < nc; c += kWarps) {
-      double a[kSlots];
+  };
+  if (nmine > 0) form(warp);
+  const double* LU = dp.lu + dp.lu_off[u];
+  const int mm = m * m;
+#pragma unroll 4
+  for (int e = tid; e < mm; e += kThreads) T[e] = LU[e];
+  __syncthreads();
+  for (int t = 0; t < nmine; ++t) {
+    const int c = warp + t * kWarps;
+    if (t > 0) form(c);
+    // L: unit lower triangle, columns j = 0 .. m-2.
 #pragma unroll
-      for (int k = 0; k < kSlots; ++k) {
-        const int i = lane + 32 * k;
-        a[k] = (i < m) ? X[i * kSolveRhsChunk + c] : 0.0;
-      }
-      for (int j = 0; j < m - 1; ++j) {
-        const double xr = __shfl_sync(0xffffffffu, slot_get(a, j >> 5), j & 31);
-        const int base = j * (m - 1) - (j * (j - 1)) / 2 - j - 1;
+    for (int kk = 0; kk < kSlots; ++kk) {
+      const int jend = min(32, m - 1 - 32 * kk);
+      for (int jj = 0; jj < jend; ++jj) {
+        const int j = 32 * kk + jj;
+        const double xr = __shfl_sync(0xffffffffu, a[kk], jj);
+        const double* col = T + j * m;
 #pragma unroll
-        for (int k = 0; k < kSlots; ++k) {
+        for (int k = kk; k < kSlots; ++k) {
           const int i = lane + 32 * k;
-          if (i > j && i < m) a[k] = fma(-T[base + i], xr, a[k]);
+          if (i > j && i < m) a[k] = fma(-col[i], xr, a[k]);
         }
       }
-#pragma unroll
-      for (int k = 0; k < kSlots; ++k) {
-        const int i = lane + 32 * k;
-        if (i < m) X[i * kSolveRhsChunk + c] = a[k];
-      }
     }
-    __syncthreads();
-    // Upper part of U with the diagonal, packed by columns: column j at j*(j+1)/2.
-    for (int j = warp; j < m; j += kWarps) {
-      const int off = (j * (j + 1)) / 2;
-      for (int i = lane; i <= j; i += 32) T[off + i] = LU[static_cast<size_t>(j) * m + i];
-    }
-    __syncthreads();
-    for (int c = warp; c < nc; c += kWarps) {
-      double a[kSlots];
+    // U with its diagonal, columns j = m-1 .. 0.
 #pragma unroll
-      for (int k = 0; k < kSlots; ++k) {
-        const int i = lane + 32 * k;
-        a[k] = (i < m) ? X[i * kSolveRhsChunk + c] : 0.0;
-      }
-      for (int j = m - 1; j >= 0; --j) {
-        const int off = (j * (j + 1)) / 2;
-        const double xr = __shfl_sync(0xffffffffu, slot_get(a, j >> 5), j & 31) / T[off + j];
+    for (int kk = kSlots - 1; kk >= 0; --kk) {
+      const int jtop = min(31, m - 1 - 32 * kk);
+      for (int jj = jtop; jj >= 0; --jj) {
+        const int j = 32 * kk + jj;
+        const double* col = T + j * m;
+        const double rd = 1.0 / col[j];
+        const double xr = __shfl_sync(0xffffffffu, a[kk], jj) * rd;
+        if (lane == jj) a[kk] = xr;
 #pragma unroll
-        for (int k = 0; k < kSlots; ++k) {
+        for (int k = 0; k <= kk; ++k) {
           const int i = lane + 32 * k;
-          if (i == j) a[k] = xr;
-          else if (i < j) a[k] = fma(-T[off + i], xr, a[k]);
+          if (i < j) a[k] = fma(-col[i], xr, a[k]);
         }
       }
-#pragma unroll
-      for (int k = 0; k < kSlots; ++k) {
-        const int i = lane + 32 * k;
-        if (i < m) xp[static_cast<size_t>(k0 + c) * n + s + i] = a[k];
-      }
     }
-    __syncthreads();
+    double* xo = xp + static_cast<size_t>(c) * n + s;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+      const int i = lane + 32 * k;
+      if (i < m) xo[i] = a[k];
+    }
   }
 }
 
@@ -453,8 +447,7 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   int32_t small_m = 0;
   for (int32_t u : plan.small_units) small_m = std::max(small_m, plan.ustart[static_cast<size_t>(u) + 1] - plan.ustart[static_cast<size_t>(u)]);
   smem_small_ = static_cast<size_t>(small_m) * small_m * sizeof(double);
-  smem_solve_ = (static_cast<size_t>(small_m) * (small_m + 1) / 2 + static_cast<size_t>(small_m) * kSolveRhsChunk) *
-                sizeof(double);
+  smem_solve_ = static_cast<size_t>(small_m) * small_m * sizeof(double);
   {
     // The dynamic shared-memory limit is a per-function process-wide
     // attribute; raise it once to the device maximum so handles of different
@@ -486,6 +479,11 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   const int32_t* lvl_large = nullptr;
   if (!upload_vec(allocs_, plan.lvl_large, &lvl_large, err)) return false;
   lvl_large_ = lvl_large;
+  const int32_t* tile0 = nullptr;
+  if (!upload_vec(allocs_, plan.lvl_large_tile0, &tile0, err)) return false;
+  lvl_large_tile0_ = tile0;
+  sync_words_ = large_sync_words(plan);
+  if (!alloc_dev(allocs_, static_cast<size_t>(sync_words_), &d_sync_, err)) return false;
   small_list_ = small_list;
   large_list_ = large_list;
   lvl_scalar_ = lvl_scalar;
@@ -555,11 +553,11 @@ int Engine::factor_status(cudaStream_t stream, std::string& err) {
     err = std::string("factor status: ") + cudaGetErrorString(e);
     return -1;
   }
-  if (st[0] == 1) {
+  if (st[0] == kFailZeroPivot) {
     err = "block factorization failed: zero pivot in diagonal block " + std::to_string(st[1]);
     return 1;
   }
-  if (st[0] == 2) {
+  if (st[0] == kFailReusedPivot) {
     err = "reused pivot order met a zero pivot in diagonal block " + std::to_string(st[1]);
     return 2;
   }
@@ -593,6 +591,7 @@ double* Engine::rhs_buffer(int32_t nrhs, std::string& err) {
 void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, int32_t nrhs, cudaStream_t stream) {
   const Plan& p = plan_;
   const int32_t nl = p.umax_level + 1;
+  if (p.large_tiles > 0) cudaMemsetAsync(d_sync_, 0, static_cast<size_t>(sync_words_) * sizeof(int32_t), stream);
   for (int32_t l = 0; l < nl; ++l) {
     const int32_t s0 = p.lvl_scalar_ptr[static_cast<size_t>(l)], s1 = p.lvl_scalar_ptr[static_cast<size_t>(l) + 1];
     const int32_t d0 = p.lvl_dense_ptr[static_cast<size_t>(l)], d1 = p.lvl_dense_ptr[static_cast<size_t>(l) + 1];
@@ -605,10 +604,7 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, int32_t nrhs
     if (d1 > d0) ++launches_solve_;
     if (d1 > d0)
       k_solve_dense<<<d1 - d0, kThreads, smem_solve_, stream>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp, nrhs);
-    const int32_t g0 = p.lvl_large_ptr[static_cast<size_t>(l)], g1 = p.lvl_large_ptr[static_cast<size_t>(l) + 1];
-    if (g1 > g0)
-      large_solve_level(dp_, p, lvl_large_ + g0, p.lvl_large.data() + g0, g1 - g0, rhs, ldr, xp, nrhs, stream,
-                        &launches_solve_);
+    large_solve_level(dp_, p, l, lvl_large_, lvl_large_tile0_, d_sync_, rhs, ldr, xp, nrhs, stream, &launches_solve_);
   }
 }
 
@@ -669,9 +665,15 @@ bool Engine::restore_rhs(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t st
 bool Engine::last_residual(cudaStream_t stream, SolveResidual& out, std::string& err) {
   out = SolveResidual{0, 0, 0, 0};
   if (last_nrhs_ <= 0) return true;
+  int32_t st[2] = {0, 0};
+  BDLU_CUDA(cudaMemcpyAsync(st, d_status_, sizeof(st), cudaMemcpyDeviceToHost, stream));
   std::vector<unsigned long long> h(static_cast<size_t>(4 * last_nrhs_));
   BDLU_CUDA(cudaMemcpyAsync(h.data(), d_norms_, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
   BDLU_CUDA(cudaStreamSynchronize(stream));
+  if (st[0] == kFailSync) {
+    err = "solve failed: a bounded wait between solve tiles ran out";
+    return false;
+  }
   double worst = -1.0;
   for (int32_t k = 0; k < last_nrhs_; ++k) {
     double v[4];

@@ -125,6 +125,9 @@ class Engine {
   const int32_t* lvl_scalar_ = nullptr;
   const int32_t* lvl_dense_ = nullptr;
   const int32_t* lvl_large_ = nullptr;
+  const int32_t* lvl_large_tile0_ = nullptr;
+  int32_t* d_sync_ = nullptr;  // tickets and ready flags of the large-unit tile solves
+  int32_t sync_words_ = 0;
   size_t smem_small_ = 0;
   size_t smem_solve_ = 0;
   int num_sms_ = 148;

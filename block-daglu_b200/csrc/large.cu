@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(256) k_diag_nopiv(DevPlan dp, int32_t k0, int3
   }
   __syncthreads();
   if (s_bad) {
-    if (threadIdx.x == 0 && atomicCAS(dp.status, 0, 2) == 0) dp.status[1] = u;
+    if (threadIdx.x == 0 && atomicCAS(dp.status, 0, kFailReusedPivot) == 0) dp.status[1] = u;
     return;
   }
   for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
@@ -531,178 +531,171 @@ __global__ void __launch_bounds__(512) k_trsm_l(DevPlan dp, int32_t k0, int32_t 
   }
 }
 
-// rhs of each row in pivot order: xp[s + k] = b[P[s + perm[k]]] - A_cpl x.
-__global__ void __launch_bounds__(kSolveThreads) k_large_rhs(DevPlan dp, const int32_t* __restrict__ units,
-                                                             const double* __restrict__ rhs, int32_t ldr,
-                                                             double* __restrict__ xp, int32_t nrhs) {
-  const int u = units[blockIdx.y];
+// ---------------------------------------------------------------------------
+// Triangular solves of large units without a launch per tile.  The unit's
+// rows are cut into kTile-row tiles; each CTA takes a ticket (atomic counter,
+// so every tile with a smaller ticket belongs to a CTA that is already
+// running) and solves one tile: forward sweeps take the unit's tiles in
+// order, backward sweeps in reverse.  A CTA forms its rows' right-hand sides
+// (forward: b - A_cpl x through the unit's final row order; backward: the
+// forward result), then for every finished tile J it stages the kTile x kTile
+// block (I, J) of the factor in shared memory, waits for tile J's ready flag
+// and accumulates block(I, J) * x_J; finally it subtracts, solves its
+// diagonal triangle (one warp per right-hand side, unknowns in registers,
+// shuffle broadcasts), stores x_I and publishes its flag.  Flags count the
+// finished right-hand-side passes.  Every wait is bounded: a wait that runs
+// out records kFailSync in the status word and publishes kAbortFlag, so the
+// tiles behind it stop too.
+constexpr int kRC = kSolveThreads / 32;  // right-hand sides per pass (one warp each)
+constexpr int kSpinLimit = 1 << 22;       // polls of a flag (~0.5 s with the back-off)
+constexpr int32_t kAbortFlag = 1 << 30;
+
+__device__ __forceinline__ bool wait_ready(const int32_t* f, int32_t need) {
+  for (int it = 0; it < kSpinLimit; ++it) {
+    const int32_t v = *reinterpret_cast<const volatile int32_t*>(f);
+    if (v >= need) {
+      __threadfence();
+      return v < kAbortFlag;
+    }
+    if (it > 64) __nanosleep(128);
+  }
+  return false;
+}
+
+template <bool kFwd>
+__global__ void __launch_bounds__(kSolveThreads) k_trsv_tiles(DevPlan dp, const int32_t* __restrict__ units,
+                                                              const int32_t* __restrict__ tile0, int32_t count,
+                                                              int32_t* ticket, int32_t* ready,
+                                                              const double* __restrict__ rhs, int32_t ldr,
+                                                              double* __restrict__ xp, int32_t nrhs) {
+  __shared__ double Ts[kTile * kTS];  // factor block; also the partial-sum exchange
+  __shared__ double xs[kTile * kRC];  // this tile's unknowns [i * kRC + c]
+  __shared__ double xj[kTile * kRC];  // finished tile's unknowns
+  __shared__ int s_tk, s_ok;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tk = atomicAdd(ticket, 1);
+  __syncthreads();
+  const int tk = s_tk;
+  const int base0 = tile0[0];
+  int q = 0;
+  while (q + 1 < count && tile0[q + 1] - base0 <= tk) ++q;
+  const int u = units[q];
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
-  const int lane = threadIdx.x & 31;
   const int n = dp.n;
-  const int nw = kSolveThreads / 32;
-  for (int k = blockIdx.x * nw + (threadIdx.x >> 5); k < m; k += gridDim.x * nw) {
-    const int r = s + dp.lperm[s + k];
-    const int p0 = dp.cpl_ptr[r], p1 = dp.cpl_ptr[r + 1];
-    for (int c = 0; c < nrhs; ++c) {
-      const double* xc = xp + static_cast<size_t>(c) * n;
-      double acc = 0.0;
-      for (int q = p0 + lane; q < p1; q += 32) acc = fma(dp.cpl_val[q], xc[dp.cpl_col[q]], acc);
-      acc = warp_sum(acc);
-      if (lane == 0) xp[s + k + static_cast<size_t>(c) * n] = rhs[dp.P[r] + static_cast<size_t>(c) * ldr] - acc;
-    }
-  }
-}
-
-// acc_r = sum_q row_r[q] * x[q] over q in [q0, q1) for 4 rows at once (more
-// loads in flight per warp); rows past `rows` contribute nothing.
-__device__ __forceinline__ void gemv4(const double* LU, int m, int i0, int rows, int q0, int q1, const double* x,
-                                      int lane, double acc[4]) {
-  acc[0] = acc[1] = acc[2] = acc[3] = 0.0;
-  const double* r0 = LU + static_cast<size_t>(i0) * m;
-#pragma unroll 4
-  for (int q = q0 + lane; q < q1; q += 32) {
-    const double xq = x[q];
-#pragma unroll
-    for (int t = 0; t < 4; ++t)
-      if (t < rows) acc[t] = fma(__ldg(r0 + static_cast<size_t>(t) * m + q), xq, acc[t]);
-  }
-#pragma unroll
-  for (int t = 0; t < 4; ++t) acc[t] = warp_sum(acc[t]);
-}
-
-// 64 x 64 triangle of tile `t0` (rows/cols t0..t0+w) solved in place on x
-// (shared or global memory).  The tile is staged in shared memory; warp 0
-// keeps the 64 unknowns in registers (two per lane) and broadcasts each
-// finished one with a shuffle.  lower: unit-lower forward sweep; else upper
-// backward sweep with division by the diagonal.
-__device__ void tile_triangle(const double* LU, int m, int t0, int w, double* x, double* Ts, bool lower) {
-  for (int t = threadIdx.x; t < w * w; t += blockDim.x) {
-    const int i = t / w, c = t - i * w;
-    Ts[i * kTS + c] = LU[static_cast<size_t>(t0 + i) * m + t0 + c];
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
-    double a = (lane < w) ? x[t0 + lane] : 0.0;
-    double b = (lane + 32 < w) ? x[t0 + 32 + lane] : 0.0;
-    if (lower) {
-      for (int r = 0; r < w; ++r) {
-        const double xr = __shfl_sync(0xffffffffu, r < 32 ? a : b, r & 31);
-        if (lane > r && lane < w) a = fma(-Ts[lane * kTS + r], xr, a);
-        if (lane + 32 > r && lane + 32 < w) b = fma(-Ts[(lane + 32) * kTS + r], xr, b);
+  const int nt = (m + kTile - 1) / kTile;
+  const int kidx = tk - (tile0[q] - base0);
+  const int I = kFwd ? kidx : nt - 1 - kidx;
+  int32_t* rdy = ready + tile0[q];
+  const int t0 = I * kTile, w = min(kTile, m - t0);
+  const double* LU = dp.lu + dp.lu_off[u];
+  const int r = tid & (kTile - 1), g = tid / kTile;  // row of the tile, 16-column group
+  constexpr int kGroups = kSolveThreads / kTile;
+  constexpr int kGCols = kTile / kGroups;
+  for (int c0 = 0; c0 < nrhs; c0 += kRC) {
+    const int nc = min(kRC, nrhs - c0);
+    const int32_t need = c0 / kRC + 1;
+    if (kFwd) {
+      for (int i = warp; i < w; i += kSolveThreads / 32) {
+        const int rr = s + dp.lperm[s + t0 + i];
+        const int p0 = dp.cpl_ptr[rr], p1 = dp.cpl_ptr[rr + 1];
+        for (int c = 0; c < nc; ++c) {
+          const double* xc = xp + static_cast<size_t>(c0 + c) * n;
+          double acc = 0.0;
+          for (int qq = p0 + lane; qq < p1; qq += 32) acc = fma(dp.cpl_val[qq], xc[dp.cpl_col[qq]], acc);
+          acc = warp_sum(acc);
+          if (lane == 0) xs[i * kRC + c] = rhs[dp.P[rr] + static_cast<size_t>(c0 + c) * ldr] - acc;
+        }
       }
     } else {
-      for (int r = w - 1; r >= 0; --r) {
-        const double d = Ts[r * kTS + r];
-        const double xr = __shfl_sync(0xffffffffu, r < 32 ? a : b, r & 31) / d;
-        if (lane == r) a = xr;
-        if (lane + 32 == r) b = xr;
-        if (lane < r) a = fma(-Ts[lane * kTS + r], xr, a);
-        if (lane + 32 < r) b = fma(-Ts[(lane + 32) * kTS + r], xr, b);
+      for (int e = tid; e < w * nc; e += kSolveThreads) {
+        const int i = e / nc, c = e - i * nc;
+        xs[i * kRC + c] = __ldcg(xp + static_cast<size_t>(c0 + c) * n + s + t0 + i);
       }
     }
-    if (lane < w) x[t0 + lane] = a;
-    if (lane + 32 < w) x[t0 + 32 + lane] = b;
-  }
-  __syncthreads();
-}
-
-// Units up to kLargeSingleMax rows: the whole solve in one CTA.
-__global__ void __launch_bounds__(kSolveThreads) k_large_single(DevPlan dp, const int32_t* __restrict__ units,
-                                                                double* __restrict__ xp, int32_t nrhs) {
-  extern __shared__ double sm[];
-  double* Ts = sm;                // kTile * kTS
-  double* x = sm + kTile * kTS;   // m
-  const int u = units[blockIdx.x];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const double* LU = dp.lu + dp.lu_off[u];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nw = kSolveThreads / 32;
-  const int nt = (m + kTile - 1) / kTile;
-  for (int c = 0; c < nrhs; ++c) {
-    double* xg = xp + static_cast<size_t>(c) * dp.n + s;
-    for (int i = threadIdx.x; i < m; i += kSolveThreads) x[i] = xg[i];
+    double acc[kRC];
+#pragma unroll
+    for (int c = 0; c < kRC; ++c) acc[c] = 0.0;
+    const int jn = kFwd ? I : nt - 1 - I;
+    bool ok = true;
+    for (int jk = 0; jk < jn; ++jk) {
+      const int J = kFwd ? jk : nt - 1 - jk;
+      const int j0 = J * kTile, jw = min(kTile, m - j0);
+      __syncthreads();
+      for (int e = tid; e < kTile * kTile; e += kSolveThreads) {
+        const int i = e / kTile, cc = e - i * kTile;
+        Ts[i * kTS + cc] = (i < w && cc < jw) ? __ldg(LU + static_cast<size_t>(t0 + i) * m + j0 + cc) : 0.0;
+      }
+      if (tid == 0) s_ok = wait_ready(rdy + J, need) ? 1 : 0;
+      __syncthreads();
+      if (!s_ok) {
+        ok = false;
+        break;
+      }
+      for (int e = tid; e < kTile * kRC; e += kSolveThreads) {
+        const int jj = e / kRC, c = e - jj * kRC;
+        xj[e] = (jj < jw && c < nc) ? __ldcg(xp + static_cast<size_t>(c0 + c) * n + s + j0 + jj) : 0.0;
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int k = 0; k < kGCols; ++k) {
+        const int cc = g * kGCols + k;
+        const double t = Ts[r * kTS + cc];
+#pragma unroll
+        for (int c = 0; c < kRC; ++c) acc[c] = fma(t, xj[cc * kRC + c], acc[c]);
+      }
+    }
+    if (!ok) {
+      if (tid == 0) {
+        atomicCAS(dp.status, 0, kFailSync);
+        atomicExch(rdy + I, kAbortFlag);
+      }
+      return;
+    }
     __syncthreads();
-    for (int I = 0; I < nt; ++I) {
-      const int t0 = I * kTile, w = min(kTile, m - t0);
-      for (int i = t0 + 4 * warp; i < t0 + w; i += 4 * nw) {
-        double acc[4];
-        const int rows = min(4, t0 + w - i);
-        gemv4(LU, m, i, rows, 0, t0, x, lane, acc);
-        if (lane < rows) x[i + lane] -= (lane == 0) ? acc[0] : (lane == 1) ? acc[1] : (lane == 2) ? acc[2] : acc[3];
-      }
-      __syncthreads();
-      tile_triangle(LU, m, t0, w, x, Ts, true);
-    }
-    for (int I = nt - 1; I >= 0; --I) {
-      const int t0 = I * kTile, w = min(kTile, m - t0);
-      for (int i = t0 + 4 * warp; i < t0 + w; i += 4 * nw) {
-        double acc[4];
-        const int rows = min(4, t0 + w - i);
-        gemv4(LU, m, i, rows, t0 + w, m, x, lane, acc);
-        if (lane < rows) x[i + lane] -= (lane == 0) ? acc[0] : (lane == 1) ? acc[1] : (lane == 2) ? acc[2] : acc[3];
-      }
-      __syncthreads();
-      tile_triangle(LU, m, t0, w, x, Ts, false);
-    }
-    for (int i = threadIdx.x; i < m; i += kSolveThreads) xg[i] = x[i];
+#pragma unroll
+    for (int c = 0; c < kRC; ++c) Ts[(g * kTile + r) * kRC + c] = acc[c];
     __syncthreads();
-  }
-}
-
-// Forward sweep step J of a tall unit: tiles I > J take x_J's update; tile
-// J + 1 then solves its triangle.  J = -1 solves tile 0 only.
-__global__ void __launch_bounds__(kSolveThreads) k_trsv_fwd_rm(DevPlan dp, int32_t u, int32_t J,
-                                                               double* __restrict__ xp, int32_t nrhs) {
-  __shared__ double Ts[kTile * kTS];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const double* LU = dp.lu + dp.lu_off[u];
-  const int I = J + 1 + blockIdx.x;
-  const int t0 = I * kTile, w = min(kTile, m - t0);
-  const int j0 = J * kTile;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int c = 0; c < nrhs; ++c) {
-    double* x = xp + static_cast<size_t>(c) * dp.n + s;
-    if (J >= 0) {
-      for (int i = t0 + 4 * warp; i < t0 + w; i += 4 * (kSolveThreads / 32)) {
-        double acc[4];
-        const int rows = min(4, t0 + w - i);
-        gemv4(LU, m, i, rows, j0, j0 + kTile, x, lane, acc);
-        if (lane < rows) x[i + lane] -= (lane == 0) ? acc[0] : (lane == 1) ? acc[1] : (lane == 2) ? acc[2] : acc[3];
-      }
-      __syncthreads();
+    for (int e = tid; e < w * nc; e += kSolveThreads) {
+      const int i = e / nc, c = e - i * nc;
+      double sum = 0.0;
+#pragma unroll
+      for (int gg = 0; gg < kGroups; ++gg) sum += Ts[(gg * kTile + i) * kRC + c];
+      xs[i * kRC + c] -= sum;
     }
-    if (I == J + 1) tile_triangle(LU, m, t0, w, x, Ts, true);
-  }
-}
-
-// Backward sweep step J of a tall unit: tiles I < J take x_J's update; tile
-// J - 1 then solves its triangle.  J = nt solves the last tile only.
-__global__ void __launch_bounds__(kSolveThreads) k_trsv_bwd_rm(DevPlan dp, int32_t u, int32_t J, int32_t nt,
-                                                               double* __restrict__ xp, int32_t nrhs) {
-  __shared__ double Ts[kTile * kTS];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const double* LU = dp.lu + dp.lu_off[u];
-  const int I = J - 1 - blockIdx.x;
-  const int t0 = I * kTile, w = min(kTile, m - t0);
-  const int j0 = J * kTile, jw = (J < nt) ? min(kTile, m - j0) : 0;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int c = 0; c < nrhs; ++c) {
-    double* x = xp + static_cast<size_t>(c) * dp.n + s;
-    if (J < nt) {
-      for (int i = t0 + 4 * warp; i < t0 + w; i += 4 * (kSolveThreads / 32)) {
-        double acc[4];
-        const int rows = min(4, t0 + w - i);
-        gemv4(LU, m, i, rows, j0, j0 + jw, x, lane, acc);
-        if (lane < rows) x[i + lane] -= (lane == 0) ? acc[0] : (lane == 1) ? acc[1] : (lane == 2) ? acc[2] : acc[3];
-      }
-      __syncthreads();
+    __syncthreads();
+    for (int e = tid; e < kTile * kTile; e += kSolveThreads) {
+      const int i = e / kTile, cc = e - i * kTile;
+      Ts[i * kTS + cc] = (i < w && cc < w) ? __ldg(LU + static_cast<size_t>(t0 + i) * m + t0 + cc) : 0.0;
     }
-    if (I == J - 1) tile_triangle(LU, m, t0, w, x, Ts, false);
+    __syncthreads();
+    if (warp < nc) {
+      const int c = warp;
+      double a = (lane < w) ? xs[lane * kRC + c] : 0.0;
+      double b = (lane + 32 < w) ? xs[(lane + 32) * kRC + c] : 0.0;
+      if (kFwd) {
+        for (int rr = 0; rr < w; ++rr) {
+          const double xr = __shfl_sync(0xffffffffu, rr < 32 ? a : b, rr & 31);
+          if (lane > rr && lane < w) a = fma(-Ts[lane * kTS + rr], xr, a);
+          if (lane + 32 > rr && lane + 32 < w) b = fma(-Ts[(lane + 32) * kTS + rr], xr, b);
+        }
+      } else {
+        for (int rr = w - 1; rr >= 0; --rr) {
+          const double d = Ts[rr * kTS + rr];
+          const double xr = __shfl_sync(0xffffffffu, rr < 32 ? a : b, rr & 31) / d;
+          if (lane == rr) a = xr;
+          if (lane + 32 == rr) b = xr;
+          if (lane < rr) a = fma(-Ts[lane * kTS + rr], xr, a);
+          if (lane + 32 < rr) b = fma(-Ts[(lane + 32) * kTS + rr], xr, b);
+        }
+      }
+      double* xo = xp + static_cast<size_t>(c0 + c) * n + s + t0;
+      if (lane < w) xo[lane] = a;
+      if (lane + 32 < w) xo[lane + 32] = b;
+    }
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) atomicExch(rdy + I, need);
   }
 }
 
@@ -723,9 +716,6 @@ cudaError_t large_setup() {
     err = cudaFuncSetAttribute(k_gemm_rm, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kGemmSmem));
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_large_perm, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 4 * 1024);
-    if (err == cudaSuccess)
-      err = cudaFuncSetAttribute(k_large_single, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (kTile * kTS + kLargeSingleMax) * static_cast<int>(sizeof(double)));
   });
   return err;
 }
@@ -803,47 +793,25 @@ cudaError_t large_scatter_reuse(const DevPlan& dp, const Plan& p, const double* 
   return cudaGetLastError();
 }
 
-cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, const int32_t* d_units, const int32_t* h_units,
-                              int32_t count, const double* rhs, int32_t ldr, double* xp, int32_t nrhs,
-                              cudaStream_t stream, int32_t* launches) {
-  if (count <= 0) return cudaSuccess;
-  int32_t mmax = 0;
-  for (int32_t k = 0; k < count; ++k) {
-    const int32_t u = h_units[k];
-    mmax = std::max(mmax, p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)]);
-  }
-  const int gx = std::min<int32_t>((mmax + 63) / 64, 64);
-  k_large_rhs<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(count)), kSolveThreads, 0, stream>>>(
-      dp, d_units, rhs, ldr, xp, nrhs);
-  ++*launches;
-  // Units are grouped by the solve they take: one CTA for the shorter ones, a
-  // tile-by-tile launch sequence per tall unit.
-  int32_t nsingle = 0;
-  for (int32_t k = 0; k < count; ++k) {
-    const int32_t u = h_units[k];
-    const int32_t m = p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)];
-    if (m <= kLargeSingleMax) ++nsingle;
-  }
-  if (nsingle > 0) {
-    // d_units is ordered with the single-CTA units first (see plan.cpp).
-    k_large_single<<<nsingle, kSolveThreads, (kTile * kTS + kLargeSingleMax) * sizeof(double), stream>>>(
-        dp, d_units, xp, nrhs);
-    ++*launches;
-  }
-  for (int32_t k = nsingle; k < count; ++k) {
-    const int32_t u = h_units[k];
-    const int32_t m = p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)];
-    const int32_t nt = (m + kTile - 1) / kTile;
-    for (int32_t J = -1; J < nt - 1; ++J) {
-      k_trsv_fwd_rm<<<(J < 0) ? 1 : nt - J - 1, kSolveThreads, 0, stream>>>(dp, u, J, xp, nrhs);
-      ++*launches;
-    }
-    for (int32_t J = nt; J > 0; --J) {
-      k_trsv_bwd_rm<<<(J == nt) ? 1 : J, kSolveThreads, 0, stream>>>(dp, u, J, nt, xp, nrhs);
-      ++*launches;
-    }
-  }
+cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, int32_t level, const int32_t* d_units,
+                              const int32_t* d_tile0, int32_t* d_sync, const double* rhs, int32_t ldr, double* xp,
+                              int32_t nrhs, cudaStream_t stream, int32_t* launches) {
+  const int32_t g0 = p.lvl_large_ptr[static_cast<size_t>(level)];
+  const int32_t g1 = p.lvl_large_ptr[static_cast<size_t>(level) + 1];
+  if (g1 <= g0) return cudaSuccess;
+  const int32_t tiles = p.lvl_large_tile0[static_cast<size_t>(g1)] - p.lvl_large_tile0[static_cast<size_t>(g0)];
+  const int32_t nl = p.umax_level + 1;
+  int32_t* tickets = d_sync + 2 * level;
+  int32_t* ready_fwd = d_sync + 2 * nl;
+  int32_t* ready_bwd = ready_fwd + p.large_tiles;
+  k_trsv_tiles<true><<<tiles, kSolveThreads, 0, stream>>>(dp, d_units + g0, d_tile0 + g0, g1 - g0, tickets, ready_fwd,
+                                                           rhs, ldr, xp, nrhs);
+  k_trsv_tiles<false><<<tiles, kSolveThreads, 0, stream>>>(dp, d_units + g0, d_tile0 + g0, g1 - g0, tickets + 1,
+                                                            ready_bwd, rhs, ldr, xp, nrhs);
+  *launches += 2;
   return cudaGetLastError();
 }
+
+int32_t large_sync_words(const Plan& p) { return 2 * (p.umax_level + 1) + 2 * p.large_tiles; }
 
 }  // namespace bdlu

@@ -27,8 +27,12 @@ cudaError_t large_scatter_reuse(const DevPlan& dp, const Plan& p, const double* 
 
 // Enqueues the solve of the large units of one level (d_units / h_units: the
 // level's list, single-CTA units first).  xp is the permuted solution.
-cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, const int32_t* d_units, const int32_t* h_units,
-                              int32_t count, const double* rhs, int32_t ldr, double* xp, int32_t nrhs,
-                              cudaStream_t stream, int32_t* launches);
+// Forward and backward solves of the large units of one level (two
+// launches).  d_sync holds large_sync_words(p) zeroed words per solve sweep.
+cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, int32_t level, const int32_t* d_units,
+                              const int32_t* d_tile0, int32_t* d_sync, const double* rhs, int32_t ldr, double* xp,
+                              int32_t nrhs, cudaStream_t stream, int32_t* launches);
+
+int32_t large_sync_words(const Plan& p);
 
 }  // namespace bdlu

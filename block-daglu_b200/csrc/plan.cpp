@@ -142,21 +142,28 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
     std::vector<int32_t> sn(p.lvl_scalar_ptr.begin(), p.lvl_scalar_ptr.end() - 1);
     std::vector<int32_t> dn(p.lvl_dense_ptr.begin(), p.lvl_dense_ptr.end() - 1);
     std::vector<int32_t> ln(p.lvl_large_ptr.begin(), p.lvl_large_ptr.end() - 1);
-    // Large units: those solved by one CTA first within each level.
-    for (int pass = 0; pass < 2; ++pass) {
-      for (int32_t u = 0; u < nu; ++u) {
-        const int32_t l = p.ulevel[static_cast<size_t>(u)];
-        const int32_t k = p.ukind[static_cast<size_t>(u)];
-        const int32_t m = p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)];
-        if (pass == 0 && k == kUnitScalar)
-          p.lvl_scalar[static_cast<size_t>(sn[static_cast<size_t>(l)]++)] = p.ustart[static_cast<size_t>(u)];
-        else if (pass == 0 && k == kUnitSmall)
-          p.lvl_dense[static_cast<size_t>(dn[static_cast<size_t>(l)]++)] = u;
-        else if (k == kUnitLarge && (pass == 0) == (m <= kLargeSingleMax))
-          p.lvl_large[static_cast<size_t>(ln[static_cast<size_t>(l)]++)] = u;
-      }
+    for (int32_t u = 0; u < nu; ++u) {
+      const int32_t l = p.ulevel[static_cast<size_t>(u)];
+      const int32_t k = p.ukind[static_cast<size_t>(u)];
+      if (k == kUnitScalar)
+        p.lvl_scalar[static_cast<size_t>(sn[static_cast<size_t>(l)]++)] = p.ustart[static_cast<size_t>(u)];
+      else if (k == kUnitSmall)
+        p.lvl_dense[static_cast<size_t>(dn[static_cast<size_t>(l)]++)] = u;
+      else
+        p.lvl_large[static_cast<size_t>(ln[static_cast<size_t>(l)]++)] = u;
     }
   }
+  // Large units of a level: largest first, so the longest tile chain claims
+  // its CTAs first.
+  auto usize = [&](int32_t u) { return p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)]; };
+  for (int32_t l = 0; l < nl; ++l)
+    std::stable_sort(p.lvl_large.begin() + p.lvl_large_ptr[static_cast<size_t>(l)],
+                     p.lvl_large.begin() + p.lvl_large_ptr[static_cast<size_t>(l) + 1],
+                     [&](int32_t a, int32_t b) { return usize(a) > usize(b); });
+  p.lvl_large_tile0.assign(p.lvl_large.size() + 1, 0);
+  for (size_t q = 0; q < p.lvl_large.size(); ++q)
+    p.lvl_large_tile0[q + 1] = p.lvl_large_tile0[q] + (usize(p.lvl_large[q]) + kSolveTile - 1) / kSolveTile;
+  p.large_tiles = p.lvl_large_tile0.back();
 
   // Blocked-LU step tables for large units.
   int32_t max_large = 0;

@@ -54,7 +54,12 @@ struct Plan {
   int32_t umax_level = 0;
   std::vector<int32_t> lvl_scalar_ptr, lvl_scalar;  // permuted rows of scalar units, by level
   std::vector<int32_t> lvl_dense_ptr, lvl_dense;    // small dense unit ids, by level
-  std::vector<int32_t> lvl_large_ptr, lvl_large;    // large unit ids by level, single-CTA solves first
+  std::vector<int32_t> lvl_large_ptr, lvl_large;    // large unit ids by level, largest first
+  // Solve tiles (kSolveTile rows) of the large units: entry q of lvl_large
+  // owns tiles lvl_large_tile0[q] .. lvl_large_tile0[q + 1] - 1 of the
+  // solve's ready-flag arrays.
+  std::vector<int32_t> lvl_large_tile0;  // lvl_large.size() + 1
+  int32_t large_tiles = 0;
   std::vector<int32_t> small_units, large_units;
   // Blocked LU steps for large units (panel width kPanel): per step, the
   // active large units and per-unit CTA prefix sums for the swap/TRSM and
@@ -76,7 +81,7 @@ struct Plan {
 constexpr int kPanel = 32;          // panel width of the blocked LU
 constexpr int kTrsmCols = 128;      // columns per CTA in the swap/TRSM kernel
 constexpr int kGemmTile = 128;      // square output tile of the update kernel
-constexpr int kLargeSingleMax = 1024;  // large units solved by a single CTA
+constexpr int kSolveTile = 64;      // row tile of the large-unit triangular solves
 
 Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max);
 
