@@ -340,6 +340,8 @@ int32_t small_unit_max() {
 
 Engine::Engine() {
   cudaStreamCreateWithFlags(&cap_stream_, cudaStreamNonBlocking);
+  cudaStreamCreateWithFlags(&cap_stream2_, cudaStreamNonBlocking);
+  for (auto& e : fork_ev_) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (auto& e : ev_) cudaEventCreate(&e);
   for (auto& e : pev_) cudaEventCreate(&e);
   int dev = 0;
@@ -350,6 +352,9 @@ Engine::Engine() {
 Engine::~Engine() {
   release();
   if (cap_stream_) cudaStreamDestroy(cap_stream_);
+  if (cap_stream2_) cudaStreamDestroy(cap_stream2_);
+  for (auto& e : fork_ev_)
+    if (e) cudaEventDestroy(e);
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
   for (auto& e : pev_)
@@ -431,6 +436,10 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   if (!upload_vec(allocs_, plan.step_unit, &d.step_unit, err)) return false;
   if (!upload_vec(allocs_, plan.step_trsm_pref, &d.step_trsm_pref, err)) return false;
   if (!upload_vec(allocs_, plan.step_gemm_pref, &d.step_gemm_pref, err)) return false;
+  if (!upload_vec(allocs_, plan.rstep_unit, &d.rstep_unit, err)) return false;
+  if (!upload_vec(allocs_, plan.rstep_strip_pref, &d.rstep_strip_pref, err)) return false;
+  if (!upload_vec(allocs_, plan.rstep_ga_pref, &d.rstep_ga_pref, err)) return false;
+  if (!upload_vec(allocs_, plan.rstep_gb_pref, &d.rstep_gb_pref, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.lu_size), &d.lu, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.piv, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.lperm, err)) return false;
@@ -515,7 +524,7 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
       cudaMemsetAsync(dp_.lu + p.lu_large_begin, 0,
                       static_cast<size_t>(p.lu_large_end - p.lu_large_begin) * sizeof(double), cap_stream_);
       cudaError_t ce = large_scatter_reuse(dp_, p, d_vals, large_list_, cap_stream_);
-      if (ce == cudaSuccess) ce = large_factor(dp_, p, large_list_, true, cap_stream_, &n_launch);
+      if (ce == cudaSuccess) ce = large_refactor(dp_, p, cap_stream_, cap_stream2_, fork_ev_[0], fork_ev_[1], &n_launch);
       cudaGraph_t g = nullptr;
       const cudaError_t ee = cudaStreamEndCapture(cap_stream_, &g);
       BDLU_CUDA(ce);
@@ -530,14 +539,10 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   } else if (!p.large_units.empty()) {
     BDLU_CUDA(cudaMemsetAsync(dp_.lu + p.lu_large_begin, 0,
                               static_cast<size_t>(p.lu_large_end - p.lu_large_begin) * sizeof(double), stream));
-    if (reuse) {
-      BDLU_CUDA(large_scatter_reuse(dp_, p, d_vals, large_list_, stream));
-    } else {
-      k_scatter_large<<<dim3(64, static_cast<unsigned>(p.large_units.size())), kThreads, 0, stream>>>(dp_, d_vals,
-                                                                                                   large_list_);
-    }
+    k_scatter_large<<<dim3(64, static_cast<unsigned>(p.large_units.size())), kThreads, 0, stream>>>(dp_, d_vals,
+                                                                                                 large_list_);
     ++launches_factor_;
-    BDLU_CUDA(large_factor(dp_, p, large_list_, reuse, stream, &launches_factor_));
+    BDLU_CUDA(large_factor(dp_, p, large_list_, stream, &launches_factor_));
   }
   BDLU_CUDA(cudaGetLastError());
   BDLU_CUDA(cudaEventRecord(ev_[1], stream));

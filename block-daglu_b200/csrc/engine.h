@@ -32,6 +32,10 @@ struct DevPlan {
   const int32_t* step_unit;
   const int32_t* step_trsm_pref;
   const int32_t* step_gemm_pref;
+  const int32_t* rstep_unit;
+  const int32_t* rstep_strip_pref;
+  const int32_t* rstep_ga_pref;
+  const int32_t* rstep_gb_pref;
   double* lu;
   int32_t* piv;
   int32_t* lperm;   // final row order of each large unit (local indices)
@@ -136,6 +140,8 @@ class Engine {
   // the stored pivot order.  Captured on cap_stream_, launched on the
   // caller's stream.
   cudaStream_t cap_stream_ = nullptr;
+  cudaStream_t cap_stream2_ = nullptr;  // second branch of the refactor graph
+  cudaEvent_t fork_ev_[2] = {nullptr, nullptr};
   cudaGraphExec_t solve_exec_ = nullptr;
   int32_t solve_exec_nrhs_ = 0;
   const double* solve_exec_b0_ = nullptr;

@@ -29,20 +29,13 @@
 // Refactor with the stored pivot order (value-only refactor; the pivot order
 // of KLU's klu_refactor is reused the same way):
 //   k_scatter_large_perm  values scattered with rows already permuted
-//   k_diag_nopiv      nb x nb diagonal block, no pivot search; a zero or
-//                     non-finite pivot flags the unit for full pivoting
-//   k_trsm_l          L21 = A21 U11^{-1}, one warp per row
-//   k_swap_trsm_rm (no swaps) and k_gemm_rm as above
+//   k_rdiag / k_rstrip / k_rgemm
+//                     64-column blocked LU without pivot search, trailing
+//                     update split for one step of lookahead (see below)
 // Solve (per level holding large units):
-//   k_large_rhs       rhs of every row in pivot order: b - A_cpl x, gathered
-//                     through the unit's final row order
-//   k_large_single    units up to kLargeSingleMax rows: one CTA, forward and
-//                     backward sweeps by 64-row tiles (row-major GEMV + a
-//                     64 x 64 triangle in shared memory)
-//   k_trsv_fwd_rm / k_trsv_bwd_rm
-//                     taller units: one launch per 64-row tile; the CTAs of
-//                     the later tiles apply the finished tile's update and the
-//                     next tile's CTA solves its diagonal triangle
+//   k_trsv_tiles<fwd/bwd>
+//                     one CTA per 64-row tile, ticket-ordered, ready flags
+//                     between tiles (see below)
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
@@ -259,8 +252,7 @@ __global__ void __launch_bounds__(kPT) k_panel_global(DevPlan dp, int32_t k0, in
 // columns right of the panel.  One thread per column.  The nb sequential swaps
 // touch at most 2*nb rows; their net permutation is formed once per CTA in
 // shared memory, so each thread loads every touched value before it stores.
-__global__ void __launch_bounds__(kTrsmCols) k_swap_trsm_rm(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
-                                                             int32_t swaps) {
+__global__ void __launch_bounds__(kTrsmCols) k_swap_trsm_rm(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
   __shared__ double L11[kPanel][kPanel + 1];
   __shared__ int rows[2 * kPanel];  // touched rows: k0..k0+nb-1 first, then the others
   __shared__ int src[2 * kPanel];   // new value of rows[q] = old value of rows[src[q]]
@@ -284,7 +276,7 @@ __global__ void __launch_bounds__(kTrsmCols) k_swap_trsm_rm(DevPlan dp, int32_t 
       src[r] = r;
     }
     // Simulate the swaps on positions: pos_of[row] via linear search (<= 64).
-    for (int r = 0; r < nb && swaps; ++r) {
+    for (int r = 0; r < nb; ++r) {
       const int p = dp.piv[s + k0 + r];
       if (p == k0 + r) continue;
       int qp = -1;
@@ -305,7 +297,6 @@ __global__ void __launch_bounds__(kTrsmCols) k_swap_trsm_rm(DevPlan dp, int32_t 
   __syncthreads();
   const int j = chunk * kTrsmCols + threadIdx.x;
   if (j >= m || (j >= k0 && j < k0 + nb)) return;
-  if (!swaps && j < k0) return;
   const int cnt = s_cnt;
   // Gather every touched row's new value (all loads first), then store.
   double nv[2 * kPanel];
@@ -449,85 +440,6 @@ __global__ void k_scatter_large_perm(DevPlan dp, const double* __restrict__ vals
     const int pos = dp.dent_pos[e];
     const int r = pos / m, c = pos - (pos / m) * m;
     A[static_cast<size_t>(dp.liperm[s + r]) * m + c] = vals[dp.dent_src[e]];
-  }
-}
-
-// Diagonal block of a step without pivot search (rows already in pivot
-// order): unblocked LU of the nb x nb block in shared memory.  A zero or
-// non-finite pivot marks the unit for a factorisation with pivoting
-// (status 2).
-__global__ void __launch_bounds__(256) k_diag_nopiv(DevPlan dp, int32_t k0, int32_t ubase) {
-  __shared__ double D[kPanel][kPanel + 1];
-  __shared__ int s_bad;
-  const int u = dp.step_unit[ubase + blockIdx.x];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const int nb = min(kPanel, m - k0);
-  double* A = dp.lu + dp.lu_off[u];
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    const int r = t / nb, c = t - r * nb;
-    D[r][c] = A[static_cast<size_t>(k0 + r) * m + k0 + c];
-  }
-  if (threadIdx.x == 0) s_bad = 0;
-  __syncthreads();
-  for (int k = 0; k < nb; ++k) {
-    const double d = D[k][k];
-    if (!(fabs(d) > 0.0) || !isfinite(d)) {
-      if (threadIdx.x == 0) s_bad = 1;
-      break;
-    }
-    const double dinv = 1.0 / d;
-    const int r = threadIdx.x / kPanel, c = threadIdx.x - (threadIdx.x / kPanel) * kPanel;
-    // 256 threads: 8 rows x 32 columns per pass.
-    for (int i = k + 1 + r; i < nb; i += 8) {
-      const double l = D[i][k] * dinv;
-      if (c > k && c < nb) D[i][c] = fma(-l, D[k][c], D[i][c]);
-      __syncwarp();
-      if (c == k) D[i][k] = l;
-    }
-    __syncthreads();
-  }
-  __syncthreads();
-  if (s_bad) {
-    if (threadIdx.x == 0 && atomicCAS(dp.status, 0, kFailReusedPivot) == 0) dp.status[1] = u;
-    return;
-  }
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    const int r = t / nb, c = t - r * nb;
-    A[static_cast<size_t>(k0 + r) * m + k0 + c] = D[r][c];
-  }
-}
-
-// L21 = A21 * U11^{-1} for the rows below the diagonal block, one warp per
-// row: lane c holds column c of the row.
-constexpr int kTrslRowsPerCta = 16;
-__global__ void __launch_bounds__(512) k_trsm_l(DevPlan dp, int32_t k0, int32_t ubase) {
-  __shared__ double Ut[kPanel][kPanel + 1];
-  __shared__ double rinv[kPanel];
-  const int u = dp.step_unit[ubase + blockIdx.y];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const int nb = min(kPanel, m - k0);
-  const int base = k0 + nb;
-  const int row0 = base + blockIdx.x * kTrslRowsPerCta * 2;
-  if (row0 >= m) return;
-  double* A = dp.lu + dp.lu_off[u];
-  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-    const int r = t / nb, c = t - r * nb;
-    Ut[r][c] = A[static_cast<size_t>(k0 + r) * m + k0 + c];
-  }
-  if (threadIdx.x < nb) rinv[threadIdx.x] = 1.0 / A[static_cast<size_t>(k0 + threadIdx.x) * m + k0 + threadIdx.x];
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int i = row0 + warp; i < min(m, row0 + kTrslRowsPerCta * 2); i += 16) {
-    double* row = A + static_cast<size_t>(i) * m + k0;
-    double x = (lane < nb) ? row[lane] : 0.0;
-    for (int q = 0; q < nb; ++q) {
-      const double lq = __shfl_sync(0xffffffffu, x, q) * rinv[q];
-      if (lane > q) x = fma(-lq, Ut[q][lane], x);
-      else if (lane == q) x = lq;
-    }
-    if (lane < nb) row[lane] = x;
   }
 }
 
@@ -699,6 +611,281 @@ __global__ void __launch_bounds__(kSolveThreads) k_trsv_tiles(DevPlan dp, const 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Value-only refactor of large units with the stored pivot order: steps of
+// kRPanel (64) columns.  Per step:
+//   k_rdiag   one CTA per unit: LU of the 64 x 64 diagonal block without
+//             pivot search, split in 32 x 32 blocks: LU(D11) by one warp with
+//             the rows in registers (pivot-row values by shuffle), then
+//             U12 = L11^{-1} D12 and L21 = D21 U11^{-1} by two warps (one
+//             column / row per lane), D22 -= L21 U12, and LU(D22) by one
+//             warp.  A zero or non-finite pivot flags the unit for full
+//             pivoting.
+//   k_rstrip  L21 = A21 U11^{-1} (row chunks) and U12 = L11^{-1} A12 (column
+//             chunks) by substitution: four threads per row (column) hold 16
+//             entries each in registers; each finished unknown is broadcast
+//             within the four by a shuffle, so no CTA barrier is needed.
+//   k_rgemm   A22 -= L21 U12, K = 64, 128 x 64 tiles, 4 x 8 accumulators per
+//             thread, two CTAs per SM.  Part "a" updates tile row 0 and tile
+//             column 0, which hold the next step's strips; part "b" the rest.
+// Part b of step k runs on a second stream beside the next step's k_rdiag,
+// k_rstrip and part a (depth-1 lookahead); the regions are disjoint: the
+// next step reads and writes rows/columns [base, base + 64) only, part b
+// writes rows >= base + 128 and columns >= base + 64.
+constexpr int kRP = kRPanel;
+constexpr int kRS = kRP + 1;
+constexpr int kRThreads = 256;
+constexpr int kHB = kRP / 2;
+constexpr int kPadRow = 72;    // padded 64-entry row: quarter q at offset 18q (16-byte loads, no conflicts)
+constexpr int kRAS = kRP + 1;  // As row stride in k_rgemm
+constexpr size_t kRGemmSmem = (static_cast<size_t>(kRTileM) * kRAS + static_cast<size_t>(kRP) * kRTileN) * sizeof(double);
+
+// LU without pivot search of the 32 x 32 block at (o, o) of D, by one warp:
+// lane i keeps row i in registers; step j takes the pivot row's entries from
+// lane j by shuffle.
+__device__ __forceinline__ void warp_lu32(double* D, int o, int lane) {
+  double v[kHB];
+#pragma unroll
+  for (int c = 0; c < kHB; ++c) v[c] = D[(o + lane) * kRS + o + c];
+#pragma unroll
+  for (int j = 0; j < kHB; ++j) {
+    const double piv = __shfl_sync(0xffffffffu, v[j], j);
+    if (lane > j) v[j] = v[j] / piv;
+    const double l = v[j];
+#pragma unroll
+    for (int c = j + 1; c < kHB; ++c) {
+      const double u = __shfl_sync(0xffffffffu, v[c], j);
+      if (lane > j) v[c] = fma(-l, u, v[c]);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < kHB; ++c) D[(o + lane) * kRS + o + c] = v[c];
+}
+
+__global__ void __launch_bounds__(kRThreads) k_rdiag(DevPlan dp, int32_t k0, int32_t ubase) {
+  __shared__ double D[kRP * kRS];
+  const int u = dp.rstep_unit[ubase + blockIdx.x];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kRP, m - k0);
+  double* A = dp.lu + dp.lu_off[u];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // Rows/columns past nb are padded with the identity.
+#pragma unroll
+  for (int e = tid; e < kRP * kRP; e += kRThreads) {
+    const int i = e / kRP, c = e - i * kRP;
+    D[i * kRS + c] = (i < nb && c < nb) ? A[static_cast<size_t>(k0 + i) * m + k0 + c] : (i == c ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  if (warp == 0) warp_lu32(D, 0, lane);
+  __syncthreads();
+  if (warp == 0) {
+    // U12 = L11^{-1} D12: lane = column kHB + lane.
+    double x[kHB];
+#pragma unroll
+    for (int r = 0; r < kHB; ++r) x[r] = D[r * kRS + kHB + lane];
+#pragma unroll
+    for (int j = 0; j < kHB; ++j)
+#pragma unroll
+      for (int r = j + 1; r < kHB; ++r) x[r] = fma(-D[r * kRS + j], x[j], x[r]);
+#pragma unroll
+    for (int r = 0; r < kHB; ++r) D[r * kRS + kHB + lane] = x[r];
+  } else if (warp == 1) {
+    // L21 = D21 U11^{-1}: lane = row kHB + lane.
+    double x[kHB];
+#pragma unroll
+    for (int c = 0; c < kHB; ++c) x[c] = D[(kHB + lane) * kRS + c];
+#pragma unroll
+    for (int j = 0; j < kHB; ++j) {
+      x[j] = x[j] / D[j * kRS + j];
+#pragma unroll
+      for (int c = j + 1; c < kHB; ++c) x[c] = fma(-x[j], D[j * kRS + c], x[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < kHB; ++c) D[(kHB + lane) * kRS + c] = x[c];
+  }
+  __syncthreads();
+  {
+    // D22 -= L21 U12: thread = row r, columns cb + 8b.
+    const int r = tid >> 3, cb = tid & 7;
+    double acc[4];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[b] = D[(kHB + r) * kRS + kHB + cb + 8 * b];
+#pragma unroll 8
+    for (int q = 0; q < kHB; ++q) {
+      const double l = D[(kHB + r) * kRS + q];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[b] = fma(-l, D[q * kRS + kHB + cb + 8 * b], acc[b]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < 4; ++b) D[(kHB + r) * kRS + kHB + cb + 8 * b] = acc[b];
+  }
+  __syncthreads();
+  if (warp == 0) warp_lu32(D, kHB, lane);
+  __syncthreads();
+  if (tid < nb) {
+    const double d = D[tid * kRS + tid];
+    if (!(fabs(d) > 0.0) || !isfinite(d)) {
+      if (atomicCAS(dp.status, 0, kFailReusedPivot) == 0) dp.status[1] = u;
+    }
+  }
+#pragma unroll 4
+  for (int e = tid; e < nb * nb; e += kRThreads) {
+    const int i = e / nb, c = e - i * nb;
+    A[static_cast<size_t>(k0 + i) * m + k0 + c] = D[i * kRS + c];
+  }
+}
+
+// Row chunks: rows o0 .. o0+w of L21 from x U11 = a.  Column chunks: columns
+// o0 .. o0+w of U12 from L11 x = b.  Thread (line = tid / 4, quarter qq)
+// holds entries 16qq .. 16qq+15 of its row (column) in registers; the
+// factor's row j of U (column j of L) is staged padded in shared memory.
+__global__ void __launch_bounds__(kRThreads) k_rstrip(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
+  __shared__ __align__(16) double T[kRP * kPadRow];
+  __shared__ double rd[kRP];
+  int a = 0;
+  while (a + 1 < nact && dp.rstep_strip_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
+  const int u = dp.rstep_unit[ubase + a];
+  const int ch = blockIdx.x - dp.rstep_strip_pref[ubase + a];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kRP, m - k0);
+  const int base = k0 + nb;
+  const int chunks = (m - base + kRP - 1) / kRP;
+  const bool rowc = ch < chunks;
+  const int o0 = base + (rowc ? ch : ch - chunks) * kRP;
+  const int w = min(kRP, m - o0);
+  double* A = dp.lu + dp.lu_off[u];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int line = tid >> 2, qq = tid & 3;
+  // T[j][18q + t]: rows: U[j][16q + t]; columns: L[16q + t][j].  Past nb the
+  // factor is the identity.
+#pragma unroll
+  for (int e = tid; e < kRP * kRP; e += kRThreads) {
+    const int j = e / kRP, c = e - j * kRP;
+    double v;
+    if (rowc) v = (j < nb && c < nb) ? A[static_cast<size_t>(k0 + j) * m + k0 + c] : (j == c ? 1.0 : 0.0);
+    else v = (j < nb && c < nb) ? A[static_cast<size_t>(k0 + c) * m + k0 + j] : (j == c ? 1.0 : 0.0);
+    T[j * kPadRow + 18 * (c >> 4) + (c & 15)] = v;
+  }
+  double x[16];
+  const bool live = line < w;
+#pragma unroll
+  for (int t = 0; t < 16; ++t) {
+    const int q = 16 * qq + t;
+    double v = 0.0;
+    if (live && q < nb)
+      v = rowc ? A[static_cast<size_t>(o0 + line) * m + k0 + q] : A[static_cast<size_t>(k0 + q) * m + o0 + line];
+    x[t] = v;
+  }
+  __syncthreads();
+  if (rowc && tid < kRP) rd[tid] = 1.0 / T[tid * kPadRow + 18 * (tid >> 4) + (tid & 15)];
+  __syncthreads();
+  const int src = (lane & ~3);
+  for (int jq = 0; jq < 4; ++jq) {
+#pragma unroll
+    for (int jt = 0; jt < 16; ++jt) {
+      const int j = 16 * jq + jt;
+      if (rowc && qq == jq) x[jt] *= rd[j];
+      const double xj = __shfl_sync(0xffffffffu, x[jt], src | jq);
+      const double2* tv = reinterpret_cast<const double2*>(T + j * kPadRow + 18 * qq);
+#pragma unroll
+      for (int t2 = 0; t2 < 8; ++t2) {
+        const double2 f = tv[t2];
+        if (qq > jq || (qq == jq && 2 * t2 > jt)) x[2 * t2] = fma(-xj, f.x, x[2 * t2]);
+        if (qq > jq || (qq == jq && 2 * t2 + 1 > jt)) x[2 * t2 + 1] = fma(-xj, f.y, x[2 * t2 + 1]);
+      }
+    }
+  }
+  if (live) {
+#pragma unroll
+    for (int t = 0; t < 16; ++t) {
+      const int q = 16 * qq + t;
+      if (q < nb) {
+        if (rowc) A[static_cast<size_t>(o0 + line) * m + k0 + q] = x[t];
+        else A[static_cast<size_t>(k0 + q) * m + o0 + line] = x[t];
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kRThreads, 2) k_rgemm(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
+                                                        int32_t part) {
+  extern __shared__ double rsm[];
+  double* As = rsm;                      // kRTileM x kRAS
+  double* Bs = rsm + kRTileM * kRAS;     // kRP x kRTileN
+  const int32_t* pref = part ? dp.rstep_gb_pref : dp.rstep_ga_pref;
+  int a = 0;
+  while (a + 1 < nact && pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
+  const int u = dp.rstep_unit[ubase + a];
+  const int t = blockIdx.x - pref[ubase + a];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kRP, m - k0);
+  const int base = k0 + nb;
+  const int rest = m - base;
+  const int ntj = (rest + kRTileN - 1) / kRTileN;
+  int ti, tj;
+  if (part == 0) {
+    if (t < ntj) {
+      ti = 0;
+      tj = t;
+    } else {
+      ti = t - ntj + 1;
+      tj = 0;
+    }
+  } else {
+    ti = 1 + t / (ntj - 1);
+    tj = 1 + t % (ntj - 1);
+  }
+  const int i0 = base + ti * kRTileM, j0 = base + tj * kRTileN;
+  double* A = dp.lu + dp.lu_off[u];
+  const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+#pragma unroll 8
+  for (int e = tid; e < kRTileM * kRP; e += kRThreads) {
+    const int r = e / kRP, q = e - r * kRP;
+    As[r * kRAS + q] = (i0 + r < m && q < nb) ? A[static_cast<size_t>(i0 + r) * m + k0 + q] : 0.0;
+  }
+#pragma unroll 8
+  for (int e = tid; e < kRP * kRTileN; e += kRThreads) {
+    const int q = e / kRTileN, c = e - q * kRTileN;
+    Bs[e] = (q < nb && j0 + c < m) ? A[static_cast<size_t>(k0 + q) * m + j0 + c] : 0.0;
+  }
+  __syncthreads();
+  // The C tile: rows i0 + ty*4 + i, columns j0 + 8b + tx.
+  double acc[4][8];
+  const bool cin = j0 + 7 * 8 + tx < m;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = i0 + ty * 4 + i;
+    const double* crow = A + static_cast<size_t>(r) * m + j0 + tx;
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+      acc[i][b] = (r < m && (cin || j0 + b * 8 + tx < m)) ? crow[b * 8] : 0.0;
+  }
+#pragma unroll 2
+  for (int k = 0; k < kRP; ++k) {
+    double x[4], y[8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) x[i] = As[(ty * 4 + i) * kRAS + k];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) y[b] = Bs[k * kRTileN + b * 8 + tx];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int b = 0; b < 8; ++b) acc[i][b] = fma(-x[i], y[b], acc[i][b]);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = i0 + ty * 4 + i;
+    double* crow = A + static_cast<size_t>(r) * m + j0 + tx;
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+      if (r < m && (cin || j0 + b * 8 + tx < m)) crow[b * 8] = acc[i][b];
+  }
+}
+
 int cluster_size_for(int rows) {
   int c = (rows + kPanelRowsMax - 1) / kPanelRowsMax;
   return std::max(1, c);
@@ -715,13 +902,15 @@ cudaError_t large_setup() {
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     err = cudaFuncSetAttribute(k_gemm_rm, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kGemmSmem));
     if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_rgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kRGemmSmem));
+    if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_large_perm, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 4 * 1024);
   });
   return err;
 }
 
-cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, bool reuse,
-                         cudaStream_t stream, int32_t* launches) {
+cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, cudaStream_t stream,
+                         int32_t* launches) {
   cudaError_t e = large_setup();
   if (e != cudaSuccess) return e;
   for (int32_t st = 0; st < p.nsteps; ++st) {
@@ -730,24 +919,6 @@ cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_larg
     if (na <= 0) continue;
     const int32_t k0 = st * kPanel;
     const int32_t rows = p.step_max_rows[static_cast<size_t>(st)];
-    if (reuse) {
-      // Rows are already in the stored pivot order: diagonal block, L21,
-      // U12 and the update, all without pivot search.
-      k_diag_nopiv<<<na, 256, 0, stream>>>(dp, k0, ub);
-      const int rows_below = rows - std::min(kPanel, rows);
-      if (rows_below > 0) {
-        const unsigned gx = static_cast<unsigned>((rows_below + 2 * kTrslRowsPerCta - 1) / (2 * kTrslRowsPerCta));
-        k_trsm_l<<<dim3(gx, static_cast<unsigned>(na)), 512, 0, stream>>>(dp, k0, ub);
-        ++*launches;
-      }
-      k_swap_trsm_rm<<<p.step_trsm_total[static_cast<size_t>(st)], kTrsmCols, 0, stream>>>(dp, k0, ub, na, 0);
-      *launches += 2;
-      if (p.step_gemm_total[static_cast<size_t>(st)] > 0) {
-        k_gemm_rm<<<p.step_gemm_total[static_cast<size_t>(st)], kGThreads, kGemmSmem, stream>>>(dp, k0, ub, na);
-        ++*launches;
-      }
-      continue;
-    }
     const int csize = cluster_size_for(rows);
     if (csize <= kClusterMaxCtas) {
       const int chunk = (rows + csize - 1) / csize;
@@ -769,7 +940,7 @@ cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_larg
     } else {
       k_panel_global<<<na, kPT, 0, stream>>>(dp, k0, ub);
     }
-    k_swap_trsm_rm<<<p.step_trsm_total[static_cast<size_t>(st)], kTrsmCols, 0, stream>>>(dp, k0, ub, na, 1);
+    k_swap_trsm_rm<<<p.step_trsm_total[static_cast<size_t>(st)], kTrsmCols, 0, stream>>>(dp, k0, ub, na);
     *launches += 2;
     if (p.step_gemm_total[static_cast<size_t>(st)] > 0) {
       k_gemm_rm<<<p.step_gemm_total[static_cast<size_t>(st)], kGThreads, kGemmSmem, stream>>>(dp, k0, ub, na);
@@ -777,7 +948,7 @@ cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_larg
     }
   }
   const int nl = static_cast<int>(p.large_units.size());
-  if (nl > 0 && !reuse) {
+  if (nl > 0) {
     int32_t mmax = 0;
     for (int32_t u : p.large_units) mmax = std::max(mmax, p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)]);
     k_large_perm<<<nl, 256, static_cast<size_t>(mmax) * sizeof(int32_t), stream>>>(dp, d_large_units);
@@ -790,6 +961,48 @@ cudaError_t large_scatter_reuse(const DevPlan& dp, const Plan& p, const double* 
                                 cudaStream_t stream) {
   if (p.large_units.empty()) return cudaSuccess;
   k_scatter_large_perm<<<dim3(64, static_cast<unsigned>(p.large_units.size())), 256, 0, stream>>>(dp, d_vals, d_large_units);
+  return cudaGetLastError();
+}
+
+cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cudaStream_t sb, cudaEvent_t ev_a,
+                           cudaEvent_t ev_b, int32_t* launches) {
+  cudaError_t e = large_setup();
+  if (e != cudaSuccess) return e;
+  // Fork: stream b starts after everything already queued on stream a.
+  if ((e = cudaEventRecord(ev_a, sa)) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(sb, ev_a, 0)) != cudaSuccess) return e;
+  for (int32_t st = 0; st < p.rsteps; ++st) {
+    const int32_t ub = p.rstep_ptr[static_cast<size_t>(st)];
+    const int32_t na = p.rstep_ptr[static_cast<size_t>(st) + 1] - ub;
+    if (na <= 0) continue;
+    const int32_t k0 = st * kRPanel;
+    k_rdiag<<<na, kRThreads, 0, sa>>>(dp, k0, ub);
+    ++*launches;
+    const int32_t ns = p.rstep_strip_total[static_cast<size_t>(st)];
+    if (ns > 0) {
+      k_rstrip<<<ns, kRThreads, 0, sa>>>(dp, k0, ub, na);
+      ++*launches;
+    }
+    // Part a of this step follows part b of the previous one (stream b so
+    // far); part b of this step follows this step's strips (stream a so far).
+    if ((e = cudaEventRecord(ev_b, sb)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(sa, ev_b, 0)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ev_a, sa)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(sb, ev_a, 0)) != cudaSuccess) return e;
+    const int32_t gb = p.rstep_gb_total[static_cast<size_t>(st)];
+    if (gb > 0) {
+      k_rgemm<<<gb, kRThreads, kRGemmSmem, sb>>>(dp, k0, ub, na, 1);
+      ++*launches;
+    }
+    const int32_t ga = p.rstep_ga_total[static_cast<size_t>(st)];
+    if (ga > 0) {
+      k_rgemm<<<ga, kRThreads, kRGemmSmem, sa>>>(dp, k0, ub, na, 0);
+      ++*launches;
+    }
+  }
+  // Join.
+  if ((e = cudaEventRecord(ev_b, sb)) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(sa, ev_b, 0)) != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

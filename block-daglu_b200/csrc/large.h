@@ -17,8 +17,8 @@ cudaError_t large_setup();
 // orders (lperm/liperm).  reuse = true: the slots were filled by
 // large_scatter_reuse in the stored row order and no pivot search is made; a
 // zero or non-finite pivot sets status code 2.
-cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, bool reuse,
-                         cudaStream_t stream, int32_t* launches);
+cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, cudaStream_t stream,
+                         int32_t* launches);
 
 // Scatters the values of all large units into their (zeroed) slots with the
 // rows in the stored pivot order.
@@ -27,6 +27,13 @@ cudaError_t large_scatter_reuse(const DevPlan& dp, const Plan& p, const double* 
 
 // Enqueues the solve of the large units of one level (d_units / h_units: the
 // level's list, single-CTA units first).  xp is the permuted solution.
+// Value-only refactor of all large units with the stored pivot order (rows
+// already scattered in that order).  Work is queued on sa and sb (forked from
+// and joined back into sa with the two events); zero or non-finite pivots set
+// the reused-pivot status.
+cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cudaStream_t sb, cudaEvent_t ev_a,
+                           cudaEvent_t ev_b, int32_t* launches);
+
 // Forward and backward solves of the large units of one level (two
 // launches).  d_sync holds large_sync_words(p) zeroed words per solve sweep.
 cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, int32_t level, const int32_t* d_units,

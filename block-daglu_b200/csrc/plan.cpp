@@ -192,6 +192,34 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
     p.step_max_rows.push_back(rows);
   }
 
+  // Value-only refactor steps (kRPanel columns).
+  p.rsteps = (max_large + kRPanel - 1) / kRPanel;
+  p.rstep_ptr.assign(static_cast<size_t>(p.rsteps) + 1, 0);
+  for (int32_t st = 0; st < p.rsteps; ++st) {
+    const int32_t k0 = st * kRPanel;
+    int32_t spre = 0, apre = 0, bpre = 0, act = 0;
+    for (int32_t u : p.large_units) {
+      const int32_t m = p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)];
+      if (m <= k0) continue;
+      const int32_t rest = m - k0 - std::min(kRPanel, m - k0);
+      const int32_t chunks = (rest + kRPanel - 1) / kRPanel;
+      const int32_t nti = (rest + kRTileM - 1) / kRTileM, ntj = (rest + kRTileN - 1) / kRTileN;
+      p.rstep_unit.push_back(u);
+      p.rstep_strip_pref.push_back(spre);
+      p.rstep_ga_pref.push_back(apre);
+      p.rstep_gb_pref.push_back(bpre);
+      spre += 2 * chunks;
+      apre += rest > 0 ? nti + ntj - 1 : 0;
+      bpre += rest > 0 ? (nti - 1) * (ntj - 1) : 0;
+      ++act;
+    }
+    p.rstep_ptr[static_cast<size_t>(st) + 1] = static_cast<int32_t>(p.rstep_unit.size());
+    p.rstep_strip_total.push_back(spre);
+    p.rstep_ga_total.push_back(apre);
+    p.rstep_gb_total.push_back(bpre);
+    p.rmax_active = std::max(p.rmax_active, act);
+  }
+
   // Canonical CSR row pointer (original coordinates) for the residual.
   p.csr_ptr.assign(static_cast<size_t>(n) + 1, 0);
   for (size_t k = 0; k < nnz; ++k) p.csr_ptr[static_cast<size_t>(a.row[k]) + 1]++;

@@ -71,6 +71,16 @@ struct Plan {
   std::vector<int32_t> step_gemm_pref;  // exclusive prefix of GEMM tiles
   std::vector<int32_t> step_trsm_total, step_gemm_total;  // per step
   std::vector<int32_t> step_max_rows;                     // per step: largest m - k0
+  // Value-only refactor of large units (stored pivot order, no pivot
+  // search): steps of kRPanel columns.  Per step and active unit: CTA
+  // prefixes of the strip kernel (row chunks then column chunks of kRPanel),
+  // of the update tiles that cover the next step's strips ("a": tile row 0
+  // and tile column 0) and of the remaining tiles ("b").
+  int32_t rsteps = 0;
+  int32_t rmax_active = 0;
+  std::vector<int32_t> rstep_ptr, rstep_unit;
+  std::vector<int32_t> rstep_strip_pref, rstep_ga_pref, rstep_gb_pref;  // per active unit, exclusive
+  std::vector<int32_t> rstep_strip_total, rstep_ga_total, rstep_gb_total;
   // Canonical CSR (original coordinates) for the residual.
   std::vector<int32_t> csr_ptr;
   double factor_flops = 0.0;
@@ -81,6 +91,9 @@ struct Plan {
 constexpr int kPanel = 32;          // panel width of the blocked LU
 constexpr int kTrsmCols = 128;      // columns per CTA in the swap/TRSM kernel
 constexpr int kGemmTile = 128;      // square output tile of the update kernel
+constexpr int kRPanel = 64;         // panel width of the value-only refactor
+constexpr int kRTileM = 128;        // update tile of the value-only refactor: rows
+constexpr int kRTileN = 64;         //   and columns
 constexpr int kSolveTile = 64;      // row tile of the large-unit triangular solves
 
 Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max);
