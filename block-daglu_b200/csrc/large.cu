@@ -640,17 +640,32 @@ constexpr int kPadRow = 72;    // padded 64-entry row: quarter q at offset 18q (
 constexpr int kRAS = kRP + 1;  // As row stride in k_rgemm
 constexpr size_t kRGemmSmem = (static_cast<size_t>(kRTileM) * kRAS + static_cast<size_t>(kRP) * kRTileN) * sizeof(double);
 
+// Reciprocal of a pivot by Newton's iteration from the single-precision
+// estimate (two steps: the relative error squares each step, from about
+// 2^-23 to below one double ulp).  Pivots outside single-precision range
+// take a plain division.
+__device__ __forceinline__ double pivot_rcp(double d) {
+  const double ad = fabs(d);
+  if (!(ad > 1e-30 && ad < 1e30)) return 1.0 / d;
+  double r = static_cast<double>(__frcp_rn(static_cast<float>(d)));
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+}
+
 // LU without pivot search of the 32 x 32 block at (o, o) of D, by one warp:
 // lane i keeps row i in registers; step j takes the pivot row's entries from
-// lane j by shuffle.
-__device__ __forceinline__ void warp_lu32(double* D, int o, int lane) {
+// lane j by shuffle.  Not inlined: the unrolled body is large and is called
+// twice per diagonal block.
+__device__ __noinline__ void warp_lu32(double* D, int o, int lane) {
   double v[kHB];
 #pragma unroll
   for (int c = 0; c < kHB; ++c) v[c] = D[(o + lane) * kRS + o + c];
 #pragma unroll
   for (int j = 0; j < kHB; ++j) {
-    const double piv = __shfl_sync(0xffffffffu, v[j], j);
-    if (lane > j) v[j] = v[j] / piv;
+    const double r = pivot_rcp(__shfl_sync(0xffffffffu, v[j], j));
+    if (lane > j) v[j] *= r;
     const double l = v[j];
 #pragma unroll
     for (int c = j + 1; c < kHB; ++c) {
@@ -691,13 +706,15 @@ __global__ void __launch_bounds__(kRThreads) k_rdiag(DevPlan dp, int32_t k0, int
 #pragma unroll
     for (int r = 0; r < kHB; ++r) D[r * kRS + kHB + lane] = x[r];
   } else if (warp == 1) {
-    // L21 = D21 U11^{-1}: lane = row kHB + lane.
+    // L21 = D21 U11^{-1}: lane = row kHB + lane; the pivot reciprocals are
+    // formed first, off the substitution's dependent chain.
     double x[kHB];
+    const double rdl = 1.0 / D[lane * kRS + lane];
 #pragma unroll
     for (int c = 0; c < kHB; ++c) x[c] = D[(kHB + lane) * kRS + c];
 #pragma unroll
     for (int j = 0; j < kHB; ++j) {
-      x[j] = x[j] / D[j * kRS + j];
+      x[j] *= __shfl_sync(0xffffffffu, rdl, j);
 #pragma unroll
       for (int c = j + 1; c < kHB; ++c) x[c] = fma(-x[j], D[j * kRS + c], x[c]);
     }
