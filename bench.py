@@ -298,13 +298,13 @@ def main():
         achieved = traffic / (ph["solve"] * 1e-3) / 1e9
         peak = peaks.get("hbm_gbs", 6650.0)
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": None, "kernel": "solve sweep (k_solve_scalar/k_solve_dense levels)",
+                    "traffic": None, "kernel": "solve sweep (k_solve_scalar / k_solve_dense / k_trsv_tiles levels)",
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"}
     else:
         achieved = flops_large / (ph["lu_small"] + ph["lu_large"]) / 1e9
         roofline = {"bound": "tensor", "achieved": achieved, "peak": dgemm, "unit": "TFLOP/s",
                     "frac": achieved / dgemm if dgemm else None, "traffic": None,
-                    "kernel": "dense block LU (k_lu_small + k_panel/k_swap_trsm/k_gemm_update), FP64",
+                    "kernel": "dense block LU phases (k_lu_small; value-only refactor k_rdiag / k_rstrip / k_rgemm), FP64",
                     "peak_source": "FP64 pipe: torch.matmul float64 8192^3 measured in this run "
                                    "(MEASURED_PEAKS.json has no FP64 figure)"}
     cpu = None
