@@ -8,6 +8,13 @@ One analyze + first factor (untimed), then steps of one value-only refactor
 (values x (1 + U(-0.1, 0.1)), fresh per step) followed by one 1-RHS solve.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                    [--workload circuit-200k|batch-256]
+
+Workload "batch-256" (independent systems): 256 systems of the 2,000-row
+block generator's kind with n log-uniform in [1,000, 50,000] and n/50 blocks,
+8 right-hand sides U(-1, 1); each step refactors all 256 systems (values
+x (1 + U(-0.1, 0.1))) and solves the 8 right-hand sides of each, through one
+batch (bdlu_batch_*); the metric is systems factored and solved per second.
 
 Prints one JSON line on rank 0.  `value` is device-timed (inputs resident in
 HBM, CUDA events per step on the launching stream, L2 flushed between steps
@@ -36,6 +43,9 @@ METRIC = "refactor+solves/s"
 N_ROWS = 200000
 CONFIG_INDEX = 1
 L2_FLUSH_BYTES = 256 << 20
+BATCH_WORKLOAD = "batch-256"
+BATCH_METRIC = "system factor+solves/s"
+BATCH_SYSTEMS, BATCH_NRHS, BATCH_CONFIG = 256, 8, 2
 
 
 def parse():
@@ -45,6 +55,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, BATCH_WORKLOAD])
     return ap.parse_args()
 
 
@@ -171,11 +182,225 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def batch_systems(count=BATCH_SYSTEMS):
+    """The batch workload's systems: block generator, n log-uniform in [1e3, 5e4]."""
+    import blockdaglu as bd
+    rng = np.random.default_rng(bd.config_seed(BATCH_CONFIG))
+    out = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(1000.0), np.log(50000.0))))
+        out.append(bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(BATCH_CONFIG, i), n))
+    return out
+
+
+def batch_step_inputs(systems, k):
+    """Step k of the batch: every system's values x (1 + U(-0.1, 0.1)), and 8 rhs U(-1, 1)."""
+    vals = np.concatenate([g.perturbed(2_000_003 + 7919 * k + i) for i, g in enumerate(systems)])
+    rng = np.random.default_rng(3_000_017 + k)
+    B = np.asfortranarray(rng.uniform(-1.0, 1.0, (sum(g.n for g in systems), BATCH_NRHS)))
+    return vals, B
+
+
+def batch_cpu_sample(systems, sample=4):
+    """Oracle port on the first `sample` systems (factor + 8-rhs solve), scaled to systems/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import blockdaglu as bd
+    import oracle
+    vals, B = batch_step_inputs(systems[:sample], 0)
+    t_all, off, voff = 0.0, 0, 0
+    for g in systems[:sample]:
+        s = bd.Solver()
+        s.set_option("analysis_only", 1)
+        assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze()
+        d = s.decomposition()
+        v = vals[voff:voff + g.nnz]
+        t0 = time.perf_counter()
+        ref = oracle.System(g.n, g.rows, g.cols, v, d["P"], d["Q"], d["R"])
+        ref.factor()
+        for j in range(BATCH_NRHS):
+            ref.solve(np.ascontiguousarray(B[off:off + g.n, j]))
+        t_all += time.perf_counter() - t0
+        off += g.n
+        voff += g.nnz
+    return {"value": sample / t_all, "unit": BATCH_METRIC, "cores": 1, "kind": "port",
+            "sample": "the first %d systems of the batch (n = %s), each factored and solved for %d rhs by the "
+                      "oracle on one thread: %.2f s" % (sample, [g.n for g in systems[:sample]], BATCH_NRHS, t_all)}
+
+
+def run_batch(args, rank, world):
+    """batch-256: 256 independent systems per step through one bdlu_batch."""
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        systems = batch_systems()
+        base = batch_cpu_sample(systems)
+        line = {"metric": BATCH_METRIC, "value": base["value"], "unit": BATCH_METRIC, "n_gpus": args.gpus,
+                "steps": 1, "warmup": 0, "ms_per_step": 1000.0 * BATCH_SYSTEMS / base["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": BATCH_WORKLOAD, "systems": BATCH_SYSTEMS,
+                                                "nrhs": BATCH_NRHS},
+                "impl": "reference", "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": BATCH_METRIC, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+    import torch
+    import blockdaglu as bd
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    systems = batch_systems()
+    batch = bd.Batch()
+    for g in systems:
+        assert batch.add((g.rows, g.cols, g.vals), g.n) >= 0, batch.last_error_message()
+    t0 = time.perf_counter()
+    assert batch.analyze(), batch.last_error_message()
+    analyze_s = time.perf_counter() - t0
+    assert batch.factor(), batch.last_error_message()
+    first = batch.stats()
+    N = batch.rows()
+    nnz = int(batch.nnz_offset(batch.count()))
+    total = args.warmup + args.steps
+    inputs = [batch_step_inputs(systems, k) for k in range(total)]
+    d_vals = [torch.from_numpy(v).to(dev) for v, _ in inputs]
+    d_B = [torch.from_numpy(np.ascontiguousarray(B.T)).to(dev) for _, B in inputs]  # (nrhs, N): column-major N x nrhs
+    d_X = torch.empty(BATCH_NRHS, N, dtype=torch.float64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    sh = stream.cuda_stream
+
+    def device_step(k):
+        assert batch.refactor_values_device(d_vals[k].data_ptr(), nnz, sh), batch.last_error_message()
+        assert batch.solve_device(d_X.data_ptr(), N, BATCH_NRHS, sh), batch.last_error_message()
+
+    for k in range(args.warmup):
+        d_X.copy_(d_B[k])
+        device_step(k)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms, phases, launches = [], [], []
+    with ClockSampler(local) as clocks:
+        for k in range(args.warmup, total):
+            flush.fill_(float(k))
+            d_X.copy_(d_B[k])
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            device_step(k)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            phases.append(batch.phase_times())
+            st = batch.stats()
+            launches.append(st["factor_launches"] + st["solve_launches"])
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    # Per-system residual of the last timed step (host, FP64).
+    X = d_X.cpu().numpy().T
+    v_last, B_last = inputs[total - 1]
+    import scipy.sparse as sp
+    worst, off, voff = 0.0, 0, 0
+    for g in systems:
+        v = v_last[voff:voff + g.nnz]
+        A = sp.csr_matrix((v, (g.rows, g.cols)), shape=(g.n, g.n))
+        anorm = float(abs(A).sum(axis=1).max())
+        x, b = X[off:off + g.n], B_last[off:off + g.n]
+        R = b - A @ x
+        rel = np.abs(R).max(axis=0) / (anorm * np.abs(x).max(axis=0) + np.abs(b).max(axis=0))
+        worst = max(worst, float(rel.max()))
+        off += g.n
+        voff += g.nnz
+    my_ms = float(sum(step_ms))
+    if dist:
+        t = torch.tensor([my_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        my_ms = float(t.item())
+    ms_per_step = my_ms / args.steps
+    value = world * BATCH_SYSTEMS * 1000.0 / ms_per_step
+    # End to end through the C ABI with host buffers.
+    pin_v = [torch.from_numpy(v).pin_memory() for v, _ in inputs]
+    pin_B = torch.empty(BATCH_NRHS, N, dtype=torch.float64).pin_memory()
+    e2e_ms = []
+    for k in range(total):
+        flush.fill_(float(k))
+        torch.cuda.synchronize()
+        pin_B.copy_(torch.from_numpy(np.ascontiguousarray(inputs[k][1].T)))
+        t0 = time.perf_counter()
+        rc = batch._lib.bdlu_batch_refactor_values(batch._b, bd._p64(pin_v[k].numpy()), nnz)
+        rc = rc or batch._lib.bdlu_batch_solve(batch._b, bd._p64(pin_B.numpy()), N, BATCH_NRHS)
+        dt = (time.perf_counter() - t0) * 1000.0
+        assert rc == 0, batch.last_error_message()
+        if k >= args.warmup:
+            e2e_ms.append(dt)
+    e2e = world * BATCH_SYSTEMS * 1000.0 / statistics.mean(e2e_ms)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    ph = {key: statistics.mean(p[key] for p in phases) for key in phases[0]}
+    peaks = measured_peaks()
+    dominant = max(("lu_small", "lu_large", "solve"), key=lambda key: ph[key])
+    if dominant == "solve":
+        traffic = 8 * first["dense_entries"] + 12 * first["nnz_offdiag"] + 8 * 4 * N * BATCH_NRHS
+        achieved = traffic / (ph["solve"] * 1e-3) / 1e9
+        peak = peaks.get("hbm_gbs", 6650.0)
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": None, "kernel": "solve sweep, 8 rhs (k_solve_scalar / k_solve_dense levels)",
+                    "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"}
+    else:
+        n8 = 8192
+        a = torch.randn(n8, n8, dtype=torch.float64, device=dev)
+        torch.matmul(a, a)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = 1e30
+        for _ in range(3):
+            e0.record()
+            torch.matmul(a, a)
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        dgemm = 2.0 * n8 ** 3 / (best * 1e-3) / 1e12
+        achieved = first["factor_flops"] / (ph["lu_small"] + ph["lu_large"]) / 1e9
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": dgemm, "unit": "TFLOP/s", "frac": achieved / dgemm,
+                    "traffic": None, "kernel": "dense block LU of all systems' blocks (k_lu_small), FP64",
+                    "peak_source": "FP64 pipe: torch.matmul float64 8192^3 measured in this run"}
+    cpu = batch_cpu_sample(systems) if (world == 1 and not args.no_cpu_baseline) else None
+    line = {
+        "metric": BATCH_METRIC, "value": value, "unit": BATCH_METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": BATCH_WORKLOAD, "systems": BATCH_SYSTEMS, "rows": N, "nnz": nnz, "nrhs": BATCH_NRHS,
+                   "nunits": first["nunits"], "max_block": first["max_unit"], "unit_levels": first["unit_levels"],
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "flushed (256 MiB write) between timed steps, outside the step window",
+                   "analyze_s": analyze_s},
+        "e2e": {"value": e2e, "unit": BATCH_METRIC, "h2d_bytes_per_step": 8 * nnz + 8 * N * BATCH_NRHS,
+                "d2h_bytes_per_step": 8 * N * BATCH_NRHS},
+        "phases_ms": ph, "residual_inf_max": worst, "roofline": roofline, "cpu_baseline": cpu,
+        "clocks": clocks.summary(), "gpu_launches": int(sum(launches)),
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == BATCH_WORKLOAD:
+        run_batch(args, rank, world)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

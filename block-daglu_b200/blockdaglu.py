@@ -89,6 +89,21 @@ def load_library(path=LIB_PATH):
         "bdlu_merge_block_boundaries": (ctypes.c_int32, [_i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p]),
         "bdlu_get_decomposition": (ctypes.c_int, [vp, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]),
         "bdlu_get_block_lu": (ctypes.c_int32, [vp, ctypes.c_int32, _f64p, _i32p]),
+        "bdlu_batch_create": (vp, []),
+        "bdlu_batch_destroy": (None, [vp]),
+        "bdlu_batch_add": (ctypes.c_int32, [vp, _i32p, _i32p, _f64p, ctypes.c_int64, ctypes.c_int32]),
+        "bdlu_batch_analyze": (ctypes.c_int, [vp]),
+        "bdlu_batch_factor": (ctypes.c_int, [vp]),
+        "bdlu_batch_refactor_values": (ctypes.c_int, [vp, _f64p, ctypes.c_int64]),
+        "bdlu_batch_refactor_values_device": (ctypes.c_int, [vp, vp, ctypes.c_int64, vp]),
+        "bdlu_batch_solve": (ctypes.c_int, [vp, _f64p, ctypes.c_int32, ctypes.c_int32]),
+        "bdlu_batch_solve_device": (ctypes.c_int, [vp, vp, ctypes.c_int32, ctypes.c_int32, vp]),
+        "bdlu_batch_count": (ctypes.c_int32, [vp]),
+        "bdlu_batch_row_offset": (ctypes.c_int64, [vp, ctypes.c_int32]),
+        "bdlu_batch_nnz_offset": (ctypes.c_int64, [vp, ctypes.c_int32]),
+        "bdlu_batch_last_error": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_int64]),
+        "bdlu_batch_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(Stats)]),
+        "bdlu_batch_phase_times": (ctypes.c_int, [vp, _f64p, ctypes.c_int32]),
         "bdlu_synth_create": (vp, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
         "bdlu_synth_destroy": (None, [vp]),
         "bdlu_synth_n": (ctypes.c_int32, [vp]),
@@ -267,6 +282,98 @@ class Solver:
         v = np.empty(cnt, np.float64)
         fn(self._h, _p32(r), _p32(c), _p64(v), cnt)
         return list(zip(r.tolist(), c.tolist(), v.tolist()))
+
+
+class Batch:
+    """Independent systems factored and solved together (bdlu_batch_*).
+
+    The reference handles one system per Solver; a Batch stands in for a loop
+    of Solvers.  Systems are added (storage only), analysed together as one
+    block-diagonal system, then factored and solved by shared launches.
+    Right-hand sides stack the systems' rows (system k at row_offset(k));
+    value-only refactors stack the systems' canonical values (nnz_offset(k)).
+    """
+
+    def __init__(self):
+        self._lib = load_library()
+        self._b = self._lib.bdlu_batch_create()
+        if not self._b:
+            raise MemoryError("bdlu_batch_create failed")
+        self._keep = []
+
+    def __del__(self):
+        b, self._b = getattr(self, "_b", None), None
+        if b and getattr(self, "_lib", None) is not None:
+            self._lib.bdlu_batch_destroy(b)
+
+    def add(self, coo, n):
+        """Adds a system (COO, dimension n > 0); returns its index, or -1."""
+        r, c, v = _coo_arrays(coo)
+        self._keep.append((r, c, v))
+        k = self._lib.bdlu_batch_add(self._b, _p32(r), _p32(c), _p64(v), len(r), int(n))
+        return k if k >= 0 else -1
+
+    def analyze(self):
+        return self._lib.bdlu_batch_analyze(self._b) == 0
+
+    def factor(self):
+        return self._lib.bdlu_batch_factor(self._b) == 0
+
+    def refactor_values(self, vals):
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        return self._lib.bdlu_batch_refactor_values(self._b, _p64(v), len(v)) == 0
+
+    def refactor_values_device(self, dptr, nnz, stream=0):
+        return self._lib.bdlu_batch_refactor_values_device(self._b, ctypes.c_void_p(dptr), nnz,
+                                                            ctypes.c_void_p(stream)) == 0
+
+    def solve_in_place(self, B):
+        """B: float64 (N,) or Fortran-ordered (N, nrhs), N = row_offset(count)."""
+        if not isinstance(B, np.ndarray) or B.dtype != np.float64:
+            raise TypeError("solve_in_place expects a float64 numpy array")
+        if B.ndim == 1:
+            ldb, nrhs = B.shape[0], 1
+        else:
+            if not B.flags.f_contiguous:
+                raise ValueError("multi-RHS B must be Fortran-ordered (column-major)")
+            ldb, nrhs = B.shape
+        if ldb != self.rows():
+            ldb = -1
+        return self._lib.bdlu_batch_solve(self._b, _p64(B), ldb, nrhs) == 0
+
+    def solve_device(self, dptr, ldb, nrhs, stream=0):
+        return self._lib.bdlu_batch_solve_device(self._b, ctypes.c_void_p(dptr), ldb, nrhs,
+                                                  ctypes.c_void_p(stream)) == 0
+
+    def count(self):
+        return self._lib.bdlu_batch_count(self._b)
+
+    def row_offset(self, k):
+        return self._lib.bdlu_batch_row_offset(self._b, int(k))
+
+    def nnz_offset(self, k):
+        return self._lib.bdlu_batch_nnz_offset(self._b, int(k))
+
+    def rows(self):
+        return self.row_offset(self.count())
+
+    def last_error(self):
+        return SolverError(self._lib.bdlu_batch_last_error(self._b, None, 0))
+
+    def last_error_message(self):
+        buf = ctypes.create_string_buffer(1024)
+        self._lib.bdlu_batch_last_error(self._b, buf, len(buf))
+        return buf.value.decode()
+
+    def stats(self):
+        st = Stats()
+        self._lib.bdlu_batch_get_stats(self._b, ctypes.byref(st))
+        return st.as_dict()
+
+    def phase_times(self):
+        out = np.zeros(5)
+        self._lib.bdlu_batch_phase_times(self._b, _p64(out), 5)
+        return dict(zip(Solver.PHASES, out.tolist()))
 
 
 def btf_order(n, col_ptr, row_ind):

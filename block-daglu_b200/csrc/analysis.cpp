@@ -571,13 +571,16 @@ AnalysisOptions analysis_options_from_env() {
   return o;
 }
 
+double drop_threshold(const AnalysisOptions& opt, int32_t n) {
+  return opt.drop_abs_lt >= 0.0 ? opt.drop_abs_lt : ((n >= 50000) ? 1e-20 : 0.0);
+}
+
 Decomposition build_decomposition(const CanonicalCoo& a, const AnalysisOptions& opt) {
   Decomposition d;
   const int32_t n = a.n;
   d.n = n;
   const size_t nnz = a.row.size();
-  double drop = opt.drop_abs_lt;
-  if (drop < 0.0) drop = (n >= 50000) ? 1e-20 : 0.0;
+  const double drop = drop_threshold(opt, n);
 
   d.P.resize(static_cast<size_t>(n));
   d.Q.resize(static_cast<size_t>(n));
@@ -588,6 +591,17 @@ Decomposition build_decomposition(const CanonicalCoo& a, const AnalysisOptions& 
     d.R_raw = R;
     d.nblocks_raw = 1;
     d.nmatch = n;
+  } else if (opt.btf) {
+    d.P = opt.btf->P;
+    d.Q = opt.btf->Q;
+    R = opt.btf->R;
+    if (static_cast<int32_t>(d.P.size()) != n || static_cast<int32_t>(d.Q.size()) != n || R.size() < 2 ||
+        R.front() != 0 || R.back() != n)
+      throw std::runtime_error("precomputed BTF ordering does not match the matrix");
+    d.nblocks_raw = static_cast<int32_t>(R.size()) - 1;
+    d.nmatch = opt.btf->nmatch;
+    d.R_raw = R;
+    if (opt.merge) R = merge_block_boundaries(R, n, opt.merge_max);
   } else {
     const Csc csc = pattern_csc(a, drop);
     R.assign(static_cast<size_t>(n) + 1, 0);

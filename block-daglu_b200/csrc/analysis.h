@@ -102,12 +102,23 @@ struct Decomposition {
   std::vector<int32_t> level_ptr, level_blocks;  // blocks_by_level, flattened
 };
 
+// A BTF ordering computed elsewhere (for a block-diagonal batch: the
+// systems' orderings, offset and concatenated).  Q is unflipped.
+struct PrecomputedBtf {
+  std::vector<int32_t> P, Q, R;  // R: nblocks + 1 boundaries
+  int32_t nmatch = 0;
+};
+
 struct AnalysisOptions {
   int32_t merge_max = 64;      // BLOCK_MERGE_MAX_SIZE, else DENSE_BLOCK_MAX, else 64
   bool merge = true;           // BLOCK_MERGE
   double drop_abs_lt = -1.0;   // DROP_ABS_LT (negative: auto, 1e-20 iff n >= 50000)
   bool single_block = false;   // global route: one block, identity P/Q
+  const PrecomputedBtf* btf = nullptr;  // used instead of btf_order when set
 };
+
+// The drop threshold build_decomposition applies for options `opt` at size n.
+double drop_threshold(const AnalysisOptions& opt, int32_t n);
 
 // Reads the reference's environment knobs (BLOCKDAGLU_* over USERALGO_*).
 AnalysisOptions analysis_options_from_env();

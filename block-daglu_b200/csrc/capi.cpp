@@ -106,6 +106,49 @@ int upload_values(bdlu_solver* h, const double* vals, bool device, cudaStream_t 
 
 }  // namespace
 
+// Analysis of an already validated canonical matrix under route `mode`
+// (solver.cpp:820-1182): signatures, decomposition, device plan and upload.
+int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf* btf) {
+  h->sig = bdlu::matrix_sig(h->n, h->coo);
+  h->sig2 = bdlu::matrix_sig2(h->n, h->coo);
+  h->value_sig = bdlu::matrix_value_sig(h->coo);
+  h->mode = mode;
+  // The GPU engine runs the block route under AUTO; "klu" forces the global
+  // route, which here means one diagonal block with partial pivoting.
+  h->global_route = (h->mode == BDLU_MODE_KLU);
+  h->decomposed = false;
+  h->factored = false;
+  h->exported = false;
+  try {
+    bdlu::AnalysisOptions opt = bdlu::analysis_options_from_env();
+    opt.single_block = h->global_route;
+    opt.btf = btf;
+    h->dec = bdlu::build_decomposition(h->coo, opt);
+    if (h->analysis_only) {
+      h->engine.reset();
+      h->decomposed = true;
+      return BDLU_OK;
+    }
+    int dev_count = 0;
+    const cudaError_t ce = cudaGetDeviceCount(&dev_count);
+    if (ce != cudaSuccess || dev_count <= 0)
+      return fail(h, BDLU_BACKEND_UNAVAILABLE,
+                  std::string("no CUDA device available: ") + (ce != cudaSuccess ? cudaGetErrorString(ce) : "0 devices"));
+    const bdlu::Plan plan = bdlu::build_plan(h->coo, h->dec, bdlu::small_unit_max());
+    if (!h->engine) h->engine = std::make_unique<bdlu::Engine>();
+    std::string err;
+    if (!h->engine->upload(plan, h->dec, h->coo, err)) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+    // The engine keeps its own value buffer; load the analysed values.
+    if (const int st = upload_values(h, h->coo.val.data(), false, nullptr)) return st;
+  } catch (const std::bad_alloc&) {
+    return fail(h, BDLU_ANALYSIS_FAILED, "out of host memory during analysis");
+  } catch (const std::exception& e) {
+    return fail(h, BDLU_ANALYSIS_FAILED, e.what());
+  }
+  h->decomposed = true;
+  return BDLU_OK;
+}
+
 extern "C" {
 
 bdlu_solver* bdlu_create(void) {
@@ -152,43 +195,7 @@ int bdlu_analyze(bdlu_solver* h) {
   clear_error(h);
   if (!h->prepared) return fail(h, BDLU_NOT_PREPARED, "set_matrix must be called before analyze");
   if (const int st = ensure_validated(h)) return st;
-  h->sig = bdlu::matrix_sig(h->n, h->coo);
-  h->sig2 = bdlu::matrix_sig2(h->n, h->coo);
-  h->value_sig = bdlu::matrix_value_sig(h->coo);
-  h->mode = pick_mode();
-  // The GPU engine runs the block route under AUTO; "klu" forces the global
-  // route, which here means one diagonal block with partial pivoting.
-  h->global_route = (h->mode == BDLU_MODE_KLU);
-  h->decomposed = false;
-  h->factored = false;
-  h->exported = false;
-  try {
-    bdlu::AnalysisOptions opt = bdlu::analysis_options_from_env();
-    opt.single_block = h->global_route;
-    h->dec = bdlu::build_decomposition(h->coo, opt);
-    if (h->analysis_only) {
-      h->engine.reset();
-      h->decomposed = true;
-      return BDLU_OK;
-    }
-    int dev_count = 0;
-    const cudaError_t ce = cudaGetDeviceCount(&dev_count);
-    if (ce != cudaSuccess || dev_count <= 0)
-      return fail(h, BDLU_BACKEND_UNAVAILABLE,
-                  std::string("no CUDA device available: ") + (ce != cudaSuccess ? cudaGetErrorString(ce) : "0 devices"));
-    const bdlu::Plan plan = bdlu::build_plan(h->coo, h->dec, bdlu::small_unit_max());
-    if (!h->engine) h->engine = std::make_unique<bdlu::Engine>();
-    std::string err;
-    if (!h->engine->upload(plan, h->dec, h->coo, err)) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
-    // The engine keeps its own value buffer; load the analysed values.
-    if (const int st = upload_values(h, h->coo.val.data(), false, nullptr)) return st;
-  } catch (const std::bad_alloc&) {
-    return fail(h, BDLU_ANALYSIS_FAILED, "out of host memory during analysis");
-  } catch (const std::exception& e) {
-    return fail(h, BDLU_ANALYSIS_FAILED, e.what());
-  }
-  h->decomposed = true;
-  return BDLU_OK;
+  return bdlu_analyze_validated(h, pick_mode(), nullptr);
 }
 
 int bdlu_factor(bdlu_solver* h) {

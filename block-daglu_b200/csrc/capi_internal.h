@@ -50,6 +50,11 @@ inline int bdlu_fail(bdlu_solver* h, int code, std::string msg) {
   return code;
 }
 
+// Analysis of h->coo (validated and canonical; h->n set) under route `mode`
+// (a bdlu_mode value); btf, if not null, replaces the BTF ordering step.
+// Returns a status code and sets the handle's error.
+int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf* btf);
+
 // Builds the export cache (P, L, U in the engine's factor order); returns a
 // status code and sets the handle's error on failure.
 int bdlu_build_export(bdlu_solver* h);

@@ -154,6 +154,44 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  * Returns BDLU_OK, or BDLU_INVALID_DIMENSION for an unknown key. */
 int bdlu_set_option(bdlu_solver* h, const char* key, double value);
 
+/* ---- Batches of independent systems ---------------------------------------
+ * The reference solves one system per Solver; its callers loop over systems
+ * (one Solver each, apps/benchmark/main.cpp:271-297).  A batch replaces that
+ * loop: the systems are analysed together as one block-diagonal system (the
+ * BTF blocks of each system, DAG levels aligned), so every block of every
+ * system is factored by the same launches and every level of every system is
+ * solved by one launch.  Each system keeps the reference's per-system
+ * semantics: its own validation (errors name the system), canonicalisation
+ * (duplicates summed, zeros dropped) and block decomposition; the block route
+ * is always used.
+ *   bdlu_batch_add: storage only; n > 0 is required; returns the system's
+ *     index, or -(status).
+ *   bdlu_batch_analyze: validates every system and analyses the batch.
+ *   Right-hand sides and solutions: rows row_offset(k) .. row_offset(k+1)-1 of
+ *     each column of B belong to system k (ldb >= row_offset(count)).
+ *   Value-only refactor: the systems' values in their canonical order, back
+ *     to back; system k's start at nnz_offset(k).
+ *   row_offset / nnz_offset take k in 0..count and return -1 before analyze.
+ * Stats, phase times and errors are those of the whole batch; the residual in
+ * the stats is taken over the block-diagonal system. */
+typedef struct bdlu_batch bdlu_batch;
+bdlu_batch* bdlu_batch_create(void);
+void bdlu_batch_destroy(bdlu_batch* b);
+int32_t bdlu_batch_add(bdlu_batch* b, const int32_t* rows, const int32_t* cols, const double* vals, int64_t nnz,
+                       int32_t n);
+int bdlu_batch_analyze(bdlu_batch* b);
+int bdlu_batch_factor(bdlu_batch* b);
+int bdlu_batch_refactor_values(bdlu_batch* b, const double* vals, int64_t nnz);
+int bdlu_batch_refactor_values_device(bdlu_batch* b, const double* d_vals, int64_t nnz, void* stream);
+int bdlu_batch_solve(bdlu_batch* b, double* B, int32_t ldb, int32_t nrhs);
+int bdlu_batch_solve_device(bdlu_batch* b, double* d_B, int32_t ldb, int32_t nrhs, void* stream);
+int32_t bdlu_batch_count(const bdlu_batch* b);
+int64_t bdlu_batch_row_offset(const bdlu_batch* b, int32_t k);
+int64_t bdlu_batch_nnz_offset(const bdlu_batch* b, int32_t k);
+int bdlu_batch_last_error(const bdlu_batch* b, char* buf, int64_t len);
+int bdlu_batch_get_stats(const bdlu_batch* b, bdlu_stats* out);
+int bdlu_batch_phase_times(bdlu_batch* b, double* ms, int32_t cap);
+
 /* ---- Dense batch solve without allocation -----------------------------------
  * No counterpart in the reference.  For callers that must not allocate
  * device memory where they solve (an allocator or memory budget closed after
