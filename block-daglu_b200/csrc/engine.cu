@@ -288,33 +288,72 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* a, double 
   atomicMax(a, static_cast<unsigned long long>(__double_as_longlong(v)));
 }
 
-// R = B - A X (original coordinates), warp per row; norms[4k..4k+3] gather
-// |r|_inf, |b|_inf, |x|_inf, |A|_inf for column k.
-__global__ void k_residual(DevPlan dp, const double* __restrict__ vals, const double* __restrict__ X,
-                           int32_t ldx, const double* __restrict__ B, int32_t ldb, double* __restrict__ R,
-                           int32_t nrhs, unsigned long long* norms) {
-  const int lane = threadIdx.x & 31;
-  const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (r >= dp.n) return;
-  const int p0 = dp.csr_ptr[r], p1 = dp.csr_ptr[r + 1];
-  double arow = 0.0;
-  for (int q = p0 + lane; q < p1; q += 32) arow += fabs(vals[q]);
-  arow = warp_sum(arow);
+// R = B - A X (original coordinates); norms[4k..4k+3] gather |r|_inf, |b|_inf,
+// |x|_inf, |A|_inf for column k.  Four lanes per row (rows hold a few
+// entries), grid-stride over rows; each thread keeps running maxima, reduced
+// per warp and per CTA, so a CTA issues four atomics per column instead of
+// one per row.
+constexpr int kResLanes = 4;
+__global__ void __launch_bounds__(kThreads) k_residual(DevPlan dp, const double* __restrict__ vals,
+                                                        const double* __restrict__ X, int32_t ldx,
+                                                        const double* __restrict__ B, int32_t ldb,
+                                                        double* __restrict__ R, int32_t nrhs,
+                                                        unsigned long long* norms) {
+  __shared__ double red[kThreads / 32][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sub = threadIdx.x & (kResLanes - 1);
+  // The loop runs over the warp's first row so that every lane takes the
+  // same iterations (the shuffles below need the whole warp).
+  const int64_t wbase = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x - lane) / kResLanes;
+  const int64_t groups = static_cast<int64_t>(gridDim.x) * blockDim.x / kResLanes;
   for (int k = 0; k < nrhs; ++k) {
     const double* xk = X + static_cast<size_t>(k) * ldx;
-    double acc = 0.0;
-    for (int q = p0 + lane; q < p1; q += 32) acc = fma(vals[q], xk[dp.csr_col[q]], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) {
-      const double b = B[r + static_cast<size_t>(k) * ldb];
-      const double res = b - acc;
-      if (R) R[r + static_cast<size_t>(k) * dp.n] = res;
-      unsigned long long* nk = norms + 4 * k;
-      atomic_max_nonneg(nk + 0, fabs(res));
-      atomic_max_nonneg(nk + 1, fabs(b));
-      atomic_max_nonneg(nk + 2, fabs(xk[r]));
-      atomic_max_nonneg(nk + 3, arow);
+    double mr = 0.0, mb = 0.0, mx = 0.0, ma = 0.0;
+    for (int64_t base = wbase; base < dp.n; base += groups) {
+      const int64_t r = base + lane / kResLanes;
+      const bool valid = r < dp.n;
+      const int p0 = valid ? dp.csr_ptr[r] : 0, p1 = valid ? dp.csr_ptr[r + 1] : 0;
+      double acc = 0.0, arow = 0.0;
+      for (int q = p0 + sub; q < p1; q += kResLanes) {
+        const double v = vals[q];
+        acc = fma(v, xk[dp.csr_col[q]], acc);
+        arow += fabs(v);
+      }
+#pragma unroll
+      for (int off = kResLanes / 2; off > 0; off >>= 1) {
+        acc += __shfl_xor_sync(0xffffffffu, acc, off, kResLanes);
+        arow += __shfl_xor_sync(0xffffffffu, arow, off, kResLanes);
+      }
+      if (valid && sub == 0) {
+        const double b = B[r + static_cast<size_t>(k) * ldb];
+        const double res = b - acc;
+        if (R) R[r + static_cast<size_t>(k) * dp.n] = res;
+        mr = fmax(mr, fabs(res));
+        mb = fmax(mb, fabs(b));
+        mx = fmax(mx, fabs(xk[r]));
+        ma = fmax(ma, arow);
+      }
     }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, off));
+      mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, off));
+      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, off));
+    }
+    if (lane == 0) {
+      red[warp][0] = mr;
+      red[warp][1] = mb;
+      red[warp][2] = mx;
+      red[warp][3] = ma;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double m = 0.0;
+      for (int w = 0; w < kThreads / 32; ++w) m = fmax(m, red[w][threadIdx.x]);
+      atomic_max_nonneg(norms + 4 * k + threadIdx.x, m);
+    }
+    __syncthreads();
   }
 }
 
@@ -452,11 +491,6 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   BDLU_CUDA(cudaMemset(d.status, 0, 2 * sizeof(int32_t)));
   BDLU_CUDA(cudaMemset(d.piv, 0, static_cast<size_t>(plan.n) * sizeof(int32_t)));
   dp_ = d;
-  smem_small_ = 0;
-  int32_t small_m = 0;
-  for (int32_t u : plan.small_units) small_m = std::max(small_m, plan.ustart[static_cast<size_t>(u) + 1] - plan.ustart[static_cast<size_t>(u)]);
-  smem_small_ = static_cast<size_t>(small_m) * small_m * sizeof(double);
-  smem_solve_ = static_cast<size_t>(small_m) * small_m * sizeof(double);
   {
     // The dynamic shared-memory limit is a per-function process-wide
     // attribute; raise it once to the device maximum so handles of different
@@ -507,11 +541,15 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   BDLU_CUDA(cudaMemsetAsync(d_status_, 0, 2 * sizeof(int32_t), stream));
   BDLU_CUDA(cudaEventRecord(ev_[0], stream));
   const int64_t ncpl = static_cast<int64_t>(p.cpl_col.size());
-  launches_factor_ = 1 + (p.small_units.empty() ? 0 : 1);
+  launches_factor_ = 1 + static_cast<int32_t>(p.small_bucket_m.size());
   k_gather<<<grid_for(std::max<int64_t>(ncpl, p.n), kThreads, num_sms_ * 8), kThreads, 0, stream>>>(dp_, d_vals, ncpl);
   BDLU_CUDA(cudaEventRecord(pev_[0], stream));
-  if (!p.small_units.empty())
-    k_lu_small<<<static_cast<int>(p.small_units.size()), kThreads, smem_small_, stream>>>(dp_, d_vals, small_list_);
+  // One launch per size bucket, shared memory sized to the bucket.
+  for (size_t bkt = 0; bkt < p.small_bucket_m.size(); ++bkt) {
+    const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
+    const size_t mb = static_cast<size_t>(p.small_bucket_m[bkt]);
+    k_lu_small<<<q1 - q0, kThreads, mb * mb * sizeof(double), stream>>>(dp_, d_vals, small_list_ + q0);
+  }
   BDLU_CUDA(cudaEventRecord(pev_[1], stream));
   if (!p.large_units.empty() && reuse) {
     if (!reuse_exec_ || d_vals != d_vals_) {
@@ -607,8 +645,10 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, int32_t nrhs
           dp_, lvl_scalar_ + s0, s1 - s0, rhs, ldr, xp, nrhs);
     }
     if (d1 > d0) ++launches_solve_;
-    if (d1 > d0)
-      k_solve_dense<<<d1 - d0, kThreads, smem_solve_, stream>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp, nrhs);
+    if (d1 > d0) {
+      const size_t mm = static_cast<size_t>(p.lvl_dense_maxm[static_cast<size_t>(l)]);
+      k_solve_dense<<<d1 - d0, kThreads, mm * mm * sizeof(double), stream>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp, nrhs);
+    }
     large_solve_level(dp_, p, l, lvl_large_, lvl_large_tile0_, d_sync_, rhs, ldr, xp, nrhs, stream, &launches_solve_);
   }
 }
@@ -643,7 +683,7 @@ bool Engine::solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_
   const int ug = grid_for(static_cast<int64_t>(n) * nrhs, kThreads, num_sms_ * 16);
   k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 0);
   BDLU_CUDA(cudaEventRecord(pev_[2], stream));
-  const int rg = grid_for(static_cast<int64_t>(n) * 32, kThreads, 1 << 30);
+  const int rg = grid_for(static_cast<int64_t>(n) * kResLanes, kThreads, num_sms_ * 8);
   for (int32_t it = 0; it < refine_iters; ++it) {
     BDLU_CUDA(cudaMemsetAsync(d_norms_, 0, static_cast<size_t>(4 * nrhs) * sizeof(unsigned long long), stream));
     k_residual<<<rg, kThreads, 0, stream>>>(dp_, d_vals_, d_B, ldb, d_b0_, n, d_r_, nrhs, d_norms_);

@@ -132,8 +132,6 @@ class Engine {
   const int32_t* lvl_large_tile0_ = nullptr;
   int32_t* d_sync_ = nullptr;  // tickets and ready flags of the large-unit tile solves
   int32_t sync_words_ = 0;
-  size_t smem_small_ = 0;
-  size_t smem_solve_ = 0;
   int num_sms_ = 148;
   // CUDA graphs of the launch sequences that repeat unchanged: the solve
   // sweep (per nrhs and work buffers) and the refactor of large units with

@@ -54,6 +54,26 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
   }
   p.lu_large_end = off;
   p.lu_size = off;
+  {
+    // Small units by size, cut into buckets at these row counts.
+    auto usz = [&](int32_t u) { return p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)]; };
+    std::stable_sort(p.small_units.begin(), p.small_units.end(), [&](int32_t x, int32_t y) { return usz(x) < usz(y); });
+    static const int32_t kCuts[] = {8, 16, 24, 32, 48, 64, 80, 96, 128};
+    p.small_bucket_ptr.assign(1, 0);
+    size_t q = 0;
+    for (int32_t cut : kCuts) {
+      const size_t q0 = q;
+      while (q < p.small_units.size() && usz(p.small_units[q]) <= cut) ++q;
+      if (q > q0) {
+        p.small_bucket_ptr.push_back(static_cast<int32_t>(q));
+        p.small_bucket_m.push_back(usz(p.small_units[q - 1]));
+      }
+    }
+    if (q < p.small_units.size()) {
+      p.small_bucket_ptr.push_back(static_cast<int32_t>(p.small_units.size()));
+      p.small_bucket_m.push_back(usz(p.small_units.back()));
+    }
+  }
 
   // Split entries into unit-diagonal entries and coupling, canonical order.
   const double drop = [&] {
@@ -153,6 +173,13 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
         p.lvl_large[static_cast<size_t>(ln[static_cast<size_t>(l)]++)] = u;
     }
   }
+  p.lvl_dense_maxm.assign(static_cast<size_t>(nl), 0);
+  for (int32_t l = 0; l < nl; ++l)
+    for (int32_t q = p.lvl_dense_ptr[static_cast<size_t>(l)]; q < p.lvl_dense_ptr[static_cast<size_t>(l) + 1]; ++q) {
+      const int32_t u = p.lvl_dense[static_cast<size_t>(q)];
+      p.lvl_dense_maxm[static_cast<size_t>(l)] =
+          std::max(p.lvl_dense_maxm[static_cast<size_t>(l)], p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)]);
+    }
   // Large units of a level: largest first, so the longest tile chain claims
   // its CTAs first.
   auto usize = [&](int32_t u) { return p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)]; };

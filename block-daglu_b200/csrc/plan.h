@@ -60,7 +60,12 @@ struct Plan {
   // solve's ready-flag arrays.
   std::vector<int32_t> lvl_large_tile0;  // lvl_large.size() + 1
   int32_t large_tiles = 0;
-  std::vector<int32_t> small_units, large_units;
+  std::vector<int32_t> small_units, large_units;  // small units by increasing size
+  // Size buckets of small_units for the factor launches (shared memory per
+  // CTA sized to the bucket's largest unit): small_units[small_bucket_ptr[b]
+  // .. small_bucket_ptr[b+1]) have at most small_bucket_m[b] rows.
+  std::vector<int32_t> small_bucket_ptr, small_bucket_m;
+  std::vector<int32_t> lvl_dense_maxm;  // per level: largest small unit (0 if none)
   // Blocked LU steps for large units (panel width kPanel): per step, the
   // active large units and per-unit CTA prefix sums for the swap/TRSM and
   // GEMM-update kernels.
