@@ -290,68 +290,88 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* a, double 
 
 // R = B - A X (original coordinates); norms[4k..4k+3] gather |r|_inf, |b|_inf,
 // |x|_inf, |A|_inf for column k.  Four lanes per row (rows hold a few
-// entries), grid-stride over rows; each thread keeps running maxima, reduced
-// per warp and per CTA, so a CTA issues four atomics per column instead of
-// one per row.
+// entries), grid-stride over rows, right-hand sides in chunks of kResRhs so
+// each pass reads the matrix once for the chunk; each thread keeps running
+// maxima, reduced per warp and per CTA, so a CTA issues four atomics per
+// column instead of one per row.
 constexpr int kResLanes = 4;
+constexpr int kResRhs = 8;
 __global__ void __launch_bounds__(kThreads) k_residual(DevPlan dp, const double* __restrict__ vals,
                                                         const double* __restrict__ X, int32_t ldx,
                                                         const double* __restrict__ B, int32_t ldb,
                                                         double* __restrict__ R, int32_t nrhs,
                                                         unsigned long long* norms) {
-  __shared__ double red[kThreads / 32][4];
+  __shared__ double red[kThreads / 32][4 * kResRhs];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int sub = threadIdx.x & (kResLanes - 1);
   // The loop runs over the warp's first row so that every lane takes the
   // same iterations (the shuffles below need the whole warp).
   const int64_t wbase = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x - lane) / kResLanes;
   const int64_t groups = static_cast<int64_t>(gridDim.x) * blockDim.x / kResLanes;
-  for (int k = 0; k < nrhs; ++k) {
-    const double* xk = X + static_cast<size_t>(k) * ldx;
-    double mr = 0.0, mb = 0.0, mx = 0.0, ma = 0.0;
+  for (int k0 = 0; k0 < nrhs; k0 += kResRhs) {
+    const int nc = min(kResRhs, nrhs - k0);
+    double mr[kResRhs], mb[kResRhs], mx[kResRhs], ma = 0.0;
+#pragma unroll
+    for (int c = 0; c < kResRhs; ++c) mr[c] = mb[c] = mx[c] = 0.0;
     for (int64_t base = wbase; base < dp.n; base += groups) {
       const int64_t r = base + lane / kResLanes;
       const bool valid = r < dp.n;
       const int p0 = valid ? dp.csr_ptr[r] : 0, p1 = valid ? dp.csr_ptr[r + 1] : 0;
-      double acc = 0.0, arow = 0.0;
+      double acc[kResRhs], arow = 0.0;
+#pragma unroll
+      for (int c = 0; c < kResRhs; ++c) acc[c] = 0.0;
       for (int q = p0 + sub; q < p1; q += kResLanes) {
         const double v = vals[q];
-        acc = fma(v, xk[dp.csr_col[q]], acc);
+        const int col = dp.csr_col[q];
         arow += fabs(v);
+#pragma unroll
+        for (int c = 0; c < kResRhs; ++c)
+          if (c < nc) acc[c] = fma(v, X[col + static_cast<size_t>(k0 + c) * ldx], acc[c]);
       }
 #pragma unroll
       for (int off = kResLanes / 2; off > 0; off >>= 1) {
-        acc += __shfl_xor_sync(0xffffffffu, acc, off, kResLanes);
         arow += __shfl_xor_sync(0xffffffffu, arow, off, kResLanes);
+#pragma unroll
+        for (int c = 0; c < kResRhs; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off, kResLanes);
       }
       if (valid && sub == 0) {
-        const double b = B[r + static_cast<size_t>(k) * ldb];
-        const double res = b - acc;
-        if (R) R[r + static_cast<size_t>(k) * dp.n] = res;
-        mr = fmax(mr, fabs(res));
-        mb = fmax(mb, fabs(b));
-        mx = fmax(mx, fabs(xk[r]));
         ma = fmax(ma, arow);
+#pragma unroll
+        for (int c = 0; c < kResRhs; ++c) {
+          if (c >= nc) continue;
+          const double bv = B[r + static_cast<size_t>(k0 + c) * ldb];
+          const double res = bv - acc[c];
+          if (R) R[r + static_cast<size_t>(k0 + c) * dp.n] = res;
+          mr[c] = fmax(mr[c], fabs(res));
+          mb[c] = fmax(mb[c], fabs(bv));
+          mx[c] = fmax(mx[c], fabs(X[r + static_cast<size_t>(k0 + c) * ldx]));
+        }
       }
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
-      mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, off));
-      mb = fmax(mb, __shfl_xor_sync(0xffffffffu, mb, off));
-      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
       ma = fmax(ma, __shfl_xor_sync(0xffffffffu, ma, off));
+#pragma unroll
+      for (int c = 0; c < kResRhs; ++c) {
+        mr[c] = fmax(mr[c], __shfl_xor_sync(0xffffffffu, mr[c], off));
+        mb[c] = fmax(mb[c], __shfl_xor_sync(0xffffffffu, mb[c], off));
+        mx[c] = fmax(mx[c], __shfl_xor_sync(0xffffffffu, mx[c], off));
+      }
     }
     if (lane == 0) {
-      red[warp][0] = mr;
-      red[warp][1] = mb;
-      red[warp][2] = mx;
-      red[warp][3] = ma;
+#pragma unroll
+      for (int c = 0; c < kResRhs; ++c) {
+        red[warp][4 * c + 0] = mr[c];
+        red[warp][4 * c + 1] = mb[c];
+        red[warp][4 * c + 2] = mx[c];
+        red[warp][4 * c + 3] = ma;
+      }
     }
     __syncthreads();
-    if (threadIdx.x < 4) {
+    if (threadIdx.x < 4 * nc) {
       double m = 0.0;
       for (int w = 0; w < kThreads / 32; ++w) m = fmax(m, red[w][threadIdx.x]);
-      atomic_max_nonneg(norms + 4 * k + threadIdx.x, m);
+      atomic_max_nonneg(norms + 4 * k0 + threadIdx.x, m);
     }
     __syncthreads();
   }
