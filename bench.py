@@ -8,7 +8,16 @@ One analyze + first factor (untimed), then steps of one value-only refactor
 (values x (1 + U(-0.1, 0.1)), fresh per step) followed by one 1-RHS solve.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
-                    [--workload circuit-200k|batch-256]
+                    [--workload circuit-200k|batch-256|serve-64]
+
+Workload "serve-64" (serving): 64 patterns of the circuit generator with n
+log-uniform in [5,000, 300,000]; requests = value-only refactor (values
+x (1 + U(-0.1, 0.1))) + solve of U{1..16} right-hand sides on a uniformly
+drawn pattern; a 150 GB device budget.  Reports the served engine's
+closed-loop throughput (value), an open-loop Poisson stream at --rate
+requests/s for --duration seconds (p50/p99 latency, arrival to result in the
+caller's buffer), and the plain FP64 path on the same requests (one request
+at a time through bdlu_refactor_solve, one Solver per pattern).
 
 Workload "batch-256" (independent systems): 256 systems of the 2,000-row
 block generator's kind with n log-uniform in [1,000, 50,000] and n/50 blocks,
@@ -46,6 +55,9 @@ L2_FLUSH_BYTES = 256 << 20
 BATCH_WORKLOAD = "batch-256"
 BATCH_METRIC = "system factor+solves/s"
 BATCH_SYSTEMS, BATCH_NRHS, BATCH_CONFIG = 256, 8, 2
+SERVE_WORKLOAD = "serve-64"
+SERVE_METRIC = "refactor+solves/s"
+SERVE_PATTERNS, SERVE_CONFIG, SERVE_BUDGET = 64, 4, 150 << 30
 
 
 def parse():
@@ -55,7 +67,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, BATCH_WORKLOAD])
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, BATCH_WORKLOAD, SERVE_WORKLOAD])
+    ap.add_argument("--rate", type=float, default=2000.0, help="serve-64: Poisson arrival rate (requests/s)")
+    ap.add_argument("--duration", type=float, default=5.0, help="serve-64: seconds of open-loop arrivals")
+    ap.add_argument("--slots", type=int, default=8, help="serve-64: concurrent request slots")
     return ap.parse_args()
 
 
@@ -393,6 +408,139 @@ def run_batch(args, rank, world):
         dist.destroy_process_group()
 
 
+def serve_patterns(count=SERVE_PATTERNS):
+    import blockdaglu as bd
+    rng = np.random.default_rng(bd.config_seed(SERVE_CONFIG))
+    sizes = [int(np.exp(rng.uniform(np.log(5000.0), np.log(300000.0)))) for _ in range(count)]
+    return [bd.Synth(bd.FAMILY_CIRCUIT, bd.config_seed(SERVE_CONFIG, i), n) for i, n in enumerate(sizes)]
+
+
+def serve_requests(patterns, count, seed, nvals=3):
+    """count requests: (pattern, values, B); values drawn from nvals perturbations per pattern."""
+    rng = np.random.default_rng(seed)
+    vals = [[g.perturbed(5_000_011 + 131 * i + j) for j in range(nvals)] for i, g in enumerate(patterns)]
+    out = []
+    for r in range(count):
+        k = int(rng.integers(len(patterns)))
+        nrhs = int(rng.integers(1, 17))
+        B = np.asfortranarray(rng.uniform(-1.0, 1.0, (patterns[k].n, nrhs)))
+        out.append((k, vals[k][r % nvals], B))
+    return out
+
+
+def run_serve(args, rank, world):
+    """serve-64: open-loop and closed-loop serving vs the plain FP64 path."""
+    import concurrent.futures as cf
+    import blockdaglu as bd
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "metric": SERVE_METRIC, "unavailable":
+                              "serve-64 has no CPU reference arm; the reference serves one request at a time per "
+                              "Solver (see the circuit-200k reference arm for its per-request cost)"}), flush=True)
+        return
+    if world > 1 and rank != 0:
+        return
+    patterns = serve_patterns()
+    srv = bd.Server(SERVE_BUDGET, args.slots)
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(8) as ex:
+        ids = list(ex.map(lambda g: srv.add_pattern((g.rows, g.cols, g.vals), g.n), patterns))
+    analyze_s = time.perf_counter() - t0
+    assert all(i >= 0 for i in ids), srv.last_error_message()
+    order = {pid: k for k, pid in enumerate(ids)}
+    # Warm-up: two requests per pattern (upload and first factor with
+    # pivoting, then the first value-only refactor, which captures its graph).
+    warm = [(k, patterns[k].vals, np.asfortranarray(np.ones((patterns[k].n, 1))))
+            for _ in range(2) for k in range(len(patterns))]
+    for (k, v, B) in warm:
+        srv.submit(ids[k], v, B)
+    srv.drain()
+    # Closed loop: all requests queued at once (saturation throughput).
+    closed = serve_requests(patterns, max(args.steps, 1) * 64, 11)
+    srv.reset_stats()
+    outs = [B.copy(order="F") for _, _, B in closed]
+    t0 = time.perf_counter()
+    rids = [srv.submit(ids[k], v, X) for (k, v, _), X in zip(closed, outs)]
+    res = [srv.wait(r) for r in rids]
+    closed_s = time.perf_counter() - t0
+    cstats = srv.stats()
+    assert all(r[0] for r in res), srv.last_error_message()
+    worst = max(r[1] for r in res)
+    value = len(closed) / closed_s
+    # Open loop: Poisson arrivals for --duration seconds, at --rate and at
+    # 70 % of the closed-loop throughput (a load the server can sustain).
+    def open_loop(rate, seed):
+        rng = np.random.default_rng(seed)
+        n_open = max(1, int(rate * args.duration))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n_open))
+        opened = serve_requests(patterns, n_open, seed + 1)
+        oouts = [B.copy(order="F") for _, _, B in opened]
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        orids = []
+        for (k, v, _), X, ta in zip(opened, oouts, arrivals):
+            dt = ta - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            orids.append(srv.submit(ids[k], v, X))
+        ores = [srv.wait(r) for r in orids]
+        secs = time.perf_counter() - t0
+        st = srv.stats()
+        assert all(r[0] for r in ores), srv.last_error_message()
+        return {"rate": rate, "requests": n_open, "seconds": secs, "throughput": st["throughput"],
+                "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+                "peak_concurrency": st["peak_concurrency"], "resident_bytes": st["resident_bytes"],
+                "evictions": st["evictions"]}, max(r[1] for r in ores)
+
+    open_spec, w1 = open_loop(args.rate, 17)
+    open_fit, w2 = open_loop(0.7 * value, 23)
+    worst = max(worst, w1, w2)
+    # Plain FP64 path: one request at a time, one Solver per pattern.
+    sample = closed[: min(len(closed), 192)]
+    solvers = {}
+    for k in sorted({k for k, _, _ in sample}):
+        s = bd.Solver()
+        g = patterns[k]
+        assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze() and s.factor(), s.last_error_message()
+        X = np.ones(g.n)
+        assert s.solve_in_place(X)
+        assert s.refactor_values(g.vals) and s.solve_in_place(X), s.last_error_message()
+        solvers[k] = s
+    t0 = time.perf_counter()
+    for k, v, B in sample:
+        X = B.copy(order="F")
+        s = solvers[k]
+        assert s._lib.bdlu_refactor_solve(s._h, bd._p64(v), len(v), bd._p64(X), X.shape[0], X.shape[1]) == 0, \
+            s.last_error_message()
+    plain = len(sample) / (time.perf_counter() - t0)
+    del solvers
+    nrhs_mean = float(np.mean([B.shape[1] for _, _, B in closed]))
+    n_mean = float(np.mean([patterns[k].n for k, _, _ in closed]))
+    nnz_mean = float(np.mean([patterns[k].nnz for k, _, _ in closed]))
+    line = {
+        "metric": SERVE_METRIC, "value": value, "unit": SERVE_METRIC, "n_gpus": 1, "steps": len(closed),
+        "warmup": len(warm), "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": SERVE_WORKLOAD, "patterns": SERVE_PATTERNS, "slots": args.slots,
+                   "budget_bytes": SERVE_BUDGET, "rows_min_max": [min(g.n for g in patterns), max(g.n for g in patterns)],
+                   "analyze_s": analyze_s, "mode": "closed loop (all requests queued), then open loop"},
+        "e2e": {"value": value, "unit": SERVE_METRIC, "h2d_bytes_per_step": int(8 * nnz_mean + 8 * n_mean * nrhs_mean),
+                "d2h_bytes_per_step": int(8 * n_mean * nrhs_mean)},
+        "served_closed_loop": {"requests": len(closed), "seconds": closed_s, "throughput": value,
+                               "p50_ms": cstats["p50_ms"], "p99_ms": cstats["p99_ms"],
+                               "peak_concurrency": cstats["peak_concurrency"]},
+        "served_open_loop": open_spec,
+        "served_open_loop_sustainable": open_fit,
+        "plain_fp64_path": {"requests": len(sample), "throughput": plain, "ratio_served_over_plain": value / plain},
+        "residual_inf_max": worst,
+        "roofline": None,
+        "cpu_baseline": None,
+        "gpu_launches": None,
+    }
+    srv.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -400,6 +548,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == BATCH_WORKLOAD:
         run_batch(args, rank, world)
+        return
+    if args.workload == SERVE_WORKLOAD:
+        run_serve(args, rank, world)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)

@@ -53,6 +53,18 @@ class Stats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("p50_ms", ctypes.c_double),
+        ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+        ("throughput", ctypes.c_double), ("resident_bytes", ctypes.c_int64), ("evictions", ctypes.c_int64),
+        ("peak_concurrency", ctypes.c_int32),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 def load_library(path=LIB_PATH):
     """Loads libbdlu.so (raises if it has not been built)."""
     global _lib
@@ -104,6 +116,18 @@ def load_library(path=LIB_PATH):
         "bdlu_batch_last_error": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_int64]),
         "bdlu_batch_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(Stats)]),
         "bdlu_batch_phase_times": (ctypes.c_int, [vp, _f64p, ctypes.c_int32]),
+        "bdlu_server_create": (vp, [ctypes.c_int64, ctypes.c_int32]),
+        "bdlu_server_destroy": (None, [vp]),
+        "bdlu_server_add_pattern": (ctypes.c_int32, [vp, _i32p, _i32p, _f64p, ctypes.c_int64, ctypes.c_int32]),
+        "bdlu_server_pattern_nnz": (ctypes.c_int64, [vp, ctypes.c_int32]),
+        "bdlu_server_pattern_bytes": (ctypes.c_int64, [vp, ctypes.c_int32]),
+        "bdlu_server_submit": (ctypes.c_int64, [vp, ctypes.c_int32, _f64p, ctypes.c_int64, _f64p, ctypes.c_int32,
+                                                ctypes.c_int32]),
+        "bdlu_server_wait": (ctypes.c_int, [vp, ctypes.c_int64, _f64p, _f64p]),
+        "bdlu_server_drain": (ctypes.c_int, [vp]),
+        "bdlu_server_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
+        "bdlu_server_reset_stats": (ctypes.c_int, [vp]),
+        "bdlu_server_last_error": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_int64]),
         "bdlu_synth_create": (vp, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
         "bdlu_synth_destroy": (None, [vp]),
         "bdlu_synth_n": (ctypes.c_int32, [vp]),
@@ -374,6 +398,90 @@ class Batch:
         out = np.zeros(5)
         self._lib.bdlu_batch_phase_times(self._b, _p64(out), 5)
         return dict(zip(Solver.PHASES, out.tolist()))
+
+
+class Server:
+    """Refactor + solve requests over resident patterns (bdlu_server_*).
+
+    add_pattern analyses a pattern on the host; submit queues a request (new
+    values in the pattern's canonical order, right-hand sides overwritten with
+    the solution) and returns its id; wait blocks for it.  Requests for
+    different patterns run concurrently on the device (continuous batching
+    over `slots` streams); a device-memory budget bounds the resident
+    patterns.  The arrays given to submit are kept alive until wait returns.
+    """
+
+    def __init__(self, memory_budget_bytes, slots=8):
+        self._lib = load_library()
+        self._s = self._lib.bdlu_server_create(int(memory_budget_bytes), int(slots))
+        if not self._s:
+            raise ValueError("bdlu_server_create failed (budget and slots must be positive)")
+        self._keep = {}
+
+    def close(self):
+        s, self._s = getattr(self, "_s", None), None
+        if s and getattr(self, "_lib", None) is not None:
+            self._lib.bdlu_server_destroy(s)
+        self._keep = {}
+
+    def __del__(self):
+        self.close()
+
+    def add_pattern(self, coo, n=-1):
+        """Returns the pattern id, or -1 (see last_error)."""
+        r, c, v = _coo_arrays(coo)
+        k = self._lib.bdlu_server_add_pattern(self._s, _p32(r), _p32(c), _p64(v), len(r), int(n))
+        return k if k >= 0 else -1
+
+    def pattern_nnz(self, pattern):
+        return self._lib.bdlu_server_pattern_nnz(self._s, int(pattern))
+
+    def pattern_bytes(self, pattern):
+        return self._lib.bdlu_server_pattern_bytes(self._s, int(pattern))
+
+    def submit(self, pattern, vals, B):
+        """vals: float64 (pattern_nnz,); B: float64 (n,) or Fortran (n, nrhs), overwritten.  Returns id or -1."""
+        v = np.ascontiguousarray(vals, dtype=np.float64)
+        if not isinstance(B, np.ndarray) or B.dtype != np.float64:
+            raise TypeError("B must be a float64 numpy array")
+        if B.ndim == 1:
+            ldb, nrhs = B.shape[0], 1
+        else:
+            if not B.flags.f_contiguous:
+                raise ValueError("multi-RHS B must be Fortran-ordered (column-major)")
+            ldb, nrhs = B.shape
+        rid = self._lib.bdlu_server_submit(self._s, int(pattern), _p64(v), len(v), _p64(B), ldb, nrhs)
+        if rid < 0:
+            return -1
+        self._keep[rid] = (v, B)
+        return rid
+
+    def wait(self, rid):
+        """Returns (ok, residual, latency_ms)."""
+        res = np.zeros(1)
+        lat = np.zeros(1)
+        st = self._lib.bdlu_server_wait(self._s, int(rid), _p64(res), _p64(lat))
+        self._keep.pop(rid, None)
+        return st == 0, float(res[0]), float(lat[0])
+
+    def drain(self):
+        return self._lib.bdlu_server_drain(self._s) == 0
+
+    def stats(self):
+        st = ServerStats()
+        self._lib.bdlu_server_get_stats(self._s, ctypes.byref(st))
+        return st.as_dict()
+
+    def reset_stats(self):
+        self._lib.bdlu_server_reset_stats(self._s)
+
+    def last_error(self):
+        return SolverError(self._lib.bdlu_server_last_error(self._s, None, 0))
+
+    def last_error_message(self):
+        buf = ctypes.create_string_buffer(1024)
+        self._lib.bdlu_server_last_error(self._s, buf, len(buf))
+        return buf.value.decode()
 
 
 def btf_order(n, col_ptr, row_ind):

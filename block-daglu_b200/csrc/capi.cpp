@@ -149,6 +149,111 @@ int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf*
   return BDLU_OK;
 }
 
+int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream) {
+  if (!h) return BDLU_NOT_PREPARED;
+  clear_error(h);
+  if (!h->decomposed) return fail(h, BDLU_NOT_PREPARED, "analyze must succeed before refactor");
+  if (!h->engine) return fail(h, BDLU_BACKEND_UNAVAILABLE, "analysis was run without a device (analysis_only)");
+  if (!vals || nnz != h->coo.nnz()) return fail(h, BDLU_INVALID_INDEX, "value count does not match the analysed pattern");
+  for (int64_t k = 0; k < nnz; ++k)
+    if (!std::isfinite(vals[k])) return fail(h, BDLU_NON_FINITE_VALUE, "matrix contains NaN or infinity");
+  std::memcpy(h->coo.val.data(), vals, static_cast<size_t>(nnz) * sizeof(double));
+  if (const int st = upload_values(h, vals, false, stream)) return st;
+  return do_factor(h, stream, h->reuse_pivots);
+}
+
+// Device upload of an analysed handle whose engine was released (or never
+// built): plan, tables and values; the next factor pivots in full.
+int bdlu_device_restore(bdlu_solver* h) {
+  if (!h->decomposed) return fail(h, BDLU_NOT_PREPARED, "analyze must succeed before a device upload");
+  if (h->engine) return BDLU_OK;
+  try {
+    const bdlu::Plan plan = bdlu::build_plan(h->coo, h->dec, bdlu::small_unit_max());
+    h->engine = std::make_unique<bdlu::Engine>();
+    std::string err;
+    if (!h->engine->upload(plan, h->dec, h->coo, err)) {
+      h->engine.reset();
+      return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+    }
+    if (const int st = upload_values(h, h->coo.val.data(), false, nullptr)) {
+      h->engine.reset();
+      return st;
+    }
+  } catch (const std::exception& e) {
+    h->engine.reset();
+    return fail(h, BDLU_ANALYSIS_FAILED, e.what());
+  }
+  h->factored = false;
+  h->exported = false;
+  return BDLU_OK;
+}
+
+void bdlu_device_release(bdlu_solver* h) {
+  h->engine.reset();
+  h->factored = false;
+  h->exported = false;
+}
+
+bool bdlu_engine_ready(const bdlu_solver* h) { return h && h->engine != nullptr; }
+
+int64_t bdlu_device_bytes(const bdlu_solver* h) {
+  return (h && h->engine) ? static_cast<int64_t>(h->engine->device_bytes()) : 0;
+}
+
+int bdlu_solve_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream) {
+  if (!h) return BDLU_NOT_PREPARED;
+  clear_error(h);
+  if (!h->factored) return fail(h, BDLU_NOT_PREPARED, "factor must succeed before solve");
+  if (!B || nrhs < 1 || ldb < h->n) return fail(h, BDLU_INVALID_RHS, "right-hand side size does not match matrix dimension");
+  for (int32_t k = 0; k < nrhs; ++k)
+    for (int32_t i = 0; i < h->n; ++i)
+      if (!std::isfinite(B[static_cast<size_t>(k) * ldb + i]))
+        return fail(h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
+  std::string err;
+  double* d_B = h->engine->rhs_buffer(nrhs, err);
+  if (!d_B) return fail(h, BDLU_SOLVE_FAILED, err);
+  cudaError_t e = cudaMemcpy2DAsync(d_B, static_cast<size_t>(h->n) * sizeof(double), B,
+                                    static_cast<size_t>(ldb) * sizeof(double), static_cast<size_t>(h->n) * sizeof(double),
+                                    static_cast<size_t>(nrhs), cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("rhs upload: ") + cudaGetErrorString(e));
+  const int iters = refine_iters_for(h);
+  if (!h->engine->solve_async(d_B, h->n, nrhs, iters, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+  e = cudaMemcpy2DAsync(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
+                        static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToHost, stream);
+  if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
+  bdlu::SolveResidual r{};
+  if (!h->engine->last_residual(stream, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+  auto relres = [](const bdlu::SolveResidual& q) {
+    const double denom = q.a_inf * q.x_inf + q.b_inf;
+    return denom > 0.0 ? q.resid_inf / denom : q.resid_inf;
+  };
+  h->last_residual = relres(r);
+  // A zero pivot met by an earlier device-side refactor surfaces here.  A
+  // refactor that reused the pivot order of large blocks is redone with
+  // pivoting when it hit a zero pivot or when the residual leaves the bound.
+  const int fst = h->engine->factor_status(stream, err);
+  const bool redo = h->engine->last_factor_reused() &&
+                    (fst == 2 || !(h->last_residual <= kReuseResidualLimit));
+  if (fst == 1 || fst < 0 || (fst == 2 && !redo)) {
+    h->factored = false;
+    return fail(h, fst < 0 ? BDLU_BACKEND_UNAVAILABLE : BDLU_FACTORIZATION_FAILED, err);
+  }
+  if (redo) {
+    if (const int st = do_factor(h, stream, false)) return st;
+    if (!h->engine->restore_rhs(d_B, h->n, nrhs, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+    if (!h->engine->solve_async(d_B, h->n, nrhs, iters, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+    e = cudaMemcpy2DAsync(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
+                          static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToHost,
+                          stream);
+    if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
+    if (!h->engine->last_residual(stream, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+    h->last_residual = relres(r);
+  }
+  h->last_refine = iters;
+  if (!std::isfinite(h->last_residual)) return fail(h, BDLU_SOLVE_FAILED, "block solve produced a non-finite solution");
+  return BDLU_OK;
+}
+
 extern "C" {
 
 bdlu_solver* bdlu_create(void) {
@@ -208,16 +313,7 @@ int bdlu_factor(bdlu_solver* h) {
 }
 
 int bdlu_refactor_values(bdlu_solver* h, const double* vals, int64_t nnz) {
-  if (!h) return BDLU_NOT_PREPARED;
-  clear_error(h);
-  if (!h->decomposed) return fail(h, BDLU_NOT_PREPARED, "analyze must succeed before refactor");
-  if (!h->engine) return fail(h, BDLU_BACKEND_UNAVAILABLE, "analysis was run without a device (analysis_only)");
-  if (!vals || nnz != h->coo.nnz()) return fail(h, BDLU_INVALID_INDEX, "value count does not match the analysed pattern");
-  for (int64_t k = 0; k < nnz; ++k)
-    if (!std::isfinite(vals[k])) return fail(h, BDLU_NON_FINITE_VALUE, "matrix contains NaN or infinity");
-  std::memcpy(h->coo.val.data(), vals, static_cast<size_t>(nnz) * sizeof(double));
-  if (const int st = upload_values(h, vals, false, nullptr)) return st;
-  return do_factor(h, nullptr, h->reuse_pivots);
+  return bdlu_refactor_values_on(h, vals, nnz, nullptr);
 }
 
 int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nnz, void* stream) {
@@ -237,57 +333,7 @@ int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nn
   return BDLU_OK;
 }
 
-int bdlu_solve(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs) {
-  if (!h) return BDLU_NOT_PREPARED;
-  clear_error(h);
-  if (!h->factored) return fail(h, BDLU_NOT_PREPARED, "factor must succeed before solve");
-  if (!B || nrhs < 1 || ldb < h->n) return fail(h, BDLU_INVALID_RHS, "right-hand side size does not match matrix dimension");
-  for (int32_t k = 0; k < nrhs; ++k)
-    for (int32_t i = 0; i < h->n; ++i)
-      if (!std::isfinite(B[static_cast<size_t>(k) * ldb + i]))
-        return fail(h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
-  std::string err;
-  double* d_B = h->engine->rhs_buffer(nrhs, err);
-  if (!d_B) return fail(h, BDLU_SOLVE_FAILED, err);
-  cudaError_t e = cudaMemcpy2D(d_B, static_cast<size_t>(h->n) * sizeof(double), B, static_cast<size_t>(ldb) * sizeof(double),
-                               static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("rhs upload: ") + cudaGetErrorString(e));
-  const int iters = refine_iters_for(h);
-  if (!h->engine->solve_async(d_B, h->n, nrhs, iters, nullptr, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-  e = cudaMemcpy2D(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
-                   static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
-  bdlu::SolveResidual r{};
-  if (!h->engine->last_residual(nullptr, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-  auto relres = [](const bdlu::SolveResidual& q) {
-    const double denom = q.a_inf * q.x_inf + q.b_inf;
-    return denom > 0.0 ? q.resid_inf / denom : q.resid_inf;
-  };
-  h->last_residual = relres(r);
-  // A zero pivot met by an earlier device-side refactor surfaces here.  A
-  // refactor that reused the pivot order of large blocks is redone with
-  // pivoting when it hit a zero pivot or when the residual leaves the bound.
-  const int fst = h->engine->factor_status(nullptr, err);
-  const bool redo = h->engine->last_factor_reused() &&
-                    (fst == 2 || !(h->last_residual <= kReuseResidualLimit));
-  if (fst == 1 || fst < 0 || (fst == 2 && !redo)) {
-    h->factored = false;
-    return fail(h, fst < 0 ? BDLU_BACKEND_UNAVAILABLE : BDLU_FACTORIZATION_FAILED, err);
-  }
-  if (redo) {
-    if (const int st = do_factor(h, nullptr, false)) return st;
-    if (!h->engine->restore_rhs(d_B, h->n, nrhs, nullptr, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-    if (!h->engine->solve_async(d_B, h->n, nrhs, iters, nullptr, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-    e = cudaMemcpy2D(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
-                     static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
-    if (!h->engine->last_residual(nullptr, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-    h->last_residual = relres(r);
-  }
-  h->last_refine = iters;
-  if (!std::isfinite(h->last_residual)) return fail(h, BDLU_SOLVE_FAILED, "block solve produced a non-finite solution");
-  return BDLU_OK;
-}
+int bdlu_solve(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs) { return bdlu_solve_on(h, B, ldb, nrhs, nullptr); }
 
 int bdlu_solve_device(bdlu_solver* h, double* d_B, int32_t ldb, int32_t nrhs, void* stream) {
   if (!h) return BDLU_NOT_PREPARED;

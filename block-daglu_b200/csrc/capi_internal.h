@@ -1,6 +1,8 @@
 // Internal state behind the opaque bdlu_solver handle (include/bdlu.h).
 #pragma once
 
+#include <cuda_runtime_api.h>
+
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -54,6 +56,20 @@ inline int bdlu_fail(bdlu_solver* h, int code, std::string msg) {
 // (a bdlu_mode value); btf, if not null, replaces the BTF ordering step.
 // Returns a status code and sets the handle's error.
 int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf* btf);
+
+// Host-buffer refactor and solve on a given stream (the C ABI's host-buffer
+// calls use the legacy default stream).  Same checks, fallbacks and
+// synchronisation as bdlu_refactor_values / bdlu_solve.
+int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream);
+int bdlu_solve_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream);
+
+// Device residency of an analysed handle: release frees every device
+// allocation (the host analysis stays); restore uploads again; bytes is the
+// device memory held now.
+void bdlu_device_release(bdlu_solver* h);
+int bdlu_device_restore(bdlu_solver* h);
+int64_t bdlu_device_bytes(const bdlu_solver* h);
+bool bdlu_engine_ready(const bdlu_solver* h);
 
 // Builds the export cache (P, L, U in the engine's factor order); returns a
 // status code and sets the handle's error on failure.

@@ -32,6 +32,7 @@ namespace bdlu {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int32_t kWorkRhs = 16;
 // ---------------------------------------------------------------------------
 // Value gather for coupling entries and scalar units.
 // ---------------------------------------------------------------------------
@@ -47,6 +48,8 @@ __global__ void k_gather(DevPlan dp, const double* __restrict__ vals, int64_t nc
     if (v == 0.0) report_failure(dp.status, static_cast<int32_t>(r));
   }
 }
+
+__global__ void k_set_i32(int32_t* p, int32_t v) { *p = v; }
 
 // ---------------------------------------------------------------------------
 // Dense LU of one unit in shared memory (column-major, leading dimension m).
@@ -160,7 +163,8 @@ __global__ void k_scatter_large(DevPlan dp, const double* __restrict__ vals, con
 // ---------------------------------------------------------------------------
 __global__ void k_solve_scalar(DevPlan dp, const int32_t* __restrict__ rows, int32_t count,
                                const double* __restrict__ rhs, int32_t ldr, double* __restrict__ xp,
-                               int32_t nrhs) {
+                               const int32_t* __restrict__ nrhs_p) {
+  const int32_t nrhs = *nrhs_p;
   const int lane = threadIdx.x & 31;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= count) return;
@@ -190,7 +194,9 @@ static_assert(32 * kSlots >= 170, "register slots must cover the shared-memory L
 
 __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int32_t* __restrict__ units,
                                                            const double* __restrict__ rhs, int32_t ldr,
-                                                           double* __restrict__ xp, int32_t nrhs) {
+                                                           double* __restrict__ xp,
+                                                           const int32_t* __restrict__ nrhs_p) {
+  const int32_t nrhs = *nrhs_p;
   extern __shared__ double T[];
   const int u = units[blockIdx.x];
   const int s = dp.ustart[u];
@@ -425,13 +431,12 @@ void Engine::drop_graphs() {
   if (reuse_exec_) cudaGraphExecDestroy(reuse_exec_);
   solve_exec_ = nullptr;
   reuse_exec_ = nullptr;
-  solve_exec_nrhs_ = 0;
   solve_exec_b0_ = nullptr;
 }
 
 void Engine::release() {
   drop_graphs();
-  for (void* p : allocs_) cudaFree(p);
+  for (auto& a : allocs_) cudaFree(a.first);
   allocs_.clear();
   d_vals_ = nullptr;
   d_status_ = nullptr;
@@ -451,21 +456,22 @@ void Engine::release() {
   } while (0)
 
 template <class T>
-static bool upload_vec(std::vector<void*>& allocs, const std::vector<T>& v, const T** out, std::string& err) {
+static bool upload_vec(std::vector<std::pair<void*, size_t>>& allocs, const std::vector<T>& v, const T** out, std::string& err) {
   void* p = nullptr;
   const size_t bytes = std::max<size_t>(v.size(), 1) * sizeof(T);
   BDLU_CUDA(cudaMalloc(&p, bytes));
-  allocs.push_back(p);
+  allocs.emplace_back(p, bytes);
   if (!v.empty()) BDLU_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
   *out = static_cast<const T*>(p);
   return true;
 }
 
 template <class T>
-static bool alloc_dev(std::vector<void*>& allocs, size_t count, T** out, std::string& err) {
+static bool alloc_dev(std::vector<std::pair<void*, size_t>>& allocs, size_t count, T** out, std::string& err) {
   void* p = nullptr;
-  BDLU_CUDA(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)));
-  allocs.push_back(p);
+  const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+  BDLU_CUDA(cudaMalloc(&p, bytes));
+  allocs.emplace_back(p, bytes);
   *out = static_cast<T*>(p);
   return true;
 }
@@ -547,6 +553,7 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   lvl_large_tile0_ = tile0;
   sync_words_ = large_sync_words(plan);
   if (!alloc_dev(allocs_, static_cast<size_t>(sync_words_), &d_sync_, err)) return false;
+  if (!alloc_dev(allocs_, 1, &d_nrhs_, err)) return false;
   small_list_ = small_list;
   large_list_ = large_list;
   lvl_scalar_ = lvl_scalar;
@@ -630,12 +637,17 @@ int Engine::factor_status(cudaStream_t stream, std::string& err) {
 
 bool Engine::ensure_work(int32_t nrhs, std::string& err) {
   if (nrhs <= work_nrhs_) return true;
+  // Work space grows to at least kWorkRhs columns at once: a reallocation
+  // (cudaMalloc synchronises the device) and the graphs it invalidates are
+  // paid once for the common right-hand-side counts.
+  nrhs = std::max(nrhs, kWorkRhs);
   const size_t nn = static_cast<size_t>(plan_.n) * static_cast<size_t>(nrhs);
   for (void* q : {static_cast<void*>(d_b0_), static_cast<void*>(d_xp_), static_cast<void*>(d_r_),
                   static_cast<void*>(d_rhs_), static_cast<void*>(d_norms_)}) {
     if (!q) continue;
     cudaFree(q);
-    allocs_.erase(std::remove(allocs_.begin(), allocs_.end(), q), allocs_.end());
+    allocs_.erase(std::remove_if(allocs_.begin(), allocs_.end(), [q](const std::pair<void*, size_t>& a) { return a.first == q; }),
+                  allocs_.end());
   }
   if (!alloc_dev(allocs_, nn, &d_b0_, err)) return false;
   if (!alloc_dev(allocs_, nn, &d_xp_, err)) return false;
@@ -646,12 +658,18 @@ bool Engine::ensure_work(int32_t nrhs, std::string& err) {
   return true;
 }
 
+size_t Engine::device_bytes() const {
+  size_t b = 0;
+  for (const auto& a : allocs_) b += a.second;
+  return b;
+}
+
 double* Engine::rhs_buffer(int32_t nrhs, std::string& err) {
   if (!ensure_work(nrhs, err)) return nullptr;
   return d_rhs_;
 }
 
-void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, int32_t nrhs, cudaStream_t stream) {
+void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_t* nrhs, cudaStream_t stream) {
   const Plan& p = plan_;
   const int32_t nl = p.umax_level + 1;
   if (p.large_tiles > 0) cudaMemsetAsync(d_sync_, 0, static_cast<size_t>(sync_words_) * sizeof(int32_t), stream);
@@ -682,24 +700,26 @@ bool Engine::solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_
   BDLU_CUDA(cudaMemcpy2DAsync(d_b0_, static_cast<size_t>(n) * sizeof(double), d_B,
                               static_cast<size_t>(ldb) * sizeof(double), static_cast<size_t>(n) * sizeof(double),
                               static_cast<size_t>(nrhs), cudaMemcpyDeviceToDevice, stream));
-  if (!solve_exec_ || solve_exec_nrhs_ != nrhs || solve_exec_b0_ != d_b0_) {
+  // The sweep's kernels read the right-hand-side count from d_nrhs_, so one
+  // graph (captured on the current work buffers) serves every count.
+  k_set_i32<<<1, 1, 0, stream>>>(d_nrhs_, nrhs);
+  if (!solve_exec_ || solve_exec_b0_ != d_b0_) {
     if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
     solve_exec_ = nullptr;
     const int32_t saved = launches_solve_;
     BDLU_CUDA(cudaStreamBeginCapture(cap_stream_, cudaStreamCaptureModeThreadLocal));
-    solve_core(d_b0_, n, d_xp_, nrhs, cap_stream_);
+    solve_core(d_b0_, n, d_xp_, d_nrhs_, cap_stream_);
     cudaGraph_t g = nullptr;
     BDLU_CUDA(cudaStreamEndCapture(cap_stream_, &g));
     const cudaError_t ie = cudaGraphInstantiate(&solve_exec_, g, 0);
     cudaGraphDestroy(g);
     BDLU_CUDA(ie);
-    solve_core_launches_ = launches_solve_ - saved;
+    solve_exec_launches_ = launches_solve_ - saved;
     launches_solve_ = saved;
-    solve_exec_nrhs_ = nrhs;
     solve_exec_b0_ = d_b0_;
   }
   BDLU_CUDA(cudaGraphLaunch(solve_exec_, stream));
-  launches_solve_ += solve_core_launches_;
+  launches_solve_ += solve_exec_launches_ + 1;
   const int ug = grid_for(static_cast<int64_t>(n) * nrhs, kThreads, num_sms_ * 16);
   k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 0);
   BDLU_CUDA(cudaEventRecord(pev_[2], stream));
@@ -707,7 +727,7 @@ bool Engine::solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_
   for (int32_t it = 0; it < refine_iters; ++it) {
     BDLU_CUDA(cudaMemsetAsync(d_norms_, 0, static_cast<size_t>(4 * nrhs) * sizeof(unsigned long long), stream));
     k_residual<<<rg, kThreads, 0, stream>>>(dp_, d_vals_, d_B, ldb, d_b0_, n, d_r_, nrhs, d_norms_);
-    solve_core(d_r_, n, d_xp_, nrhs, stream);
+    solve_core(d_r_, n, d_xp_, d_nrhs_, stream);
     k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 1);
   }
   BDLU_CUDA(cudaMemsetAsync(d_norms_, 0, static_cast<size_t>(4 * nrhs) * sizeof(unsigned long long), stream));

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "plan.h"
@@ -63,6 +64,9 @@ class Engine {
   // Returns false and sets `err` on a CUDA error.
   bool upload(const Plan& plan, const Decomposition& dec, const CanonicalCoo& a, std::string& err);
 
+  // Device bytes held by this engine (plan tables, LU arena, values, work).
+  size_t device_bytes() const;
+
   // Enqueues the numeric factor of every unit from canonical-order values
   // already on the device (d_vals, nnz entries).  reuse_pivots: large units
   // keep the row order of the last full factorisation (no pivot search);
@@ -104,11 +108,11 @@ class Engine {
  private:
   void release();
   bool ensure_work(int32_t nrhs, std::string& err);
-  void solve_core(const double* rhs, int32_t ldr, double* xp, int32_t nrhs, cudaStream_t stream);
+  void solve_core(const double* rhs, int32_t ldr, double* xp, const int32_t* nrhs, cudaStream_t stream);
 
   Plan plan_;
   DevPlan dp_{};
-  std::vector<void*> allocs_;
+  std::vector<std::pair<void*, size_t>> allocs_;  // device allocations and their bytes
   double* d_vals_ = nullptr;
   int32_t* d_status_ = nullptr;
   // Solve work space, grown to the largest nrhs seen.
@@ -140,12 +144,13 @@ class Engine {
   cudaStream_t cap_stream_ = nullptr;
   cudaStream_t cap_stream2_ = nullptr;  // second branch of the refactor graph
   cudaEvent_t fork_ev_[2] = {nullptr, nullptr};
+  // Solve-sweep graph, valid for the work buffers it was captured on.
   cudaGraphExec_t solve_exec_ = nullptr;
-  int32_t solve_exec_nrhs_ = 0;
+  int32_t solve_exec_launches_ = 0;
   const double* solve_exec_b0_ = nullptr;
+  int32_t* d_nrhs_ = nullptr;  // right-hand-side count read by the sweep's kernels
   cudaGraphExec_t reuse_exec_ = nullptr;
   int32_t reuse_launches_ = 0;
-  int32_t solve_core_launches_ = 0;
   void drop_graphs();
   bool have_pivots_ = false;  // a full factorisation of this pattern succeeded
   bool last_reuse_ = false;

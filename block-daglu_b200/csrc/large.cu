@@ -479,7 +479,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_trsv_tiles(DevPlan dp, const 
                                                               const int32_t* __restrict__ tile0, int32_t count,
                                                               int32_t* ticket, int32_t* ready,
                                                               const double* __restrict__ rhs, int32_t ldr,
-                                                              double* __restrict__ xp, int32_t nrhs) {
+                                                              double* __restrict__ xp,
+                                                              const int32_t* __restrict__ nrhs_p) {
+  const int32_t nrhs = *nrhs_p;
   __shared__ double Ts[kTile * kTS];  // factor block; also the partial-sum exchange
   __shared__ double xs[kTile * kRC];  // this tile's unknowns [i * kRC + c]
   __shared__ double xj[kTile * kRC];  // finished tile's unknowns
@@ -1025,7 +1027,7 @@ cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cu
 
 cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, int32_t level, const int32_t* d_units,
                               const int32_t* d_tile0, int32_t* d_sync, const double* rhs, int32_t ldr, double* xp,
-                              int32_t nrhs, cudaStream_t stream, int32_t* launches) {
+                              const int32_t* nrhs, cudaStream_t stream, int32_t* launches) {
   const int32_t g0 = p.lvl_large_ptr[static_cast<size_t>(level)];
   const int32_t g1 = p.lvl_large_ptr[static_cast<size_t>(level) + 1];
   if (g1 <= g0) return cudaSuccess;

@@ -35,10 +35,11 @@ cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cu
                            cudaEvent_t ev_b, int32_t* launches);
 
 // Forward and backward solves of the large units of one level (two
-// launches).  d_sync holds large_sync_words(p) zeroed words per solve sweep.
+// launches).  d_sync holds large_sync_words(p) zeroed words per solve sweep;
+// nrhs points to the right-hand-side count in device memory.
 cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, int32_t level, const int32_t* d_units,
                               const int32_t* d_tile0, int32_t* d_sync, const double* rhs, int32_t ldr, double* xp,
-                              int32_t nrhs, cudaStream_t stream, int32_t* launches);
+                              const int32_t* nrhs, cudaStream_t stream, int32_t* launches);
 
 int32_t large_sync_words(const Plan& p);
 

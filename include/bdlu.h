@@ -192,6 +192,62 @@ int bdlu_batch_last_error(const bdlu_batch* b, char* buf, int64_t len);
 int bdlu_batch_get_stats(const bdlu_batch* b, bdlu_stats* out);
 int bdlu_batch_phase_times(bdlu_batch* b, double* ms, int32_t cap);
 
+/* ---- Serving: refactor + solve requests over resident patterns -------------
+ * The reference serves one request at a time per Solver.  A server keeps many
+ * patterns (each analysed once on the host when added; plan, factors and work
+ * space on the device while resident) and runs value-only refactor + solve
+ * requests with continuous batching: `slots` workers, each with its own CUDA
+ * stream, take the oldest queued request whose pattern is not being served,
+ * so requests for different patterns overlap on the device and requests for
+ * one pattern run in arrival order.  A pattern is uploaded when a request for
+ * it is admitted; if the device-memory budget would be exceeded, idle
+ * resident patterns are released, least recently used first, and a request
+ * waits while busy patterns hold the memory.  A pattern that cannot fit even
+ * alone fails its requests with BDLU_BACKEND_UNAVAILABLE.  Each request runs
+ * exactly what bdlu_refactor_solve runs (same checks, pivot-order reuse and
+ * fallback, residual), so its result does not depend on what else is served.
+ *   add_pattern: COO + n (>= 0, or -1 to infer); host analysis; returns the
+ *     pattern id or -(status).  Values per request: pattern_nnz(id), in the
+ *     canonical order.
+ *   submit: vals (pattern_nnz values) and B (ldb >= n, nrhs columns) are
+ *     read and B overwritten with X by a worker; both must stay valid until
+ *     bdlu_server_wait returns for the request.  Returns a request id or
+ *     -(status).
+ *   wait: blocks until the request is done; returns its status and, if the
+ *     pointers are not NULL, its relative residual and latency (submit to
+ *     result in B, ms).
+ *   get_stats: latency percentiles and throughput over completed requests
+ *     since creation or the last reset_stats.
+ *   destroy: finishes queued requests first. */
+typedef struct bdlu_server bdlu_server;
+typedef struct bdlu_server_stats {
+  int64_t completed;
+  int64_t failed;
+  double p50_ms;
+  double p99_ms;
+  double mean_ms;
+  double max_ms;
+  double throughput;        /* completed requests per second, first submit to last completion */
+  int64_t resident_bytes;   /* device bytes of resident patterns (estimates for ones being uploaded) */
+  int64_t evictions;        /* patterns released to admit others */
+  int32_t peak_concurrency; /* most requests running at once */
+} bdlu_server_stats;
+bdlu_server* bdlu_server_create(int64_t memory_budget_bytes, int32_t slots);
+void bdlu_server_destroy(bdlu_server* s);
+int32_t bdlu_server_add_pattern(bdlu_server* s, const int32_t* rows, const int32_t* cols, const double* vals,
+                                int64_t nnz, int32_t n);
+int64_t bdlu_server_pattern_nnz(bdlu_server* s, int32_t pattern);
+/* Device bytes the pattern takes: measured once it has been resident, an
+ * estimate from its plan before. */
+int64_t bdlu_server_pattern_bytes(bdlu_server* s, int32_t pattern);
+int64_t bdlu_server_submit(bdlu_server* s, int32_t pattern, const double* vals, int64_t nnz, double* B, int32_t ldb,
+                           int32_t nrhs);
+int bdlu_server_wait(bdlu_server* s, int64_t request, double* residual, double* latency_ms);
+int bdlu_server_drain(bdlu_server* s);
+int bdlu_server_get_stats(bdlu_server* s, bdlu_server_stats* out);
+int bdlu_server_reset_stats(bdlu_server* s);
+int bdlu_server_last_error(const bdlu_server* s, char* buf, int64_t len);
+
 /* ---- Dense batch solve without allocation -----------------------------------
  * No counterpart in the reference.  For callers that must not allocate
  * device memory where they solve (an allocator or memory budget closed after
