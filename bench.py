@@ -8,7 +8,16 @@ One analyze + first factor (untimed), then steps of one value-only refactor
 (values x (1 + U(-0.1, 0.1)), fresh per step) followed by one 1-RHS solve.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
-                    [--workload circuit-200k|batch-256|serve-64]
+                    [--workload circuit-200k|batch-256|serve-64|precision-200]
+
+Workload "precision-200" (precision): 200 irreducible blocks of U{2000..8000}
+rows with ~20 entries per row plus Pareto-sized small blocks (about 10 % of
+the rows), a geometric row ramp giving block condition numbers near kappa;
+instance a kappa = 1e4, instance b kappa = 1e8; 16 right-hand sides U(-1, 1).
+Per instance: one full factorisation with pivoting + 16-rhs solve on the FP64
+route and on the mixed route (TF32 tensor-core trailing updates, FP64
+refinement to <= 1e-12, precision ladder); reports time, refinement steps,
+the level used and the mixed solution's error against the FP64 one.
 
 Workload "serve-64" (serving): 64 patterns of the circuit generator with n
 log-uniform in [5,000, 300,000]; requests = value-only refactor (values
@@ -58,6 +67,9 @@ BATCH_SYSTEMS, BATCH_NRHS, BATCH_CONFIG = 256, 8, 2
 SERVE_WORKLOAD = "serve-64"
 SERVE_METRIC = "refactor+solves/s"
 SERVE_PATTERNS, SERVE_CONFIG, SERVE_BUDGET = 64, 4, 150 << 30
+PREC_WORKLOAD = "precision-200"
+PREC_METRIC = "factor+16-rhs solves/s"
+PREC_BLOCKS, PREC_CONFIG, PREC_NRHS = 200, 3, 16
 
 
 def parse():
@@ -67,7 +79,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, BATCH_WORKLOAD, SERVE_WORKLOAD])
+    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, BATCH_WORKLOAD, SERVE_WORKLOAD, PREC_WORKLOAD])
+    ap.add_argument("--blocks", type=int, default=PREC_BLOCKS, help="precision-200: number of large blocks")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve-64: Poisson arrival rate (requests/s)")
     ap.add_argument("--duration", type=float, default=5.0, help="serve-64: seconds of open-loop arrivals")
     ap.add_argument("--slots", type=int, default=8, help="serve-64: concurrent request slots")
@@ -541,6 +554,72 @@ def run_serve(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_precision(args, rank, world):
+    """precision-200: FP64 route vs mixed route, kappa 1e4 and 1e8."""
+    import blockdaglu as bd
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "metric": PREC_METRIC, "unavailable":
+                              "precision-200 needs about 45 GB of dense FP64 factors; the single-thread oracle port "
+                              "would take hours (see the circuit-200k reference arm)"}), flush=True)
+        return
+    if world > 1 and rank != 0:
+        return
+    out = {}
+    for label, kexp in (("a", 4), ("b", 8)):
+        g = bd.Synth(bd.FAMILY_PRECISION, bd.config_seed(PREC_CONFIG, kexp), args.blocks, kexp)
+        rng = np.random.default_rng(kexp)
+        B = np.asfortranarray(rng.uniform(-1.0, 1.0, (g.n, PREC_NRHS)))
+        res = {"n": g.n, "nnz": int(g.nnz)}
+        X64 = None
+        for mode in (0, 1):
+            s = bd.Solver()
+            s.set_option("precision", mode)
+            s.set_option("refactor_pivoting", 1)   # every factorisation searches pivots
+            t0 = time.perf_counter()
+            assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze(), s.last_error_message()
+            analyze_s = time.perf_counter() - t0
+            assert s.factor(), s.last_error_message()   # warm-up (upload, first launch of every kernel)
+            steps = []
+            for k in range(max(1, min(args.steps, 2))):
+                v = g.perturbed(900 + k)
+                X = B.copy(order="F")
+                t0 = time.perf_counter()
+                assert s.refactor_values(v), s.last_error_message()
+                tf = time.perf_counter() - t0
+                assert s.solve_in_place(X), s.last_error_message()
+                steps.append((time.perf_counter() - t0, tf))
+            st = s.stats()
+            ph = s.phase_times()
+            key = "fp64" if mode == 0 else "mixed"
+            res[key] = {"seconds_per_step": statistics.mean(t for t, _ in steps),
+                        "factor_seconds": statistics.mean(f for _, f in steps),
+                        "residual_inf": st["residual_inf"], "refine_iters": st["refine_iters"],
+                        "precision_level": {0: "fp64", 1: "tf32", 2: "3xtf32"}[st["precision"]],
+                        "factor_flops": st["factor_flops"], "max_block": st["max_unit"], "analyze_s": analyze_s,
+                        "last_phases_ms": ph}
+            if mode == 0:
+                X64 = X.copy()
+            else:
+                res["mixed"]["error_vs_fp64"] = float(np.max(np.abs(X - X64)) / np.max(np.abs(X64)))
+            del s
+        res["speedup_mixed_over_fp64"] = res["fp64"]["seconds_per_step"] / res["mixed"]["seconds_per_step"]
+        out[label] = res
+        del g
+    a = out["a"]
+    value = 1.0 / a["mixed"]["seconds_per_step"]
+    line = {"metric": PREC_METRIC, "value": value, "unit": PREC_METRIC, "n_gpus": 1, "steps": max(1, min(args.steps, 2)),
+            "warmup": 1, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64 storage, tf32 tensor-core updates, f64 refinement", "data": "synthetic",
+            "config": {"workload": PREC_WORKLOAD, "blocks": args.blocks, "nrhs": PREC_NRHS,
+                       "value_from": "instance a (kappa 1e4), mixed route, host buffers"},
+            "instances": out, "roofline": None, "cpu_baseline": None, "gpu_launches": None}
+    flops = a["mixed"]["factor_flops"]
+    line["tensor_update_tflops"] = flops / a["mixed"]["factor_seconds"] / 1e12
+    line["fp64_update_tflops"] = flops / a["fp64"]["factor_seconds"] / 1e12
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -551,6 +630,9 @@ def main():
         return
     if args.workload == SERVE_WORKLOAD:
         run_serve(args, rank, world)
+        return
+    if args.workload == PREC_WORKLOAD:
+        run_precision(args, rank, world)
         return
     if args.impl == "reference":
         run_reference(args, rank, world)

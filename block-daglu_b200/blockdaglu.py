@@ -47,6 +47,7 @@ class Stats(ctypes.Structure):
         ("nnz", ctypes.c_int64), ("nnz_offdiag", ctypes.c_int64), ("dense_entries", ctypes.c_int64),
         ("factor_flops", ctypes.c_double), ("residual_inf", ctypes.c_double),
         ("last_factor_ms", ctypes.c_double), ("last_solve_ms", ctypes.c_double),
+        ("precision", ctypes.c_int32),
     ]
 
     def as_dict(self):

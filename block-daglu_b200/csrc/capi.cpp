@@ -78,6 +78,7 @@ int ensure_validated(bdlu_solver* h) {
 // met that way falls back to a factorisation with pivoting.
 int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   std::string err;
+  h->engine->set_precision(h->mixed ? h->prec_level : 0);
   for (int attempt = 0; attempt < 2; ++attempt) {
     const bool r = reuse && attempt == 0;
     if (!h->engine->factor_async(h->engine->values_buffer(), stream, err, r))
@@ -217,39 +218,73 @@ int bdlu_solve_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStre
                                     static_cast<size_t>(nrhs), cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("rhs upload: ") + cudaGetErrorString(e));
   const int iters = refine_iters_for(h);
-  if (!h->engine->solve_async(d_B, h->n, nrhs, iters, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-  e = cudaMemcpy2DAsync(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
-                        static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToHost, stream);
-  if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
-  bdlu::SolveResidual r{};
-  if (!h->engine->last_residual(stream, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
   auto relres = [](const bdlu::SolveResidual& q) {
     const double denom = q.a_inf * q.x_inf + q.b_inf;
     return denom > 0.0 ? q.resid_inf / denom : q.resid_inf;
   };
-  h->last_residual = relres(r);
-  // A zero pivot met by an earlier device-side refactor surfaces here.  A
-  // refactor that reused the pivot order of large blocks is redone with
-  // pivoting when it hit a zero pivot or when the residual leaves the bound.
-  const int fst = h->engine->factor_status(stream, err);
-  const bool redo = h->engine->last_factor_reused() &&
-                    (fst == 2 || !(h->last_residual <= kReuseResidualLimit));
-  if (fst == 1 || fst < 0 || (fst == 2 && !redo)) {
+  bdlu::SolveResidual r{};
+  // Solve from the stored right-hand sides and read the residual.
+  auto solve_once = [&]() -> int {
+    if (!h->engine->solve_async(d_B, h->n, nrhs, iters, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+    if (!h->engine->last_residual(stream, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+    h->last_residual = relres(r);
+    return BDLU_OK;
+  };
+  auto redo_factor = [&]() -> int {
+    if (const int st = do_factor(h, stream, false)) return st;
+    if (!h->engine->restore_rhs(d_B, h->n, nrhs, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+    return BDLU_OK;
+  };
+  if (const int st = solve_once()) return st;
+  // A zero pivot met by an earlier device-side refactor surfaces here; a
+  // refactor that reused the pivot order of large blocks is then redone with
+  // pivoting.
+  int fst = h->engine->factor_status(stream, err);
+  if (fst == 1 || fst < 0 || (fst == 2 && !h->engine->last_factor_reused())) {
     h->factored = false;
     return fail(h, fst < 0 ? BDLU_BACKEND_UNAVAILABLE : BDLU_FACTORIZATION_FAILED, err);
   }
-  if (redo) {
-    if (const int st = do_factor(h, stream, false)) return st;
-    if (!h->engine->restore_rhs(d_B, h->n, nrhs, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-    if (!h->engine->solve_async(d_B, h->n, nrhs, iters, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-    e = cudaMemcpy2DAsync(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
-                          static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToHost,
-                          stream);
-    if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
-    if (!h->engine->last_residual(stream, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-    h->last_residual = relres(r);
+  if (fst == 2) {
+    if (const int st = redo_factor()) return st;
+    if (const int st = solve_once()) return st;
   }
-  h->last_refine = iters;
+  int32_t steps = 0;
+  if (h->mixed) {
+    // Mixed route: FP64 refinement until the residual bound; a level whose
+    // refinement stagnates (less than a halving per step after two steps, or
+    // kMaxRefine steps) is replaced by the next one (TF32 -> 3xTF32 -> FP64)
+    // for this and later factorisations, and the system is factored again.
+    constexpr int kMaxRefine = 30;
+    while (true) {
+      double prev = h->last_residual;
+      int k = 0;
+      while (!(h->last_residual <= kReuseResidualLimit) && k < kMaxRefine) {
+        if (!h->engine->refine_async(d_B, h->n, nrhs, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+        if (!h->engine->last_residual(stream, r, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+        h->last_residual = relres(r);
+        ++k;
+        if (k >= 2 && !(h->last_residual < 0.5 * prev)) break;
+        prev = h->last_residual;
+      }
+      steps += k;
+      if (h->last_residual <= kReuseResidualLimit || h->prec_level == 0) break;
+      h->prec_level = (h->prec_level == 1) ? 2 : 0;
+      if (const int st = do_factor(h, stream, h->engine->last_factor_reused())) return st;
+      if (!h->engine->restore_rhs(d_B, h->n, nrhs, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+      if (const int st = solve_once()) return st;
+    }
+  }
+  // A refactor that reused the pivot order and still misses the bound is
+  // redone with pivoting.
+  if (h->engine->last_factor_reused() && !(h->last_residual <= kReuseResidualLimit)) {
+    if (const int st = redo_factor()) return st;
+    if (const int st = solve_once()) return st;
+  }
+  e = cudaMemcpy2DAsync(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
+                        static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
+  h->last_refine = iters + steps;
   if (!std::isfinite(h->last_residual)) return fail(h, BDLU_SOLVE_FAILED, "block solve produced a non-finite solution");
   return BDLU_OK;
 }
@@ -386,6 +421,7 @@ int bdlu_get_stats(const bdlu_solver* h, bdlu_stats* out) {
   for (int32_t b = 0; b < h->dec.nblocks; ++b) out->max_block = std::max(out->max_block, h->dec.R[static_cast<size_t>(b) + 1] - h->dec.R[static_cast<size_t>(b)]);
   out->nnz_offdiag = h->dec.off_ptr.empty() ? 0 : h->dec.off_ptr.back();
   out->refine_iters = h->last_refine;
+  out->precision = h->engine ? h->engine->precision() : 0;
   out->residual_inf = h->last_residual;
   if (h->engine) {
     auto* e = const_cast<bdlu::Engine*>(h->engine.get());
@@ -423,6 +459,15 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
   }
   if (k == "analysis_only") {
     h->analysis_only = value != 0.0;
+    return BDLU_OK;
+  }
+  if (k == "precision") {
+    // 0: FP64 throughout; 1: mixed (tensor-core trailing updates of large
+    // blocks, FP64 refinement, ladder TF32 -> 3xTF32 -> FP64).  Takes effect
+    // at the next factor; switching restarts the ladder at TF32.
+    if (value != 0.0 && value != 1.0) return BDLU_INVALID_DIMENSION;
+    h->mixed = value == 1.0;
+    h->prec_level = 1;
     return BDLU_OK;
   }
   return BDLU_INVALID_DIMENSION;

@@ -32,6 +32,8 @@ struct bdlu_solver {
   int32_t refine_iters = -1;  // -1: REFINE_ITERS env, else 0
   bool analysis_only = false; // host analysis without device upload (inspection, CPU tests)
   bool reuse_pivots = true;   // value-only refactors keep the pivot order of large blocks
+  bool mixed = false;         // "precision" = 1: tensor-core updates + FP64 refinement
+  int32_t prec_level = 1;     // mixed route's current level: 1 TF32, 2 3xTF32, 0 FP64 (sticky)
   // Error state (solver.h:122-123).
   int last_error = BDLU_OK;
   std::string last_message;

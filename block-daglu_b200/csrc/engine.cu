@@ -579,6 +579,10 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   }
   BDLU_CUDA(cudaEventRecord(pev_[1], stream));
   if (!p.large_units.empty() && reuse) {
+    if (reuse_exec_ && reuse_prec_ != prec_) {
+      cudaGraphExecDestroy(reuse_exec_);
+      reuse_exec_ = nullptr;
+    }
     if (!reuse_exec_ || d_vals != d_vals_) {
       if (d_vals != d_vals_) {
         err = "refactor with the stored pivot order reads the engine's value buffer";
@@ -589,7 +593,8 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
       cudaMemsetAsync(dp_.lu + p.lu_large_begin, 0,
                       static_cast<size_t>(p.lu_large_end - p.lu_large_begin) * sizeof(double), cap_stream_);
       cudaError_t ce = large_scatter_reuse(dp_, p, d_vals, large_list_, cap_stream_);
-      if (ce == cudaSuccess) ce = large_refactor(dp_, p, cap_stream_, cap_stream2_, fork_ev_[0], fork_ev_[1], &n_launch);
+      if (ce == cudaSuccess)
+        ce = large_refactor(dp_, p, cap_stream_, cap_stream2_, fork_ev_[0], fork_ev_[1], &n_launch, prec_);
       cudaGraph_t g = nullptr;
       const cudaError_t ee = cudaStreamEndCapture(cap_stream_, &g);
       BDLU_CUDA(ce);
@@ -598,6 +603,7 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
       cudaGraphDestroy(g);
       BDLU_CUDA(ie);
       reuse_launches_ = n_launch + 1;
+      reuse_prec_ = prec_;
     }
     BDLU_CUDA(cudaGraphLaunch(reuse_exec_, stream));
     launches_factor_ += reuse_launches_;
@@ -607,7 +613,7 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
     k_scatter_large<<<dim3(64, static_cast<unsigned>(p.large_units.size())), kThreads, 0, stream>>>(dp_, d_vals,
                                                                                                  large_list_);
     ++launches_factor_;
-    BDLU_CUDA(large_factor(dp_, p, large_list_, stream, &launches_factor_));
+    BDLU_CUDA(large_factor(dp_, p, large_list_, stream, &launches_factor_, prec_));
   }
   BDLU_CUDA(cudaGetLastError());
   BDLU_CUDA(cudaEventRecord(ev_[1], stream));
@@ -724,18 +730,37 @@ bool Engine::solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_
   k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 0);
   BDLU_CUDA(cudaEventRecord(pev_[2], stream));
   const int rg = grid_for(static_cast<int64_t>(n) * kResLanes, kThreads, num_sms_ * 8);
-  for (int32_t it = 0; it < refine_iters; ++it) {
-    BDLU_CUDA(cudaMemsetAsync(d_norms_, 0, static_cast<size_t>(4 * nrhs) * sizeof(unsigned long long), stream));
-    k_residual<<<rg, kThreads, 0, stream>>>(dp_, d_vals_, d_B, ldb, d_b0_, n, d_r_, nrhs, d_norms_);
-    solve_core(d_r_, n, d_xp_, d_nrhs_, stream);
-    k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 1);
-  }
+  for (int32_t it = 0; it < refine_iters; ++it) refine_core(d_B, ldb, nrhs, stream);
   BDLU_CUDA(cudaMemsetAsync(d_norms_, 0, static_cast<size_t>(4 * nrhs) * sizeof(unsigned long long), stream));
   k_residual<<<rg, kThreads, 0, stream>>>(dp_, d_vals_, d_B, ldb, d_b0_, n, nullptr, nrhs, d_norms_);
   BDLU_CUDA(cudaGetLastError());
   BDLU_CUDA(cudaEventRecord(ev_[3], stream));
   last_nrhs_ = nrhs;
   solve_timed_ = true;
+  return true;
+}
+
+void Engine::refine_core(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream) {
+  const int32_t n = plan_.n;
+  const int ug = grid_for(static_cast<int64_t>(n) * nrhs, kThreads, num_sms_ * 16);
+  const int rg = grid_for(static_cast<int64_t>(n) * kResLanes, kThreads, num_sms_ * 8);
+  cudaMemsetAsync(d_norms_, 0, static_cast<size_t>(4 * nrhs) * sizeof(unsigned long long), stream);
+  k_residual<<<rg, kThreads, 0, stream>>>(dp_, d_vals_, d_B, ldb, d_b0_, n, d_r_, nrhs, d_norms_);
+  solve_core(d_r_, n, d_xp_, d_nrhs_, stream);
+  k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 1);
+  launches_solve_ += 3;
+}
+
+bool Engine::refine_async(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream, std::string& err) {
+  const int32_t n = plan_.n;
+  const int rg = grid_for(static_cast<int64_t>(n) * kResLanes, kThreads, num_sms_ * 8);
+  k_set_i32<<<1, 1, 0, stream>>>(d_nrhs_, nrhs);
+  refine_core(d_B, ldb, nrhs, stream);
+  BDLU_CUDA(cudaMemsetAsync(d_norms_, 0, static_cast<size_t>(4 * nrhs) * sizeof(unsigned long long), stream));
+  k_residual<<<rg, kThreads, 0, stream>>>(dp_, d_vals_, d_B, ldb, d_b0_, n, nullptr, nrhs, d_norms_);
+  BDLU_CUDA(cudaGetLastError());
+  launches_solve_ += 2;
+  last_nrhs_ = nrhs;
   return true;
 }
 

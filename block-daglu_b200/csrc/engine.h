@@ -84,6 +84,14 @@ class Engine {
                    std::string& err);
   // Copies the right-hand sides saved by the last solve_async back into d_B.
   bool restore_rhs(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream, std::string& err);
+  // One FP64 refinement step on the solution in d_B (from the last solve):
+  // r = b - A x, x += A^{-1} r with the current factors; then the residual
+  // norms of the new x (read by last_residual).
+  bool refine_async(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream, std::string& err);
+  // Trailing-update arithmetic of large blocks for the next factor:
+  // 0 FP64, 1 TF32 tensor cores, 2 3xTF32.
+  void set_precision(int32_t prec) { prec_ = prec; }
+  int32_t precision() const { return prec_; }
   // Residual norms of the last solve (synchronises the stream), worst column.
   bool last_residual(cudaStream_t stream, SolveResidual& out, std::string& err);
 
@@ -109,6 +117,9 @@ class Engine {
   void release();
   bool ensure_work(int32_t nrhs, std::string& err);
   void solve_core(const double* rhs, int32_t ldr, double* xp, const int32_t* nrhs, cudaStream_t stream);
+  void refine_core(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream);
+  int32_t prec_ = 0;
+  int32_t reuse_prec_ = 0;
 
   Plan plan_;
   DevPlan dp_{};

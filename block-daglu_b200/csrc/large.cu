@@ -905,6 +905,189 @@ __global__ void __launch_bounds__(kRThreads, 2) k_rgemm(DevPlan dp, int32_t k0, 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core trailing updates for the mixed-precision route: a 128 x 64 tile
+// C -= L U with TF32 operands and FP32 accumulation (mma.sync m16n8k8), the
+// operands rounded from the FP64 storage while staged in shared memory.  With
+// split3, each operand is split a = hi + lo (both TF32, lo = tf32(a - hi)) and
+// C -= hi hi + hi lo + lo hi ("3xTF32", a published way to reach about FP32
+// accuracy on TF32 units).  The panels, pivot search and storage stay FP64;
+// FP64 iterative refinement on the host side recovers the accuracy.
+// 256 threads: 8 warps in a 4 x 2 grid of 32 x 32 warp tiles (2 x 4 mma tiles).
+constexpr int kTM = 128;
+constexpr int kTN = 64;
+constexpr int kTBS = kTN + 8;  // B stage row stride (words): conflict-free fragment loads
+
+template <int K>
+constexpr int tf32_smem_words() {
+  return 2 * (kTM * (K + 4) + K * kTBS);
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// C = A[i0 : i0+128, j0 : j0+64] -= A[i0 :, k0 : k0+kk] * A[k0 : k0+kk, j0 :]
+// on a row-major m x m block (kk <= K; rows/columns past m are skipped).
+template <int K>
+__device__ void tile_update_tf32(double* A, int m, int i0, int j0, int k0, int kk, bool split3, uint32_t* sm) {
+  constexpr int kAS = K + 4;  // A stage row stride (words)
+  uint32_t* Ah = sm;
+  uint32_t* Bh = Ah + kTM * kAS;
+  uint32_t* Al = Bh + K * kTBS;
+  uint32_t* Bl = Al + kTM * kAS;
+  const int tid = threadIdx.x;
+  for (int e = tid; e < kTM * K; e += blockDim.x) {
+    const int r = e / K, q = e - r * K;
+    const double v = (i0 + r < m && q < kk) ? A[static_cast<size_t>(i0 + r) * m + k0 + q] : 0.0;
+    const float f = static_cast<float>(v);
+    const uint32_t h = to_tf32(f);
+    Ah[r * kAS + q] = h;
+    if (split3) Al[r * kAS + q] = to_tf32(f - __uint_as_float(h));
+  }
+  for (int e = tid; e < K * kTN; e += blockDim.x) {
+    const int q = e / kTN, c = e - q * kTN;
+    const double v = (q < kk && j0 + c < m) ? A[static_cast<size_t>(k0 + q) * m + j0 + c] : 0.0;
+    const float f = static_cast<float>(v);
+    const uint32_t h = to_tf32(f);
+    Bh[q * kTBS + c] = h;
+    if (split3) Bl[q * kTBS + c] = to_tf32(f - __uint_as_float(h));
+  }
+  __syncthreads();
+  const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
+  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+  float acc[2][4][4];
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0f;
+#pragma unroll 2
+  for (int ks = 0; ks < K; ks += 8) {
+    uint32_t af[2][4], bf[4][2];
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi) {
+      const int r = wm + mi * 16 + g;
+      af[mi][0] = Ah[r * kAS + ks + t4];
+      af[mi][1] = Ah[(r + 8) * kAS + ks + t4];
+      af[mi][2] = Ah[r * kAS + ks + t4 + 4];
+      af[mi][3] = Ah[(r + 8) * kAS + ks + t4 + 4];
+    }
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) {
+      const int c = wn + ni * 8 + g;
+      bf[ni][0] = Bh[(ks + t4) * kTBS + c];
+      bf[ni][1] = Bh[(ks + t4 + 4) * kTBS + c];
+    }
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) mma_tf32(acc[mi][ni], af[mi], bf[ni]);
+    if (split3) {
+      uint32_t al[2][4], bl[4][2];
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi) {
+        const int r = wm + mi * 16 + g;
+        al[mi][0] = Al[r * kAS + ks + t4];
+        al[mi][1] = Al[(r + 8) * kAS + ks + t4];
+        al[mi][2] = Al[r * kAS + ks + t4 + 4];
+        al[mi][3] = Al[(r + 8) * kAS + ks + t4 + 4];
+      }
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        const int c = wn + ni * 8 + g;
+        bl[ni][0] = Bl[(ks + t4) * kTBS + c];
+        bl[ni][1] = Bl[(ks + t4 + 4) * kTBS + c];
+      }
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+          mma_tf32(acc[mi][ni], af[mi], bl[ni]);
+          mma_tf32(acc[mi][ni], al[mi], bf[ni]);
+        }
+    }
+  }
+  // acc[mi][ni][2h + b]: row wm + 16mi + g + 8h, column wn + 8ni + 2t4 + b.
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = i0 + wm + mi * 16 + g + 8 * h;
+      if (r >= m) continue;
+      double* row = A + static_cast<size_t>(r) * m;
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        const int c = j0 + wn + ni * 8 + 2 * t4;
+        if (c < m) row[c] -= static_cast<double>(acc[mi][ni][2 * h]);
+        if (c + 1 < m) row[c + 1] -= static_cast<double>(acc[mi][ni][2 * h + 1]);
+      }
+    }
+}
+
+// Value-only refactor update (k_rgemm's tiles) on tensor cores.
+__global__ void __launch_bounds__(kRThreads) k_rgemm_tf32(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
+                                                          int32_t part, int32_t split3) {
+  extern __shared__ uint32_t tsm[];
+  const int32_t* pref = part ? dp.rstep_gb_pref : dp.rstep_ga_pref;
+  int a = 0;
+  while (a + 1 < nact && pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
+  const int u = dp.rstep_unit[ubase + a];
+  const int t = blockIdx.x - pref[ubase + a];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kRP, m - k0);
+  const int base = k0 + nb;
+  const int rest = m - base;
+  const int ntj = (rest + kRTileN - 1) / kRTileN;
+  int ti, tj;
+  if (part == 0) {
+    if (t < ntj) {
+      ti = 0;
+      tj = t;
+    } else {
+      ti = t - ntj + 1;
+      tj = 0;
+    }
+  } else {
+    ti = 1 + t / (ntj - 1);
+    tj = 1 + t % (ntj - 1);
+  }
+  tile_update_tf32<kRP>(dp.lu + dp.lu_off[u], m, base + ti * kRTileM, base + tj * kRTileN, k0, nb, split3 != 0, tsm);
+}
+
+// First-factor update (k_gemm_rm's 128 x 128 tiles, panel depth kPanel) on
+// tensor cores: two 128 x 64 halves.
+__global__ void __launch_bounds__(kRThreads) k_gemm_rm_tf32(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
+                                                            int32_t split3) {
+  extern __shared__ uint32_t tsm[];
+  int a = 0;
+  while (a + 1 < nact && dp.step_gemm_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
+  const int u = dp.step_unit[ubase + a];
+  const int tile = blockIdx.x - dp.step_gemm_pref[ubase + a];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kPanel, m - k0);
+  const int base = k0 + nb;
+  const int rest = m - base;
+  const int nt = (rest + kGT - 1) / kGT;
+  const int ti = tile % nt, tj = tile / nt;
+  double* A = dp.lu + dp.lu_off[u];
+  tile_update_tf32<kPanel>(A, m, base + ti * kGT, base + tj * kGT, k0, nb, split3 != 0, tsm);
+  __syncthreads();
+  tile_update_tf32<kPanel>(A, m, base + ti * kGT, base + tj * kGT + kTN, k0, nb, split3 != 0, tsm);
+}
+
 int cluster_size_for(int rows) {
   int c = (rows + kPanelRowsMax - 1) / kPanelRowsMax;
   return std::max(1, c);
@@ -923,13 +1106,19 @@ cudaError_t large_setup() {
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_rgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kRGemmSmem));
     if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_rgemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 tf32_smem_words<kRP>() * 4);
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_gemm_rm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 tf32_smem_words<kPanel>() * 4);
+    if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_large_perm, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 4 * 1024);
   });
   return err;
 }
 
 cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, cudaStream_t stream,
-                         int32_t* launches) {
+                         int32_t* launches, int32_t prec) {
   cudaError_t e = large_setup();
   if (e != cudaSuccess) return e;
   for (int32_t st = 0; st < p.nsteps; ++st) {
@@ -962,7 +1151,11 @@ cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_larg
     k_swap_trsm_rm<<<p.step_trsm_total[static_cast<size_t>(st)], kTrsmCols, 0, stream>>>(dp, k0, ub, na);
     *launches += 2;
     if (p.step_gemm_total[static_cast<size_t>(st)] > 0) {
-      k_gemm_rm<<<p.step_gemm_total[static_cast<size_t>(st)], kGThreads, kGemmSmem, stream>>>(dp, k0, ub, na);
+      if (prec > 0)
+        k_gemm_rm_tf32<<<p.step_gemm_total[static_cast<size_t>(st)], kRThreads, tf32_smem_words<kPanel>() * 4, stream>>>(
+            dp, k0, ub, na, prec == 2);
+      else
+        k_gemm_rm<<<p.step_gemm_total[static_cast<size_t>(st)], kGThreads, kGemmSmem, stream>>>(dp, k0, ub, na);
       ++*launches;
     }
   }
@@ -984,7 +1177,7 @@ cudaError_t large_scatter_reuse(const DevPlan& dp, const Plan& p, const double* 
 }
 
 cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cudaStream_t sb, cudaEvent_t ev_a,
-                           cudaEvent_t ev_b, int32_t* launches) {
+                           cudaEvent_t ev_b, int32_t* launches, int32_t prec) {
   cudaError_t e = large_setup();
   if (e != cudaSuccess) return e;
   // Fork: stream b starts after everything already queued on stream a.
@@ -1009,13 +1202,16 @@ cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cu
     if ((e = cudaEventRecord(ev_a, sa)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(sb, ev_a, 0)) != cudaSuccess) return e;
     const int32_t gb = p.rstep_gb_total[static_cast<size_t>(st)];
+    constexpr size_t kTfSmem = tf32_smem_words<kRP>() * 4;
     if (gb > 0) {
-      k_rgemm<<<gb, kRThreads, kRGemmSmem, sb>>>(dp, k0, ub, na, 1);
+      if (prec > 0) k_rgemm_tf32<<<gb, kRThreads, kTfSmem, sb>>>(dp, k0, ub, na, 1, prec == 2);
+      else k_rgemm<<<gb, kRThreads, kRGemmSmem, sb>>>(dp, k0, ub, na, 1);
       ++*launches;
     }
     const int32_t ga = p.rstep_ga_total[static_cast<size_t>(st)];
     if (ga > 0) {
-      k_rgemm<<<ga, kRThreads, kRGemmSmem, sa>>>(dp, k0, ub, na, 0);
+      if (prec > 0) k_rgemm_tf32<<<ga, kRThreads, kTfSmem, sa>>>(dp, k0, ub, na, 0, prec == 2);
+      else k_rgemm<<<ga, kRThreads, kRGemmSmem, sa>>>(dp, k0, ub, na, 0);
       ++*launches;
     }
   }

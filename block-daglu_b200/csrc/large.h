@@ -17,8 +17,9 @@ cudaError_t large_setup();
 // orders (lperm/liperm).  reuse = true: the slots were filled by
 // large_scatter_reuse in the stored row order and no pivot search is made; a
 // zero or non-finite pivot sets status code 2.
+// prec: 0 FP64 trailing updates; 1 TF32 tensor-core updates; 2 3xTF32.
 cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_large_units, cudaStream_t stream,
-                         int32_t* launches);
+                         int32_t* launches, int32_t prec);
 
 // Scatters the values of all large units into their (zeroed) slots with the
 // rows in the stored pivot order.
@@ -32,7 +33,7 @@ cudaError_t large_scatter_reuse(const DevPlan& dp, const Plan& p, const double* 
 // and joined back into sa with the two events); zero or non-finite pivots set
 // the reused-pivot status.
 cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cudaStream_t sb, cudaEvent_t ev_a,
-                           cudaEvent_t ev_b, int32_t* launches);
+                           cudaEvent_t ev_b, int32_t* launches, int32_t prec);
 
 // Forward and backward solves of the large units of one level (two
 // launches).  d_sync holds large_sync_words(p) zeroed words per solve sweep;

@@ -129,6 +129,7 @@ typedef struct bdlu_stats {
   double residual_inf;       /* |Ax-b|_inf / (|A|_inf |x|_inf + |b|_inf), last solve, worst rhs */
   double last_factor_ms;     /* device time of the last factor */
   double last_solve_ms;      /* device time of the last solve */
+  int32_t precision;         /* trailing-update arithmetic of the last factor: 0 FP64, 1 TF32, 2 3xTF32 */
 } bdlu_stats;
 int bdlu_get_stats(const bdlu_solver* h, bdlu_stats* out);
 
@@ -151,6 +152,15 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  *   "analysis_only": 1 makes analyze stop after the host analysis (no device
  *     upload); factor then reports BDLU_BACKEND_UNAVAILABLE.  For structure
  *     inspection on machines without a GPU.
+ *   "precision": 0 (default) FP64 throughout.  1 selects the mixed route: the
+ *     trailing updates of blocks above the shared-memory size run on tensor
+ *     cores with TF32 operands and FP32 accumulation (panels, pivoting and
+ *     storage stay FP64), and host-buffer solves refine in FP64 until the
+ *     relative residual is <= 1e-12.  A level whose refinement stagnates is
+ *     replaced for this and later factorisations: TF32, then 3xTF32 (about
+ *     FP32 accuracy), then FP64.  stats.precision and stats.refine_iters
+ *     report the level and the refinement steps.  Device-pointer solves run
+ *     "refine_iters" steps only.
  * Returns BDLU_OK, or BDLU_INVALID_DIMENSION for an unknown key. */
 int bdlu_set_option(bdlu_solver* h, const char* key, double value);
 
