@@ -267,6 +267,11 @@ int bdlu_solve_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStre
         prev = h->last_residual;
       }
       steps += k;
+      // Every refinement step costs a solve: a level that needed more than
+      // kSlowRefine steps is replaced for the next factorisation as well.
+      constexpr int kSlowRefine = 4;
+      if (h->last_residual <= kReuseResidualLimit && k > kSlowRefine && h->prec_level != 0)
+        h->prec_level = (h->prec_level == 1) ? 2 : 0;
       if (h->last_residual <= kReuseResidualLimit || h->prec_level == 0) break;
       h->prec_level = (h->prec_level == 1) ? 2 : 0;
       if (const int st = do_factor(h, stream, h->engine->last_factor_reused())) return st;

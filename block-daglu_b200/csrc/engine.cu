@@ -406,6 +406,8 @@ int32_t small_unit_max() {
 Engine::Engine() {
   cudaStreamCreateWithFlags(&cap_stream_, cudaStreamNonBlocking);
   cudaStreamCreateWithFlags(&cap_stream2_, cudaStreamNonBlocking);
+  for (auto& a : aux_) cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking);
+  for (auto& e : aux_ev_) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (auto& e : fork_ev_) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (auto& e : ev_) cudaEventCreate(&e);
   for (auto& e : pev_) cudaEventCreate(&e);
@@ -418,6 +420,10 @@ Engine::~Engine() {
   release();
   if (cap_stream_) cudaStreamDestroy(cap_stream_);
   if (cap_stream2_) cudaStreamDestroy(cap_stream2_);
+  for (auto& a : aux_)
+    if (a) cudaStreamDestroy(a);
+  for (auto& e : aux_ev_)
+    if (e) cudaEventDestroy(e);
   for (auto& e : fork_ev_)
     if (e) cudaEventDestroy(e);
   for (auto& e : ev_)
@@ -427,9 +433,10 @@ Engine::~Engine() {
 }
 
 void Engine::drop_graphs() {
-  if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
+  for (auto& ge : solve_exec_)
+    if (ge) cudaGraphExecDestroy(ge);
   if (reuse_exec_) cudaGraphExecDestroy(reuse_exec_);
-  solve_exec_ = nullptr;
+  solve_exec_[0] = solve_exec_[1] = nullptr;
   reuse_exec_ = nullptr;
   solve_exec_b0_ = nullptr;
 }
@@ -571,11 +578,24 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   launches_factor_ = 1 + static_cast<int32_t>(p.small_bucket_m.size());
   k_gather<<<grid_for(std::max<int64_t>(ncpl, p.n), kThreads, num_sms_ * 8), kThreads, 0, stream>>>(dp_, d_vals, ncpl);
   BDLU_CUDA(cudaEventRecord(pev_[0], stream));
-  // One launch per size bucket, shared memory sized to the bucket.
-  for (size_t bkt = 0; bkt < p.small_bucket_m.size(); ++bkt) {
-    const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
-    const size_t mb = static_cast<size_t>(p.small_bucket_m[bkt]);
-    k_lu_small<<<q1 - q0, kThreads, mb * mb * sizeof(double), stream>>>(dp_, d_vals, small_list_ + q0);
+  // One launch per size bucket, shared memory sized to the bucket; the
+  // buckets run side by side on the auxiliary streams (forked from and
+  // joined back into `stream`), largest units first.
+  if (!p.small_bucket_m.empty()) {
+    BDLU_CUDA(cudaEventRecord(fork_ev_[0], stream));
+    const size_t nbk = p.small_bucket_m.size();
+    for (size_t q = 0; q < nbk; ++q) {
+      const size_t bkt = nbk - 1 - q;
+      cudaStream_t sb = aux_[q % kAux];
+      if (q < static_cast<size_t>(kAux)) BDLU_CUDA(cudaStreamWaitEvent(sb, fork_ev_[0], 0));
+      const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
+      const size_t mb = static_cast<size_t>(p.small_bucket_m[bkt]);
+      k_lu_small<<<q1 - q0, kThreads, mb * mb * sizeof(double), sb>>>(dp_, d_vals, small_list_ + q0);
+    }
+    for (int q = 0; q < kAux && q < static_cast<int>(nbk); ++q) {
+      BDLU_CUDA(cudaEventRecord(aux_ev_[q], aux_[q]));
+      BDLU_CUDA(cudaStreamWaitEvent(stream, aux_ev_[q], 0));
+    }
   }
   BDLU_CUDA(cudaEventRecord(pev_[1], stream));
   if (!p.large_units.empty() && reuse) {
@@ -675,7 +695,8 @@ double* Engine::rhs_buffer(int32_t nrhs, std::string& err) {
   return d_rhs_;
 }
 
-void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_t* nrhs, cudaStream_t stream) {
+void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_t* nrhs, bool wide,
+                        cudaStream_t stream) {
   const Plan& p = plan_;
   const int32_t nl = p.umax_level + 1;
   if (p.large_tiles > 0) cudaMemsetAsync(d_sync_, 0, static_cast<size_t>(sync_words_) * sizeof(int32_t), stream);
@@ -693,7 +714,8 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_
       const size_t mm = static_cast<size_t>(p.lvl_dense_maxm[static_cast<size_t>(l)]);
       k_solve_dense<<<d1 - d0, kThreads, mm * mm * sizeof(double), stream>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp, nrhs);
     }
-    large_solve_level(dp_, p, l, lvl_large_, lvl_large_tile0_, d_sync_, rhs, ldr, xp, nrhs, stream, &launches_solve_);
+    large_solve_level(dp_, p, l, lvl_large_, lvl_large_tile0_, d_sync_, rhs, ldr, xp, nrhs, wide, stream,
+                      &launches_solve_);
   }
 }
 
@@ -707,25 +729,30 @@ bool Engine::solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_
                               static_cast<size_t>(ldb) * sizeof(double), static_cast<size_t>(n) * sizeof(double),
                               static_cast<size_t>(nrhs), cudaMemcpyDeviceToDevice, stream));
   // The sweep's kernels read the right-hand-side count from d_nrhs_, so one
-  // graph (captured on the current work buffers) serves every count.
+  // graph per tile-kernel width (up to 8 and up to 16 right-hand sides per
+  // pass), captured on the current work buffers, serves every count.
   k_set_i32<<<1, 1, 0, stream>>>(d_nrhs_, nrhs);
-  if (!solve_exec_ || solve_exec_b0_ != d_b0_) {
-    if (solve_exec_) cudaGraphExecDestroy(solve_exec_);
-    solve_exec_ = nullptr;
-    const int32_t saved = launches_solve_;
-    BDLU_CUDA(cudaStreamBeginCapture(cap_stream_, cudaStreamCaptureModeThreadLocal));
-    solve_core(d_b0_, n, d_xp_, d_nrhs_, cap_stream_);
-    cudaGraph_t g = nullptr;
-    BDLU_CUDA(cudaStreamEndCapture(cap_stream_, &g));
-    const cudaError_t ie = cudaGraphInstantiate(&solve_exec_, g, 0);
-    cudaGraphDestroy(g);
-    BDLU_CUDA(ie);
-    solve_exec_launches_ = launches_solve_ - saved;
-    launches_solve_ = saved;
+  const int wide = nrhs > 8 ? 1 : 0;
+  if (solve_exec_b0_ != d_b0_) {
+    for (auto& ge : solve_exec_)
+      if (ge) cudaGraphExecDestroy(ge);
+    solve_exec_[0] = solve_exec_[1] = nullptr;
     solve_exec_b0_ = d_b0_;
   }
-  BDLU_CUDA(cudaGraphLaunch(solve_exec_, stream));
-  launches_solve_ += solve_exec_launches_ + 1;
+  if (!solve_exec_[wide]) {
+    const int32_t saved = launches_solve_;
+    BDLU_CUDA(cudaStreamBeginCapture(cap_stream_, cudaStreamCaptureModeThreadLocal));
+    solve_core(d_b0_, n, d_xp_, d_nrhs_, wide != 0, cap_stream_);
+    cudaGraph_t g = nullptr;
+    BDLU_CUDA(cudaStreamEndCapture(cap_stream_, &g));
+    const cudaError_t ie = cudaGraphInstantiate(&solve_exec_[wide], g, 0);
+    cudaGraphDestroy(g);
+    BDLU_CUDA(ie);
+    solve_exec_launches_[wide] = launches_solve_ - saved;
+    launches_solve_ = saved;
+  }
+  BDLU_CUDA(cudaGraphLaunch(solve_exec_[wide], stream));
+  launches_solve_ += solve_exec_launches_[wide] + 1;
   const int ug = grid_for(static_cast<int64_t>(n) * nrhs, kThreads, num_sms_ * 16);
   k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 0);
   BDLU_CUDA(cudaEventRecord(pev_[2], stream));
@@ -746,7 +773,7 @@ void Engine::refine_core(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t st
   const int rg = grid_for(static_cast<int64_t>(n) * kResLanes, kThreads, num_sms_ * 8);
   cudaMemsetAsync(d_norms_, 0, static_cast<size_t>(4 * nrhs) * sizeof(unsigned long long), stream);
   k_residual<<<rg, kThreads, 0, stream>>>(dp_, d_vals_, d_B, ldb, d_b0_, n, d_r_, nrhs, d_norms_);
-  solve_core(d_r_, n, d_xp_, d_nrhs_, stream);
+  solve_core(d_r_, n, d_xp_, d_nrhs_, nrhs > 8, stream);
   k_unpermute<<<ug, kThreads, 0, stream>>>(dp_.Q, n, d_xp_, d_B, ldb, nrhs, 1);
   launches_solve_ += 3;
 }

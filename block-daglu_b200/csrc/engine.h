@@ -116,7 +116,7 @@ class Engine {
  private:
   void release();
   bool ensure_work(int32_t nrhs, std::string& err);
-  void solve_core(const double* rhs, int32_t ldr, double* xp, const int32_t* nrhs, cudaStream_t stream);
+  void solve_core(const double* rhs, int32_t ldr, double* xp, const int32_t* nrhs, bool wide, cudaStream_t stream);
   void refine_core(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream);
   int32_t prec_ = 0;
   int32_t reuse_prec_ = 0;
@@ -155,9 +155,14 @@ class Engine {
   cudaStream_t cap_stream_ = nullptr;
   cudaStream_t cap_stream2_ = nullptr;  // second branch of the refactor graph
   cudaEvent_t fork_ev_[2] = {nullptr, nullptr};
-  // Solve-sweep graph, valid for the work buffers it was captured on.
-  cudaGraphExec_t solve_exec_ = nullptr;
-  int32_t solve_exec_launches_ = 0;
+  // Auxiliary streams for the small-unit factor buckets.
+  static constexpr int kAux = 4;
+  cudaStream_t aux_[kAux] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t aux_ev_[kAux] = {nullptr, nullptr, nullptr, nullptr};
+  // Solve-sweep graphs (tile kernels 8 and 16 wide), valid for the work
+  // buffers they were captured on.
+  cudaGraphExec_t solve_exec_[2] = {nullptr, nullptr};
+  int32_t solve_exec_launches_[2] = {0, 0};
   const double* solve_exec_b0_ = nullptr;
   int32_t* d_nrhs_ = nullptr;  // right-hand-side count read by the sweep's kernels
   cudaGraphExec_t reuse_exec_ = nullptr;

@@ -458,9 +458,16 @@ __global__ void k_scatter_large_perm(DevPlan dp, const double* __restrict__ vals
 // finished right-hand-side passes.  Every wait is bounded: a wait that runs
 // out records kFailSync in the status word and publishes kAbortFlag, so the
 // tiles behind it stop too.
-constexpr int kRC = kSolveThreads / 32;  // right-hand sides per pass (one warp each)
+// Right-hand sides per pass: kernels exist for 8 and 16 (the 16-wide one
+// reads each factor block once for up to 16 right-hand sides; the 8-wide one
+// keeps fewer registers and a shorter tile chain for few right-hand sides).
 constexpr int kSpinLimit = 1 << 22;       // polls of a flag (~0.5 s with the back-off)
 constexpr int32_t kAbortFlag = 1 << 30;
+constexpr int kTLoads = kTile * kTile / kSolveThreads;  // block entries each thread stages
+template <int kRC>
+constexpr size_t trsv_smem() {
+  return (static_cast<size_t>(kTile) * kTS + 2 * static_cast<size_t>(kTile) * kRC) * sizeof(double);
+}
 
 __device__ __forceinline__ bool wait_ready(const int32_t* f, int32_t need) {
   for (int it = 0; it < kSpinLimit; ++it) {
@@ -474,17 +481,30 @@ __device__ __forceinline__ bool wait_ready(const int32_t* f, int32_t need) {
   return false;
 }
 
-template <bool kFwd>
-__global__ void __launch_bounds__(kSolveThreads) k_trsv_tiles(DevPlan dp, const int32_t* __restrict__ units,
+// Entries (i, c) of the kTile x kTile block at (t0, j0) that thread `tid`
+// stages: e = tid + kSolveThreads * k, i = e / kTile, c = e % kTile.
+__device__ __forceinline__ void load_block(const double* __restrict__ LU, int m, int t0, int w, int j0, int jw,
+                                           int tid, double (&v)[kTLoads]) {
+#pragma unroll
+  for (int k = 0; k < kTLoads; ++k) {
+    const int e = tid + kSolveThreads * k;
+    const int i = e / kTile, c = e - i * kTile;
+    v[k] = (i < w && c < jw) ? __ldg(LU + static_cast<size_t>(t0 + i) * m + j0 + c) : 0.0;
+  }
+}
+
+template <bool kFwd, int kRC>
+__global__ void __launch_bounds__(kSolveThreads, 2) k_trsv_tiles(DevPlan dp, const int32_t* __restrict__ units,
                                                               const int32_t* __restrict__ tile0, int32_t count,
                                                               int32_t* ticket, int32_t* ready,
                                                               const double* __restrict__ rhs, int32_t ldr,
                                                               double* __restrict__ xp,
                                                               const int32_t* __restrict__ nrhs_p) {
   const int32_t nrhs = *nrhs_p;
-  __shared__ double Ts[kTile * kTS];  // factor block; also the partial-sum exchange
-  __shared__ double xs[kTile * kRC];  // this tile's unknowns [i * kRC + c]
-  __shared__ double xj[kTile * kRC];  // finished tile's unknowns
+  extern __shared__ double tsm_d[];
+  double* Ts = tsm_d;                  // factor block; also the partial-sum exchange
+  double* xs = Ts + kTile * kTS;       // this tile's unknowns [i * kRC + c]
+  double* xj = xs + kTile * kRC;       // finished tile's unknowns
   __shared__ int s_tk, s_ok;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_tk = atomicAdd(ticket, 1);
@@ -506,11 +526,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_trsv_tiles(DevPlan dp, const 
   const int r = tid & (kTile - 1), g = tid / kTile;  // row of the tile, 16-column group
   constexpr int kGroups = kSolveThreads / kTile;
   constexpr int kGCols = kTile / kGroups;
+  constexpr int kWarps = kSolveThreads / 32;
   for (int c0 = 0; c0 < nrhs; c0 += kRC) {
     const int nc = min(kRC, nrhs - c0);
     const int32_t need = c0 / kRC + 1;
     if (kFwd) {
-      for (int i = warp; i < w; i += kSolveThreads / 32) {
+      for (int i = warp; i < w; i += kWarps) {
         const int rr = s + dp.lperm[s + t0 + i];
         const int p0 = dp.cpl_ptr[rr], p1 = dp.cpl_ptr[rr + 1];
         for (int c = 0; c < nc; ++c) {
@@ -532,13 +553,32 @@ __global__ void __launch_bounds__(kSolveThreads) k_trsv_tiles(DevPlan dp, const 
     for (int c = 0; c < kRC; ++c) acc[c] = 0.0;
     const int jn = kFwd ? I : nt - 1 - I;
     bool ok = true;
+    // The next block is loaded into registers while the current one is
+    // used, so the loads overlap the arithmetic and the flag wait.
+    // nxt: the next coupling block, and after the last one the diagonal
+    // block, so the triangle's operands are in flight before they are needed.
+    double nxt[kTLoads];
+    if (jn > 0) {
+      const int J = kFwd ? 0 : nt - 1;
+      load_block(LU, m, t0, w, J * kTile, min(kTile, m - J * kTile), tid, nxt);
+    } else {
+      load_block(LU, m, t0, w, t0, w, tid, nxt);
+    }
     for (int jk = 0; jk < jn; ++jk) {
       const int J = kFwd ? jk : nt - 1 - jk;
       const int j0 = J * kTile, jw = min(kTile, m - j0);
       __syncthreads();
-      for (int e = tid; e < kTile * kTile; e += kSolveThreads) {
-        const int i = e / kTile, cc = e - i * kTile;
-        Ts[i * kTS + cc] = (i < w && cc < jw) ? __ldg(LU + static_cast<size_t>(t0 + i) * m + j0 + cc) : 0.0;
+#pragma unroll
+      for (int k = 0; k < kTLoads; ++k) {
+        const int e = tid + kSolveThreads * k;
+        const int i = e / kTile, c = e - i * kTile;
+        Ts[i * kTS + c] = nxt[k];
+      }
+      if (jk + 1 < jn) {
+        const int J2 = kFwd ? jk + 1 : nt - 2 - jk;
+        load_block(LU, m, t0, w, J2 * kTile, min(kTile, m - J2 * kTile), tid, nxt);
+      } else {
+        load_block(LU, m, t0, w, t0, w, tid, nxt);
       }
       if (tid == 0) s_ok = wait_ready(rdy + J, need) ? 1 : 0;
       __syncthreads();
@@ -546,17 +586,24 @@ __global__ void __launch_bounds__(kSolveThreads) k_trsv_tiles(DevPlan dp, const 
         ok = false;
         break;
       }
-      for (int e = tid; e < kTile * kRC; e += kSolveThreads) {
+#pragma unroll
+      for (int k = 0; k < kTile * kRC / kSolveThreads; ++k) {
+        const int e = tid + kSolveThreads * k;
         const int jj = e / kRC, c = e - jj * kRC;
         xj[e] = (jj < jw && c < nc) ? __ldcg(xp + static_cast<size_t>(c0 + c) * n + s + j0 + jj) : 0.0;
       }
       __syncthreads();
-#pragma unroll 4
+#pragma unroll 1
       for (int k = 0; k < kGCols; ++k) {
         const int cc = g * kGCols + k;
         const double t = Ts[r * kTS + cc];
+        const double2* xv = reinterpret_cast<const double2*>(xj + cc * kRC);
 #pragma unroll
-        for (int c = 0; c < kRC; ++c) acc[c] = fma(t, xj[cc * kRC + c], acc[c]);
+        for (int c2 = 0; c2 < kRC / 2; ++c2) {
+          const double2 x2 = xv[c2];
+          acc[2 * c2] = fma(t, x2.x, acc[2 * c2]);
+          acc[2 * c2 + 1] = fma(t, x2.y, acc[2 * c2 + 1]);
+        }
       }
     }
     if (!ok) {
@@ -578,34 +625,87 @@ __global__ void __launch_bounds__(kSolveThreads) k_trsv_tiles(DevPlan dp, const 
       xs[i * kRC + c] -= sum;
     }
     __syncthreads();
-    for (int e = tid; e < kTile * kTile; e += kSolveThreads) {
-      const int i = e / kTile, cc = e - i * kTile;
-      Ts[i * kTS + cc] = (i < w && cc < w) ? __ldg(LU + static_cast<size_t>(t0 + i) * m + t0 + cc) : 0.0;
+#pragma unroll
+    for (int k = 0; k < kTLoads; ++k) {
+      const int e = tid + kSolveThreads * k;
+      const int i = e / kTile, c = e - i * kTile;
+      Ts[i * kTS + c] = nxt[k];
     }
     __syncthreads();
+    // Each warp sweeps right-hand side `warp` and, when more than kWarps are
+    // in this pass, also warp + kWarps alongside (their chains overlap).
     if (warp < nc) {
-      const int c = warp;
-      double a = (lane < w) ? xs[lane * kRC + c] : 0.0;
-      double b = (lane + 32 < w) ? xs[(lane + 32) * kRC + c] : 0.0;
-      if (kFwd) {
+      const int ca = warp, cb = warp + kWarps;
+      const bool two = kRC > kWarps && cb < nc;
+      double a0 = (lane < w) ? xs[lane * kRC + ca] : 0.0;
+      double b0 = (lane + 32 < w) ? xs[(lane + 32) * kRC + ca] : 0.0;
+      double a1 = (two && lane < w) ? xs[lane * kRC + cb] : 0.0;
+      double b1 = (two && lane + 32 < w) ? xs[(lane + 32) * kRC + cb] : 0.0;
+      if (two) {
+        if (kFwd) {
+          for (int rr = 0; rr < w; ++rr) {
+            const double x0 = __shfl_sync(0xffffffffu, rr < 32 ? a0 : b0, rr & 31);
+            const double x1 = __shfl_sync(0xffffffffu, rr < 32 ? a1 : b1, rr & 31);
+            if (lane > rr && lane < w) {
+              const double t = Ts[lane * kTS + rr];
+              a0 = fma(-t, x0, a0);
+              a1 = fma(-t, x1, a1);
+            }
+            if (lane + 32 > rr && lane + 32 < w) {
+              const double t = Ts[(lane + 32) * kTS + rr];
+              b0 = fma(-t, x0, b0);
+              b1 = fma(-t, x1, b1);
+            }
+          }
+        } else {
+          for (int rr = w - 1; rr >= 0; --rr) {
+            const double d = Ts[rr * kTS + rr];
+            const double x0 = __shfl_sync(0xffffffffu, rr < 32 ? a0 : b0, rr & 31) / d;
+            const double x1 = __shfl_sync(0xffffffffu, rr < 32 ? a1 : b1, rr & 31) / d;
+            if (lane == rr) {
+              a0 = x0;
+              a1 = x1;
+            }
+            if (lane + 32 == rr) {
+              b0 = x0;
+              b1 = x1;
+            }
+            if (lane < rr) {
+              const double t = Ts[lane * kTS + rr];
+              a0 = fma(-t, x0, a0);
+              a1 = fma(-t, x1, a1);
+            }
+            if (lane + 32 < rr) {
+              const double t = Ts[(lane + 32) * kTS + rr];
+              b0 = fma(-t, x0, b0);
+              b1 = fma(-t, x1, b1);
+            }
+          }
+        }
+      } else if (kFwd) {
         for (int rr = 0; rr < w; ++rr) {
-          const double xr = __shfl_sync(0xffffffffu, rr < 32 ? a : b, rr & 31);
-          if (lane > rr && lane < w) a = fma(-Ts[lane * kTS + rr], xr, a);
-          if (lane + 32 > rr && lane + 32 < w) b = fma(-Ts[(lane + 32) * kTS + rr], xr, b);
+          const double x0 = __shfl_sync(0xffffffffu, rr < 32 ? a0 : b0, rr & 31);
+          if (lane > rr && lane < w) a0 = fma(-Ts[lane * kTS + rr], x0, a0);
+          if (lane + 32 > rr && lane + 32 < w) b0 = fma(-Ts[(lane + 32) * kTS + rr], x0, b0);
         }
       } else {
         for (int rr = w - 1; rr >= 0; --rr) {
           const double d = Ts[rr * kTS + rr];
-          const double xr = __shfl_sync(0xffffffffu, rr < 32 ? a : b, rr & 31) / d;
-          if (lane == rr) a = xr;
-          if (lane + 32 == rr) b = xr;
-          if (lane < rr) a = fma(-Ts[lane * kTS + rr], xr, a);
-          if (lane + 32 < rr) b = fma(-Ts[(lane + 32) * kTS + rr], xr, b);
+          const double x0 = __shfl_sync(0xffffffffu, rr < 32 ? a0 : b0, rr & 31) / d;
+          if (lane == rr) a0 = x0;
+          if (lane + 32 == rr) b0 = x0;
+          if (lane < rr) a0 = fma(-Ts[lane * kTS + rr], x0, a0);
+          if (lane + 32 < rr) b0 = fma(-Ts[(lane + 32) * kTS + rr], x0, b0);
         }
       }
-      double* xo = xp + static_cast<size_t>(c0 + c) * n + s + t0;
-      if (lane < w) xo[lane] = a;
-      if (lane + 32 < w) xo[lane + 32] = b;
+      double* xo = xp + static_cast<size_t>(c0 + ca) * n + s + t0;
+      if (lane < w) xo[lane] = a0;
+      if (lane + 32 < w) xo[lane + 32] = b0;
+      if (two) {
+        double* xo1 = xp + static_cast<size_t>(c0 + cb) * n + s + t0;
+        if (lane < w) xo1[lane] = a1;
+        if (lane + 32 < w) xo1[lane + 32] = b1;
+      }
     }
     __threadfence();
     __syncthreads();
@@ -1106,6 +1206,18 @@ cudaError_t large_setup() {
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_rgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kRGemmSmem));
     if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_trsv_tiles<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(trsv_smem<16>()));
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_trsv_tiles<false, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(trsv_smem<16>()));
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_trsv_tiles<true, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(trsv_smem<8>()));
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_trsv_tiles<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(trsv_smem<8>()));
+    if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_rgemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  tf32_smem_words<kRP>() * 4);
     if (err == cudaSuccess)
@@ -1223,7 +1335,7 @@ cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cu
 
 cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, int32_t level, const int32_t* d_units,
                               const int32_t* d_tile0, int32_t* d_sync, const double* rhs, int32_t ldr, double* xp,
-                              const int32_t* nrhs, cudaStream_t stream, int32_t* launches) {
+                              const int32_t* nrhs, bool wide, cudaStream_t stream, int32_t* launches) {
   const int32_t g0 = p.lvl_large_ptr[static_cast<size_t>(level)];
   const int32_t g1 = p.lvl_large_ptr[static_cast<size_t>(level) + 1];
   if (g1 <= g0) return cudaSuccess;
@@ -1232,10 +1344,17 @@ cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, int32_t level, c
   int32_t* tickets = d_sync + 2 * level;
   int32_t* ready_fwd = d_sync + 2 * nl;
   int32_t* ready_bwd = ready_fwd + p.large_tiles;
-  k_trsv_tiles<true><<<tiles, kSolveThreads, 0, stream>>>(dp, d_units + g0, d_tile0 + g0, g1 - g0, tickets, ready_fwd,
-                                                           rhs, ldr, xp, nrhs);
-  k_trsv_tiles<false><<<tiles, kSolveThreads, 0, stream>>>(dp, d_units + g0, d_tile0 + g0, g1 - g0, tickets + 1,
-                                                            ready_bwd, rhs, ldr, xp, nrhs);
+  if (wide) {
+    k_trsv_tiles<true, 16><<<tiles, kSolveThreads, trsv_smem<16>(), stream>>>(
+        dp, d_units + g0, d_tile0 + g0, g1 - g0, tickets, ready_fwd, rhs, ldr, xp, nrhs);
+    k_trsv_tiles<false, 16><<<tiles, kSolveThreads, trsv_smem<16>(), stream>>>(
+        dp, d_units + g0, d_tile0 + g0, g1 - g0, tickets + 1, ready_bwd, rhs, ldr, xp, nrhs);
+  } else {
+    k_trsv_tiles<true, 8><<<tiles, kSolveThreads, trsv_smem<8>(), stream>>>(
+        dp, d_units + g0, d_tile0 + g0, g1 - g0, tickets, ready_fwd, rhs, ldr, xp, nrhs);
+    k_trsv_tiles<false, 8><<<tiles, kSolveThreads, trsv_smem<8>(), stream>>>(
+        dp, d_units + g0, d_tile0 + g0, g1 - g0, tickets + 1, ready_bwd, rhs, ldr, xp, nrhs);
+  }
   *launches += 2;
   return cudaGetLastError();
 }

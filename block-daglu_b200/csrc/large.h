@@ -37,10 +37,11 @@ cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cu
 
 // Forward and backward solves of the large units of one level (two
 // launches).  d_sync holds large_sync_words(p) zeroed words per solve sweep;
-// nrhs points to the right-hand-side count in device memory.
+// nrhs points to the right-hand-side count in device memory; wide selects the
+// 16-per-pass kernels (for counts above 8).
 cudaError_t large_solve_level(const DevPlan& dp, const Plan& p, int32_t level, const int32_t* d_units,
                               const int32_t* d_tile0, int32_t* d_sync, const double* rhs, int32_t ldr, double* xp,
-                              const int32_t* nrhs, cudaStream_t stream, int32_t* launches);
+                              const int32_t* nrhs, bool wide, cudaStream_t stream, int32_t* launches);
 
 int32_t large_sync_words(const Plan& p);
 
