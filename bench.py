@@ -141,6 +141,16 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(ms, dist, device=None):
+    """Replicas: the slowest rank's time (all_reduce MAX); ms unchanged on one process."""
+    if dist is None:
+        return float(ms)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -346,11 +356,7 @@ def run_batch(args, rank, world):
         worst = max(worst, float(rel.max()))
         off += g.n
         voff += g.nnz
-    my_ms = float(sum(step_ms))
-    if dist:
-        t = torch.tensor([my_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        my_ms = float(t.item())
+    my_ms = max_over_ranks(sum(step_ms), dist, dev)
     ms_per_step = my_ms / args.steps
     value = world * BATCH_SYSTEMS * 1000.0 / ms_per_step
     # End to end through the C ABI with host buffers.
@@ -701,11 +707,7 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    my_ms = float(sum(step_ms))
-    if dist:
-        t = torch.tensor([my_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        my_ms = float(t.item())
+    my_ms = max_over_ranks(sum(step_ms), dist, dev)
     ms_per_step = my_ms / args.steps
     value = world * 1000.0 / ms_per_step
 
