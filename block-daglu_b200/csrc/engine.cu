@@ -54,11 +54,12 @@ __global__ void k_set_i32(int32_t* p, int32_t v) { *p = v; }
 // ---------------------------------------------------------------------------
 // Dense LU of one unit in shared memory (column-major, leading dimension m).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double* __restrict__ vals,
+template <int kT>
+__global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __restrict__ vals,
                                                         const int32_t* __restrict__ units) {
   extern __shared__ double A[];
-  __shared__ double s_best[kThreads / 32];
-  __shared__ int s_bi[kThreads / 32];
+  __shared__ double s_best[kT / 32];
+  __shared__ int s_bi[kT / 32];
   __shared__ int s_piv;
   __shared__ double s_pbest;
   const int u = units[blockIdx.x];
@@ -66,9 +67,9 @@ __global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double*
   const int m = dp.ustart[u + 1] - s;
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
-  for (int i = tid; i < m * m; i += kThreads) A[i] = 0.0;
+  for (int i = tid; i < m * m; i += kT) A[i] = 0.0;
   __syncthreads();
-  for (int64_t e = dp.dent_ptr[u] + tid; e < dp.dent_ptr[u + 1]; e += kThreads) A[dp.dent_pos[e]] = vals[dp.dent_src[e]];
+  for (int64_t e = dp.dent_ptr[u] + tid; e < dp.dent_ptr[u + 1]; e += kT) A[dp.dent_pos[e]] = vals[dp.dent_src[e]];
   __syncthreads();
   int32_t* piv = dp.piv + s;
   for (int k = 0; k < m; ++k) {
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double*
     // Pivot: each warp scans a strided share of rows k..m-1.
     double best = 0.0;
     int bi = m;
-    for (int i = k + tid; i < m; i += kThreads) {
+    for (int i = k + tid; i < m; i += kT) {
       const double a = fabs(colk[i]);
       if (bi == m || a > best) {
         best = a;
@@ -90,8 +91,8 @@ __global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double*
     }
     __syncthreads();
     if (warp == 0) {
-      best = (lane < kThreads / 32) ? s_best[lane] : 0.0;
-      bi = (lane < kThreads / 32) ? s_bi[lane] : m;
+      best = (lane < kT / 32) ? s_best[lane] : 0.0;
+      bi = (lane < kT / 32) ? s_bi[lane] : m;
       warp_pivot_reduce(best, bi, m);
       if (lane == 0) {
         s_piv = bi;
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double*
     }
     if (tid == 0) piv[k] = p;
     if (p != k) {
-      for (int j = tid; j < m; j += kThreads) {
+      for (int j = tid; j < m; j += kT) {
         double* c = A + static_cast<size_t>(j) * m;
         const double t = c[k];
         c[k] = c[p];
@@ -115,10 +116,10 @@ __global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double*
     }
     __syncthreads();
     const double akk = colk[k];
-    for (int i = k + 1 + tid; i < m; i += kThreads) colk[i] = __ddiv_rn(colk[i], akk);
+    for (int i = k + 1 + tid; i < m; i += kT) colk[i] = __ddiv_rn(colk[i], akk);
     __syncthreads();
     const int r = m - k - 1;
-    for (int t = tid; t < r * r; t += kThreads) {
+    for (int t = tid; t < r * r; t += kT) {
       const int jj = t / r, ii = t - jj * r;
       const int i = k + 1 + ii, j = k + 1 + jj;
       double* c = A + static_cast<size_t>(j) * m;
@@ -127,11 +128,11 @@ __global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double*
     __syncthreads();
   }
   double* out = dp.lu + dp.lu_off[u];
-  for (int i = tid; i < m * m; i += kThreads) out[i] = A[i];
+  for (int i = tid; i < m * m; i += kT) out[i] = A[i];
   // Final row order (row k of the factor is local row lperm[k]) for the solve.
   __syncthreads();
   int32_t* ord = reinterpret_cast<int32_t*>(A);
-  for (int k = tid; k < m; k += kThreads) ord[k] = k;
+  for (int k = tid; k < m; k += kT) ord[k] = k;
   __syncthreads();
   if (tid == 0) {
     for (int k = 0; k < m; ++k) {
@@ -144,7 +145,7 @@ __global__ void __launch_bounds__(kThreads) k_lu_small(DevPlan dp, const double*
     }
   }
   __syncthreads();
-  for (int k = tid; k < m; k += kThreads) dp.lperm[s + k] = ord[k];
+  for (int k = tid; k < m; k += kT) dp.lperm[s + k] = ord[k];
 }
 
 // ---------------------------------------------------------------------------
@@ -512,6 +513,7 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   if (!upload_vec(allocs_, plan.rstep_strip_pref, &d.rstep_strip_pref, err)) return false;
   if (!upload_vec(allocs_, plan.rstep_ga_pref, &d.rstep_ga_pref, err)) return false;
   if (!upload_vec(allocs_, plan.rstep_gb_pref, &d.rstep_gb_pref, err)) return false;
+  if (!alloc_dev(allocs_, static_cast<size_t>(plan.rmax_active) * kRPanel * kRPanel, &d.dscratch, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.lu_size), &d.lu, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.piv, err)) return false;
   if (!alloc_dev(allocs_, static_cast<size_t>(plan.n), &d.lperm, err)) return false;
@@ -535,7 +537,11 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
       const int dyn = optin - 2048;
-      attr_err = cudaFuncSetAttribute(k_lu_small, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      attr_err = cudaFuncSetAttribute(k_lu_small<kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_lu_small<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_lu_small<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_solve_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     });
@@ -590,7 +596,12 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
       if (q < static_cast<size_t>(kAux)) BDLU_CUDA(cudaStreamWaitEvent(sb, fork_ev_[0], 0));
       const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
       const size_t mb = static_cast<size_t>(p.small_bucket_m[bkt]);
-      k_lu_small<<<q1 - q0, kThreads, mb * mb * sizeof(double), sb>>>(dp_, d_vals, small_list_ + q0);
+      const size_t smem = mb * mb * sizeof(double);
+      // CTA width follows the unit size: narrow CTAs let more small units
+      // run per SM and make the per-column barriers cheaper.
+      if (mb <= 32) k_lu_small<64><<<q1 - q0, 64, smem, sb>>>(dp_, d_vals, small_list_ + q0);
+      else if (mb <= 64) k_lu_small<128><<<q1 - q0, 128, smem, sb>>>(dp_, d_vals, small_list_ + q0);
+      else k_lu_small<kThreads><<<q1 - q0, kThreads, smem, sb>>>(dp_, d_vals, small_list_ + q0);
     }
     for (int q = 0; q < kAux && q < static_cast<int>(nbk); ++q) {
       BDLU_CUDA(cudaEventRecord(aux_ev_[q], aux_[q]));

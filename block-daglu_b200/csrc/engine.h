@@ -37,6 +37,7 @@ struct DevPlan {
   const int32_t* rstep_strip_pref;
   const int32_t* rstep_ga_pref;
   const int32_t* rstep_gb_pref;
+  double* dscratch;  // refactor: factored diagonal block per active unit of a step
   double* lu;
   int32_t* piv;
   int32_t* lperm;   // final row order of each large unit (local indices)

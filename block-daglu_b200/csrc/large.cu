@@ -29,7 +29,7 @@
 // Refactor with the stored pivot order (value-only refactor; the pivot order
 // of KLU's klu_refactor is reused the same way):
 //   k_scatter_large_perm  values scattered with rows already permuted
-//   k_rdiag / k_rstrip / k_rgemm
+//   k_rpanel / k_rgemm
 //                     64-column blocked LU without pivot search, trailing
 //                     update split for one step of lookahead (see below)
 // Solve (per level holding large units):
@@ -716,24 +716,21 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_trsv_tiles(DevPlan dp, con
 // ---------------------------------------------------------------------------
 // Value-only refactor of large units with the stored pivot order: steps of
 // kRPanel (64) columns.  Per step:
-//   k_rdiag   one CTA per unit: LU of the 64 x 64 diagonal block without
-//             pivot search, split in 32 x 32 blocks: LU(D11) by one warp with
-//             the rows in registers (pivot-row values by shuffle), then
-//             U12 = L11^{-1} D12 and L21 = D21 U11^{-1} by two warps (one
-//             column / row per lane), D22 -= L21 U12, and LU(D22) by one
-//             warp.  A zero or non-finite pivot flags the unit for full
-//             pivoting.
-//   k_rstrip  L21 = A21 U11^{-1} (row chunks) and U12 = L11^{-1} A12 (column
-//             chunks) by substitution: four threads per row (column) hold 16
-//             entries each in registers; each finished unknown is broadcast
-//             within the four by a shuffle, so no CTA barrier is needed.
+//   k_rpanel  L21 = A21 U11^{-1} (row chunks) and U12 = L11^{-1} A12 (column
+//             chunks); every CTA first factors the 64 x 64 diagonal block in
+//             shared memory without pivot search (32 x 32 warp LUs with the
+//             rows in registers, two warps for the coupling triangles, one
+//             small product), then solves its strip by substitution (four
+//             threads per line, entries in registers, no barriers).  A zero
+//             or non-finite pivot flags the unit for full pivoting.
 //   k_rgemm   A22 -= L21 U12, K = 64, 128 x 64 tiles, 4 x 8 accumulators per
 //             thread, two CTAs per SM.  Part "a" updates tile row 0 and tile
-//             column 0, which hold the next step's strips; part "b" the rest.
-// Part b of step k runs on a second stream beside the next step's k_rdiag,
-// k_rstrip and part a (depth-1 lookahead); the regions are disjoint: the
-// next step reads and writes rows/columns [base, base + 64) only, part b
-// writes rows >= base + 128 and columns >= base + 64.
+//             column 0, which hold the next step's strips, and places the
+//             factored diagonal block; part "b" updates the rest.
+// Part b of step k runs on a second stream beside the next step's k_rpanel
+// and part a (depth-1 lookahead); the regions are disjoint: the next step
+// reads and writes rows/columns [base, base + 64) only, part b writes rows
+// >= base + 128 and columns >= base + 64.
 constexpr int kRP = kRPanel;
 constexpr int kRS = kRP + 1;
 constexpr int kRThreads = 256;
@@ -779,13 +776,11 @@ __device__ __noinline__ void warp_lu32(double* D, int o, int lane) {
   for (int c = 0; c < kHB; ++c) D[(o + lane) * kRS + o + c] = v[c];
 }
 
-__global__ void __launch_bounds__(kRThreads) k_rdiag(DevPlan dp, int32_t k0, int32_t ubase) {
-  __shared__ double D[kRP * kRS];
-  const int u = dp.rstep_unit[ubase + blockIdx.x];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const int nb = min(kRP, m - k0);
-  double* A = dp.lu + dp.lu_off[u];
+// LU without pivot search of the kRP x kRP diagonal block at (k0, k0) of a
+// row-major m x m unit into shared memory D (stride kRS; rows/columns past nb
+// padded with the identity): LU(D11) by one warp, U12 = L11^{-1} D12 and
+// L21 = D21 U11^{-1} by two warps, D22 -= L21 U12, LU(D22) by one warp.
+__device__ void diag_lu(double* D, const double* A, int m, int k0, int nb) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   // Rows/columns past nb are padded with the identity.
 #pragma unroll
@@ -843,26 +838,27 @@ __global__ void __launch_bounds__(kRThreads) k_rdiag(DevPlan dp, int32_t k0, int
   __syncthreads();
   if (warp == 0) warp_lu32(D, kHB, lane);
   __syncthreads();
-  if (tid < nb) {
-    const double d = D[tid * kRS + tid];
-    if (!(fabs(d) > 0.0) || !isfinite(d)) {
-      if (atomicCAS(dp.status, 0, kFailReusedPivot) == 0) dp.status[1] = u;
-    }
-  }
-#pragma unroll 4
-  for (int e = tid; e < nb * nb; e += kRThreads) {
-    const int i = e / nb, c = e - i * nb;
-    A[static_cast<size_t>(k0 + i) * m + k0 + c] = D[i * kRS + c];
-  }
 }
 
-// Row chunks: rows o0 .. o0+w of L21 from x U11 = a.  Column chunks: columns
-// o0 .. o0+w of U12 from L11 x = b.  Thread (line = tid / 4, quarter qq)
-// holds entries 16qq .. 16qq+15 of its row (column) in registers; the
-// factor's row j of U (column j of L) is staged padded in shared memory.
-__global__ void __launch_bounds__(kRThreads) k_rstrip(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
-  __shared__ __align__(16) double T[kRP * kPadRow];
-  __shared__ double rd[kRP];
+// Panel of one step, fused: every CTA of a unit factors the diagonal block
+// itself (diag_lu, redundantly: the CTAs run side by side, so the
+// factorisation adds no time to the step's dependent chain), then solves its
+// strip.  Row chunks: rows o0 .. o0+w of L21 from x U11 = a.  Column chunks:
+// columns o0 .. o0+w of U12 from L11 x = b.  Thread (line = tid / 4,
+// quarter qq) holds entries 16qq .. 16qq+15 of its row (column) in
+// registers; the factor's row j of U (column j of L) is staged padded in
+// shared memory.  Chunk 0 checks the pivots and leaves the factored block in
+// dp.dscratch (slot = the unit's index in the step); the step's update (part
+// a) copies it into the arena once every CTA here has read the unfactored
+// block.  A unit with nothing left to solve gets one CTA for that.
+constexpr size_t kRPanelSmem =
+    (static_cast<size_t>(kRP) * kRS + static_cast<size_t>(kRP) * kPadRow + kRP) * sizeof(double);
+
+__global__ void __launch_bounds__(kRThreads) k_rpanel(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
+  extern __shared__ double psm[];
+  double* D = psm;                    // kRP x kRS
+  double* T = D + kRP * kRS;          // kRP x kPadRow (16-byte aligned: kRP * kRS is even)
+  double* rd = T + kRP * kPadRow;     // kRP
   int a = 0;
   while (a + 1 < nact && dp.rstep_strip_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
   const int u = dp.rstep_unit[ubase + a];
@@ -874,20 +870,11 @@ __global__ void __launch_bounds__(kRThreads) k_rstrip(DevPlan dp, int32_t k0, in
   const int chunks = (m - base + kRP - 1) / kRP;
   const bool rowc = ch < chunks;
   const int o0 = base + (rowc ? ch : ch - chunks) * kRP;
-  const int w = min(kRP, m - o0);
+  const int w = max(0, min(kRP, m - o0));
   double* A = dp.lu + dp.lu_off[u];
   const int tid = threadIdx.x, lane = tid & 31;
   const int line = tid >> 2, qq = tid & 3;
-  // T[j][18q + t]: rows: U[j][16q + t]; columns: L[16q + t][j].  Past nb the
-  // factor is the identity.
-#pragma unroll
-  for (int e = tid; e < kRP * kRP; e += kRThreads) {
-    const int j = e / kRP, c = e - j * kRP;
-    double v;
-    if (rowc) v = (j < nb && c < nb) ? A[static_cast<size_t>(k0 + j) * m + k0 + c] : (j == c ? 1.0 : 0.0);
-    else v = (j < nb && c < nb) ? A[static_cast<size_t>(k0 + c) * m + k0 + j] : (j == c ? 1.0 : 0.0);
-    T[j * kPadRow + 18 * (c >> 4) + (c & 15)] = v;
-  }
+  // The strip's entries go to registers first (their loads overlap the LU).
   double x[16];
   const bool live = line < w;
 #pragma unroll
@@ -898,8 +885,25 @@ __global__ void __launch_bounds__(kRThreads) k_rstrip(DevPlan dp, int32_t k0, in
       v = rowc ? A[static_cast<size_t>(o0 + line) * m + k0 + q] : A[static_cast<size_t>(k0 + q) * m + o0 + line];
     x[t] = v;
   }
+  diag_lu(D, A, m, k0, nb);
   __syncthreads();
-  if (rowc && tid < kRP) rd[tid] = 1.0 / T[tid * kPadRow + 18 * (tid >> 4) + (tid & 15)];
+  if (ch == 0) {
+    if (tid < nb) {
+      const double d = D[tid * kRS + tid];
+      if (!(fabs(d) > 0.0) || !isfinite(d)) {
+        if (atomicCAS(dp.status, 0, kFailReusedPivot) == 0) dp.status[1] = u;
+      }
+    }
+    double* out = dp.dscratch + static_cast<size_t>(a) * kRP * kRP;
+#pragma unroll 4
+    for (int e = tid; e < kRP * kRP; e += kRThreads) out[e] = D[(e / kRP) * kRS + (e % kRP)];
+  }
+  // T[j][18q + t]: rows: U[j][16q + t]; columns: L[16q + t][j].
+  for (int e = tid; e < kRP * kRP; e += kRThreads) {
+    const int j = e / kRP, c = e - j * kRP;
+    T[j * kPadRow + 18 * (c >> 4) + (c & 15)] = rowc ? D[j * kRS + c] : D[c * kRS + j];
+  }
+  if (rowc && tid < kRP) rd[tid] = 1.0 / D[tid * kRS + tid];
   __syncthreads();
   const int src = (lane & ~3);
   for (int jq = 0; jq < 4; ++jq) {
@@ -929,6 +933,16 @@ __global__ void __launch_bounds__(kRThreads) k_rstrip(DevPlan dp, int32_t k0, in
   }
 }
 
+// Copies the factored diagonal block of step k0 (left by k_rpanel in
+// dp.dscratch slot a) into the arena; run by the first part-a CTA of a unit.
+__device__ __forceinline__ void place_diag(const DevPlan& dp, double* A, int m, int k0, int nb, int a) {
+  const double* src = dp.dscratch + static_cast<size_t>(a) * kRP * kRP;
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int i = e / nb, c = e - i * nb;
+    A[static_cast<size_t>(k0 + i) * m + k0 + c] = src[i * kRP + c];
+  }
+}
+
 __global__ void __launch_bounds__(kRThreads, 2) k_rgemm(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
                                                         int32_t part) {
   extern __shared__ double rsm[];
@@ -945,6 +959,10 @@ __global__ void __launch_bounds__(kRThreads, 2) k_rgemm(DevPlan dp, int32_t k0, 
   const int base = k0 + nb;
   const int rest = m - base;
   const int ntj = (rest + kRTileN - 1) / kRTileN;
+  if (part == 0 && t == 0) {
+    place_diag(dp, dp.lu + dp.lu_off[u], m, k0, nb, a);
+    if (rest <= 0) return;
+  }
   int ti, tj;
   if (part == 0) {
     if (t < ntj) {
@@ -1150,6 +1168,10 @@ __global__ void __launch_bounds__(kRThreads) k_rgemm_tf32(DevPlan dp, int32_t k0
   const int base = k0 + nb;
   const int rest = m - base;
   const int ntj = (rest + kRTileN - 1) / kRTileN;
+  if (part == 0 && t == 0) {
+    place_diag(dp, dp.lu + dp.lu_off[u], m, k0, nb, a);
+    if (rest <= 0) return;
+  }
   int ti, tj;
   if (part == 0) {
     if (t < ntj) {
@@ -1205,6 +1227,8 @@ cudaError_t large_setup() {
     err = cudaFuncSetAttribute(k_gemm_rm, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kGemmSmem));
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_rgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kRGemmSmem));
+    if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_rpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kRPanelSmem));
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_trsv_tiles<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(trsv_smem<16>()));
@@ -1300,13 +1324,9 @@ cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cu
     const int32_t na = p.rstep_ptr[static_cast<size_t>(st) + 1] - ub;
     if (na <= 0) continue;
     const int32_t k0 = st * kRPanel;
-    k_rdiag<<<na, kRThreads, 0, sa>>>(dp, k0, ub);
-    ++*launches;
     const int32_t ns = p.rstep_strip_total[static_cast<size_t>(st)];
-    if (ns > 0) {
-      k_rstrip<<<ns, kRThreads, 0, sa>>>(dp, k0, ub, na);
-      ++*launches;
-    }
+    k_rpanel<<<ns, kRThreads, kRPanelSmem, sa>>>(dp, k0, ub, na);
+    ++*launches;
     // Part a of this step follows part b of the previous one (stream b so
     // far); part b of this step follows this step's strips (stream a so far).
     if ((e = cudaEventRecord(ev_b, sb)) != cudaSuccess) return e;

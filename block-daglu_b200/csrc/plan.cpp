@@ -235,8 +235,8 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
       p.rstep_strip_pref.push_back(spre);
       p.rstep_ga_pref.push_back(apre);
       p.rstep_gb_pref.push_back(bpre);
-      spre += 2 * chunks;
-      apre += rest > 0 ? nti + ntj - 1 : 0;
+      spre += std::max(1, 2 * chunks);        // at least one CTA factors the diagonal block
+      apre += rest > 0 ? nti + ntj - 1 : 1;   // part a places the factored block
       bpre += rest > 0 ? (nti - 1) * (ntj - 1) : 0;
       ++act;
     }

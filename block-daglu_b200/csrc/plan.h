@@ -78,9 +78,10 @@ struct Plan {
   std::vector<int32_t> step_max_rows;                     // per step: largest m - k0
   // Value-only refactor of large units (stored pivot order, no pivot
   // search): steps of kRPanel columns.  Per step and active unit: CTA
-  // prefixes of the strip kernel (row chunks then column chunks of kRPanel),
-  // of the update tiles that cover the next step's strips ("a": tile row 0
-  // and tile column 0) and of the remaining tiles ("b").
+  // prefixes of the panel kernel (row chunks then column chunks of kRPanel,
+  // at least one), of the update tiles that cover the next step's strips
+  // ("a": tile row 0 and tile column 0, at least one, which places the
+  // factored diagonal block) and of the remaining tiles ("b").
   int32_t rsteps = 0;
   int32_t rmax_active = 0;
   std::vector<int32_t> rstep_ptr, rstep_unit;
