@@ -405,8 +405,13 @@ int32_t small_unit_max() {
 }
 
 Engine::Engine() {
-  cudaStreamCreateWithFlags(&cap_stream_, cudaStreamNonBlocking);
-  cudaStreamCreateWithFlags(&cap_stream2_, cudaStreamNonBlocking);
+  // The refactor graph's dependent chain is captured on the highest-priority
+  // stream and its lookahead branch on the lowest, so waiting chain CTAs are
+  // scheduled ahead of the branch's (the graph keeps node priorities).
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  cudaStreamCreateWithPriority(&cap_stream_, cudaStreamNonBlocking, prio_high);
+  cudaStreamCreateWithPriority(&cap_stream2_, cudaStreamNonBlocking, prio_low);
   for (auto& a : aux_) cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking);
   for (auto& e : aux_ev_) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (auto& e : fork_ev_) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
@@ -630,7 +635,7 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
       const cudaError_t ee = cudaStreamEndCapture(cap_stream_, &g);
       BDLU_CUDA(ce);
       BDLU_CUDA(ee);
-      const cudaError_t ie = cudaGraphInstantiate(&reuse_exec_, g, 0);
+      const cudaError_t ie = cudaGraphInstantiate(&reuse_exec_, g, cudaGraphInstantiateFlagUseNodePriority);
       cudaGraphDestroy(g);
       BDLU_CUDA(ie);
       reuse_launches_ = n_launch + 1;
