@@ -716,22 +716,46 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_
   const Plan& p = plan_;
   const int32_t nl = p.umax_level + 1;
   if (p.large_tiles > 0) cudaMemsetAsync(d_sync_, 0, static_cast<size_t>(sync_words_) * sizeof(int32_t), stream);
+  // Within a level the scalar rows, the small dense units and the large
+  // units are independent: when a level has more than one kind, the others
+  // run on auxiliary streams forked from `stream` and joined back, so the
+  // level costs about its slowest part instead of their sum.
   for (int32_t l = 0; l < nl; ++l) {
     const int32_t s0 = p.lvl_scalar_ptr[static_cast<size_t>(l)], s1 = p.lvl_scalar_ptr[static_cast<size_t>(l) + 1];
     const int32_t d0 = p.lvl_dense_ptr[static_cast<size_t>(l)], d1 = p.lvl_dense_ptr[static_cast<size_t>(l) + 1];
-    if (s1 > s0) {
+    const int32_t g0 = p.lvl_large_ptr[static_cast<size_t>(l)], g1 = p.lvl_large_ptr[static_cast<size_t>(l) + 1];
+    const bool has_s = s1 > s0, has_d = d1 > d0, has_g = g1 > g0;
+    const int kinds = static_cast<int>(has_s) + static_cast<int>(has_d) + static_cast<int>(has_g);
+    cudaStream_t st_s = stream, st_d = stream, st_g = stream;
+    if (kinds > 1) {
+      cudaEventRecord(fork_ev_[0], stream);
+      int used = 0;
+      if (has_d && (has_s)) st_d = aux_[used++];
+      if (has_g && (has_s || has_d)) st_g = aux_[used++];
+      for (int q = 0; q < used; ++q) cudaStreamWaitEvent(aux_[q], fork_ev_[0], 0);
+    }
+    if (has_s) {
       ++launches_solve_;
       const int warps_per_cta = kThreads / 32;
-      k_solve_scalar<<<(s1 - s0 + warps_per_cta - 1) / warps_per_cta, kThreads, 0, stream>>>(
+      k_solve_scalar<<<(s1 - s0 + warps_per_cta - 1) / warps_per_cta, kThreads, 0, st_s>>>(
           dp_, lvl_scalar_ + s0, s1 - s0, rhs, ldr, xp, nrhs);
     }
-    if (d1 > d0) ++launches_solve_;
-    if (d1 > d0) {
+    if (has_d) {
+      ++launches_solve_;
       const size_t mm = static_cast<size_t>(p.lvl_dense_maxm[static_cast<size_t>(l)]);
-      k_solve_dense<<<d1 - d0, kThreads, mm * mm * sizeof(double), stream>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp, nrhs);
+      k_solve_dense<<<d1 - d0, kThreads, mm * mm * sizeof(double), st_d>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp, nrhs);
     }
-    large_solve_level(dp_, p, l, lvl_large_, lvl_large_tile0_, d_sync_, rhs, ldr, xp, nrhs, wide, stream,
+    large_solve_level(dp_, p, l, lvl_large_, lvl_large_tile0_, d_sync_, rhs, ldr, xp, nrhs, wide, st_g,
                       &launches_solve_);
+    if (kinds > 1) {
+      int q = 0;
+      for (cudaStream_t sx : {st_d, st_g}) {
+        if (sx == stream) continue;
+        cudaEventRecord(aux_ev_[q], sx);
+        cudaStreamWaitEvent(stream, aux_ev_[q], 0);
+        ++q;
+      }
+    }
   }
 }
 
