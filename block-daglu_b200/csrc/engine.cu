@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int3
                                                            double* __restrict__ xp,
                                                            const int32_t* __restrict__ nrhs_p) {
   const int32_t nrhs = *nrhs_p;
-  extern __shared__ double T[];
+  extern __shared__ __align__(16) double T[];
   const int u = units[blockIdx.x];
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
@@ -228,12 +228,47 @@ __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int3
       }
     }
   };
-  if (nmine > 0) form(warp);
+  // The unit's factor slot is contiguous and 256-byte aligned: one bulk
+  // copy (TMA) stages it while the warps form their right-hand sides.
+  __shared__ __align__(8) uint64_t mbar;
   const double* LU = dp.lu + dp.lu_off[u];
-  const int mm = m * m;
-#pragma unroll 4
-  for (int e = tid; e < mm; e += kThreads) T[e] = LU[e];
+  const uint32_t bytes = static_cast<uint32_t>((m * m + 1) / 2) * 16u;  // slots are padded to 32 doubles
+  const uint32_t mbar_s = static_cast<uint32_t>(__cvta_generic_to_shared(&mbar));
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_s));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
   __syncthreads();
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar_s), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            static_cast<uint32_t>(__cvta_generic_to_shared(T))),
+        "l"(LU), "r"(bytes), "r"(mbar_s)
+        : "memory");
+  }
+  if (nmine > 0) form(warp);
+  // Bounded wait for the copy (phase 0); on a timeout the unit reports a
+  // synchronisation failure, waits once more for the copy in flight, and
+  // skips its sweeps.
+  bool staged = false;
+  for (int pass = 0; pass < 2 && !staged; ++pass) {
+    for (int it = 0; it < (1 << 22); ++it) {
+      uint32_t done = 0;
+      asm volatile(
+          "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+          : "=r"(done)
+          : "r"(mbar_s)
+          : "memory");
+      if (done) {
+        staged = true;
+        break;
+      }
+    }
+    if (!staged && pass == 0 && tid == 0) atomicCAS(dp.status, 0, kFailSync);
+  }
+  __syncthreads();
+  if (!staged) return;
   for (int t = 0; t < nmine; ++t) {
     const int c = warp + t * kWarps;
     if (t > 0) form(c);
@@ -743,7 +778,8 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_
     if (has_d) {
       ++launches_solve_;
       const size_t mm = static_cast<size_t>(p.lvl_dense_maxm[static_cast<size_t>(l)]);
-      k_solve_dense<<<d1 - d0, kThreads, mm * mm * sizeof(double), st_d>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp, nrhs);
+      k_solve_dense<<<d1 - d0, kThreads, mm * mm * sizeof(double) + 16, st_d>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp,
+                                                                                nrhs);
     }
     large_solve_level(dp_, p, l, lvl_large_, lvl_large_tile0_, d_sync_, rhs, ldr, xp, nrhs, wide, st_g,
                       &launches_solve_);
