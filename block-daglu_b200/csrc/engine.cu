@@ -54,14 +54,24 @@ __global__ void k_set_i32(int32_t* p, int32_t v) { *p = v; }
 // ---------------------------------------------------------------------------
 // Dense LU of one unit in shared memory (column-major, leading dimension m).
 // ---------------------------------------------------------------------------
+// Warp-level pivot candidate: the largest |v| (ties to the smallest row,
+// rows with i == none taking no part) and the signed value of that entry.
+__device__ __forceinline__ void warp_pivot_signed(double v, int i, int none, double& best, int& bi, double& sv) {
+  double a = (i == none) ? 0.0 : fabs(v);
+  int idx = i;
+  warp_pivot_reduce(a, idx, none);
+  const unsigned who = __ballot_sync(0xffffffffu, i != none && i == idx);
+  sv = __shfl_sync(0xffffffffu, v, who ? __ffs(who) - 1 : 0);
+  best = a;
+  bi = idx;
+}
+
 template <int kT>
 __global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __restrict__ vals,
-                                                        const int32_t* __restrict__ units) {
+                                                  const int32_t* __restrict__ units) {
   extern __shared__ double A[];
-  __shared__ double s_best[kT / 32];
+  __shared__ double s_best[kT / 32], s_val[kT / 32];
   __shared__ int s_bi[kT / 32];
-  __shared__ int s_piv;
-  __shared__ double s_pbest;
   const int u = units[blockIdx.x];
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
@@ -72,58 +82,82 @@ __global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __res
   for (int64_t e = dp.dent_ptr[u] + tid; e < dp.dent_ptr[u + 1]; e += kT) A[dp.dent_pos[e]] = vals[dp.dent_src[e]];
   __syncthreads();
   int32_t* piv = dp.piv + s;
-  for (int k = 0; k < m; ++k) {
-    double* colk = A + static_cast<size_t>(k) * m;
-    // Pivot: each warp scans a strided share of rows k..m-1.
-    double best = 0.0;
-    int bi = m;
-    for (int i = k + tid; i < m; i += kT) {
-      const double a = fabs(colk[i]);
-      if (bi == m || a > best) {
-        best = a;
-        bi = i;
-      }
-    }
-    warp_pivot_reduce(best, bi, m);
+  // Two barriers per column.  Pivot candidates of column k (first strict
+  // maximum of |a|, with the signed value) come from the update of step k-1
+  // (column 0: scanned first); after the barrier every thread combines the
+  // per-warp candidates itself.  The row swap and the multipliers of column k
+  // then run in one phase (the multipliers read the pivot row before the
+  // swap: a'_pk = a_kk); the update of step k also collects column k+1's
+  // candidates.  The arithmetic is the reference micro-kernel's, operation
+  // for operation.  A lane keeps the first strict maximum of its rows.
+  {
+    const int i = (tid < m) ? tid : m;
+    double best, sv;
+    int bi;
+    warp_pivot_signed(i < m ? A[i] : 0.0, i, m, best, bi, sv);
     if (lane == 0) {
       s_best[warp] = best;
       s_bi[warp] = bi;
+      s_val[warp] = sv;
     }
-    __syncthreads();
-    if (warp == 0) {
-      best = (lane < kT / 32) ? s_best[lane] : 0.0;
-      bi = (lane < kT / 32) ? s_bi[lane] : m;
-      warp_pivot_reduce(best, bi, m);
-      if (lane == 0) {
-        s_piv = bi;
-        s_pbest = best;
+  }
+  __syncthreads();
+  for (int k = 0; k < m; ++k) {
+    double best = s_best[0], pv = s_val[0];
+    int p = s_bi[0];
+#pragma unroll
+    for (int w = 1; w < kT / 32; ++w) {
+      const double ob = s_best[w];
+      const int oi = s_bi[w];
+      if (oi != m && (p == m || ob > best || (ob == best && oi < p))) {
+        best = ob;
+        p = oi;
+        pv = s_val[w];
       }
     }
-    __syncthreads();
-    const int p = s_piv;
-    if (s_pbest == 0.0) {
+    if (p == m || best == 0.0) {
       if (tid == 0) report_failure(dp.status, u);
       return;
     }
+    double* colk = A + static_cast<size_t>(k) * m;
     if (tid == 0) piv[k] = p;
+    const double akk = colk[k];
     if (p != k) {
       for (int j = tid; j < m; j += kT) {
+        if (j == k) continue;
         double* c = A + static_cast<size_t>(j) * m;
         const double t = c[k];
         c[k] = c[p];
         c[p] = t;
       }
     }
+    for (int i = k + 1 + tid; i < m; i += kT) colk[i] = __ddiv_rn(i == p ? akk : colk[i], pv);
     __syncthreads();
-    const double akk = colk[k];
-    for (int i = k + 1 + tid; i < m; i += kT) colk[i] = __ddiv_rn(colk[i], akk);
-    __syncthreads();
-    const int r = m - k - 1;
-    for (int t = tid; t < r * r; t += kT) {
-      const int jj = t / r, ii = t - jj * r;
-      const int i = k + 1 + ii, j = k + 1 + jj;
+    if (tid == 0) colk[k] = pv;
+    // Update: warp per column (column k+1 is warp 0's, which also yields the
+    // next pivot candidates), lane per row.
+    double cb = 0.0, cv = 0.0;
+    int ci = m;
+    for (int j = k + 1 + warp; j < m; j += kT / 32) {
       double* c = A + static_cast<size_t>(j) * m;
-      c[i] = __dsub_rn(c[i], __dmul_rn(colk[i], c[k]));
+      const double ukj = c[k];
+      for (int i = k + 1 + lane; i < m; i += 32) {
+        const double v = __dsub_rn(c[i], __dmul_rn(colk[i], ukj));
+        c[i] = v;
+        if (j == k + 1 && (ci == m || fabs(v) > cb)) {
+          cb = fabs(v);
+          cv = v;
+          ci = i;
+        }
+      }
+    }
+    double nb, nsv;
+    int nbi;
+    warp_pivot_signed(cv, ci, m, nb, nbi, nsv);
+    if (lane == 0) {
+      s_best[warp] = nb;
+      s_bi[warp] = nbi;
+      s_val[warp] = nsv;
     }
     __syncthreads();
   }
