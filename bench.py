@@ -84,6 +84,8 @@ def parse():
     ap.add_argument("--rate", type=float, default=2000.0, help="serve-64: Poisson arrival rate (requests/s)")
     ap.add_argument("--duration", type=float, default=5.0, help="serve-64: seconds of open-loop arrivals")
     ap.add_argument("--slots", type=int, default=8, help="serve-64: concurrent request slots")
+    ap.add_argument("--refactor-schedule", type=int, default=0, choices=[0, 1],
+                    help="circuit-200k: large-block refactor as a step chain (0) or one tile task graph (1)")
     return ap.parse_args()
 
 
@@ -655,6 +657,7 @@ def main():
     stream = torch.cuda.current_stream(dev)
     g = circuit_system()
     s = bd.Solver()
+    assert s.set_option("refactor_schedule", args.refactor_schedule)
     assert s.set_matrix((g.rows, g.cols, g.vals), g.n), s.last_error_message()
     t0 = time.perf_counter()
     assert s.analyze(), s.last_error_message()
@@ -764,7 +767,8 @@ def main():
         achieved = flops_large / (ph["lu_small"] + ph["lu_large"]) / 1e9
         roofline = {"bound": "tensor", "achieved": achieved, "peak": dgemm, "unit": "TFLOP/s",
                     "frac": achieved / dgemm if dgemm else None, "traffic": None,
-                    "kernel": "dense block LU phases (k_lu_small; value-only refactor k_rdiag / k_rstrip / k_rgemm), FP64",
+                    "kernel": "dense block LU phases (k_lu_small; value-only refactor: k_rdag tile task graph, "
+                              "or k_rpanel / k_rgemm step chain), FP64",
                     "peak_source": "FP64 pipe: torch.matmul float64 8192^3 measured in this run "
                                    "(MEASURED_PEAKS.json has no FP64 figure)"}
     cpu = None
@@ -778,6 +782,7 @@ def main():
                    "nunits": first["nunits"], "max_block": first["max_unit"], "unit_levels": first["unit_levels"],
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "flushed (256 MiB write) between timed steps, outside the step window",
+                   "refactor_schedule": "step chain" if args.refactor_schedule == 0 else "task graph",
                    "analyze_s": analyze_s},
         "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8 * nnz + 8 * g.n, "d2h_bytes_per_step": 8 * g.n},
         "phases_ms": ph,

@@ -79,6 +79,7 @@ int ensure_validated(bdlu_solver* h) {
 int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
+  h->engine->set_refactor_schedule(h->refactor_schedule);
   for (int attempt = 0; attempt < 2; ++attempt) {
     const bool r = reuse && attempt == 0;
     if (!h->engine->factor_async(h->engine->values_buffer(), stream, err, r))
@@ -460,6 +461,12 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
   }
   if (k == "refactor_pivoting") {
     h->reuse_pivots = value == 0.0;
+    return BDLU_OK;
+  }
+  if (k == "refactor_schedule") {
+    if (value != 0.0 && value != 1.0) return BDLU_INVALID_DIMENSION;
+    h->refactor_schedule = static_cast<int32_t>(value);
+    if (h->engine) h->engine->set_refactor_schedule(h->refactor_schedule);
     return BDLU_OK;
   }
   if (k == "analysis_only") {

@@ -34,6 +34,7 @@ struct bdlu_solver {
   bool reuse_pivots = true;   // value-only refactors keep the pivot order of large blocks
   bool mixed = false;         // "precision" = 1: tensor-core updates + FP64 refinement
   int32_t prec_level = 1;     // mixed route's current level: 1 TF32, 2 3xTF32, 0 FP64 (sticky)
+  int32_t refactor_schedule = 0;  // 0 step chain, 1 tile task graph (Engine::set_refactor_schedule)
   // Error state (solver.h:122-123).
   int last_error = BDLU_OK;
   std::string last_message;

@@ -524,6 +524,8 @@ void Engine::release() {
   d_status_ = nullptr;
   d_b0_ = d_xp_ = d_r_ = d_rhs_ = nullptr;
   d_norms_ = nullptr;
+  d_rtask_ = nullptr;
+  d_rwords_ = nullptr;
   work_nrhs_ = 0;
   dp_ = DevPlan{};
 }
@@ -641,6 +643,10 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   sync_words_ = large_sync_words(plan);
   if (!alloc_dev(allocs_, static_cast<size_t>(sync_words_), &d_sync_, err)) return false;
   if (!alloc_dev(allocs_, 1, &d_nrhs_, err)) return false;
+  if (plan.rtasks > 0) {
+    if (!upload_vec(allocs_, plan.rtask, &d_rtask_, err)) return false;
+    if (!alloc_dev(allocs_, static_cast<size_t>(plan.rt_words), &d_rwords_, err)) return false;
+  }
   small_list_ = small_list;
   large_list_ = large_list;
   lvl_scalar_ = lvl_scalar;
@@ -684,7 +690,7 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   }
   BDLU_CUDA(cudaEventRecord(pev_[1], stream));
   if (!p.large_units.empty() && reuse) {
-    if (reuse_exec_ && reuse_prec_ != prec_) {
+    if (reuse_exec_ && (reuse_prec_ != prec_ || reuse_schedule_ != schedule_)) {
       cudaGraphExecDestroy(reuse_exec_);
       reuse_exec_ = nullptr;
     }
@@ -698,8 +704,12 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
       cudaMemsetAsync(dp_.lu + p.lu_large_begin, 0,
                       static_cast<size_t>(p.lu_large_end - p.lu_large_begin) * sizeof(double), cap_stream_);
       cudaError_t ce = large_scatter_reuse(dp_, p, d_vals, large_list_, cap_stream_);
-      if (ce == cudaSuccess)
-        ce = large_refactor(dp_, p, cap_stream_, cap_stream2_, fork_ev_[0], fork_ev_[1], &n_launch, prec_);
+      if (ce == cudaSuccess) {
+        if (prec_ == 0 && schedule_ == 1 && p.rtasks > 0)
+          ce = large_refactor_dag(dp_, p, d_rtask_, d_rwords_, cap_stream_, &n_launch);
+        else
+          ce = large_refactor(dp_, p, cap_stream_, cap_stream2_, fork_ev_[0], fork_ev_[1], &n_launch, prec_);
+      }
       cudaGraph_t g = nullptr;
       const cudaError_t ee = cudaStreamEndCapture(cap_stream_, &g);
       BDLU_CUDA(ce);
@@ -709,6 +719,7 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
       BDLU_CUDA(ie);
       reuse_launches_ = n_launch + 1;
       reuse_prec_ = prec_;
+      reuse_schedule_ = schedule_;
     }
     BDLU_CUDA(cudaGraphLaunch(reuse_exec_, stream));
     launches_factor_ += reuse_launches_;
@@ -740,6 +751,12 @@ int Engine::factor_status(cudaStream_t stream, std::string& err) {
   }
   if (st[0] == kFailReusedPivot) {
     err = "reused pivot order met a zero pivot in diagonal block " + std::to_string(st[1]);
+    return 2;
+  }
+  if (st[0] == kFailRefactorSync) {
+    // Only the tile-graph refactor (stored pivot order) sets this; the
+    // caller redoes the factor with pivoting, which does not use it.
+    err = "refactor task graph: a bounded wait between tiles ran out";
     return 2;
   }
   if (!last_reuse_) have_pivots_ = true;

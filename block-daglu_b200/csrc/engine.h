@@ -93,6 +93,10 @@ class Engine {
   // 0 FP64, 1 TF32 tensor cores, 2 3xTF32.
   void set_precision(int32_t prec) { prec_ = prec; }
   int32_t precision() const { return prec_; }
+  // Schedule of the FP64 value-only refactor of large units: 0 the step
+  // chain (panel and update launches on two graph branches), 1 one
+  // persistent kernel over the tile task graph (when the plan has one).
+  void set_refactor_schedule(int32_t s) { schedule_ = s; }
   // Residual norms of the last solve (synchronises the stream), worst column.
   bool last_residual(cudaStream_t stream, SolveResidual& out, std::string& err);
 
@@ -121,6 +125,10 @@ class Engine {
   void refine_core(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream);
   int32_t prec_ = 0;
   int32_t reuse_prec_ = 0;
+  int32_t schedule_ = 0;
+  int32_t reuse_schedule_ = 0;
+  const int32_t* d_rtask_ = nullptr;  // task list of the tile-graph refactor (4 words per task)
+  int32_t* d_rwords_ = nullptr;       // its ticket and tile version words
 
   Plan plan_;
   DevPlan dp_{};

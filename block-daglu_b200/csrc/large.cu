@@ -717,10 +717,9 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_trsv_tiles(DevPlan dp, con
 // Value-only refactor of large units with the stored pivot order: steps of
 // kRPanel (64) columns.  Per step:
 //   k_rpanel  L21 = A21 U11^{-1} (row chunks) and U12 = L11^{-1} A12 (column
-//             chunks); every CTA first factors the 64 x 64 diagonal block in
-//             shared memory without pivot search (32 x 32 warp LUs with the
-//             rows in registers, two warps for the coupling triangles, one
-//             small product), then solves its strip by substitution (four
+//             chunks); every CTA first factors the 64 x 64 diagonal block
+//             without pivot search (diag_lu: rows in registers, one barrier
+//             per column), then solves its strip by substitution (four
 //             threads per line, entries in registers, no barriers).  A zero
 //             or non-finite pivot flags the unit for full pivoting.
 //   k_rgemm   A22 -= L21 U12, K = 64, 128 x 64 tiles, 4 x 8 accumulators per
@@ -734,7 +733,6 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_trsv_tiles(DevPlan dp, con
 constexpr int kRP = kRPanel;
 constexpr int kRS = kRP + 1;
 constexpr int kRThreads = 256;
-constexpr int kHB = kRP / 2;
 constexpr int kPadRow = 72;    // padded 64-entry row: quarter q at offset 18q (16-byte loads, no conflicts)
 constexpr int kRAS = kRP + 1;  // As row stride in k_rgemm
 constexpr size_t kRGemmSmem = (static_cast<size_t>(kRTileM) * kRAS + static_cast<size_t>(kRP) * kRTileN) * sizeof(double);
@@ -753,151 +751,99 @@ __device__ __forceinline__ double pivot_rcp(double d) {
   return fma(r, e, r);
 }
 
-// LU without pivot search of the 32 x 32 block at (o, o) of D, by one warp:
-// lane i keeps row i in registers; step j takes the pivot row's entries from
-// lane j by shuffle.  Not inlined: the unrolled body is large and is called
-// twice per diagonal block.
-__device__ __noinline__ void warp_lu32(double* D, int o, int lane) {
-  double v[kHB];
-#pragma unroll
-  for (int c = 0; c < kHB; ++c) v[c] = D[(o + lane) * kRS + o + c];
-#pragma unroll
-  for (int j = 0; j < kHB; ++j) {
-    const double r = pivot_rcp(__shfl_sync(0xffffffffu, v[j], j));
-    if (lane > j) v[j] *= r;
-    const double l = v[j];
-#pragma unroll
-    for (int c = j + 1; c < kHB; ++c) {
-      const double u = __shfl_sync(0xffffffffu, v[c], j);
-      if (lane > j) v[c] = fma(-l, u, v[c]);
-    }
-  }
-#pragma unroll
-  for (int c = 0; c < kHB; ++c) D[(o + lane) * kRS + o + c] = v[c];
-}
-
 // LU without pivot search of the kRP x kRP diagonal block at (k0, k0) of a
 // row-major m x m unit into shared memory D (stride kRS; rows/columns past nb
-// padded with the identity): LU(D11) by one warp, U12 = L11^{-1} D12 and
-// L21 = D21 U11^{-1} by two warps, D22 -= L21 U12, LU(D22) by one warp.
+// padded with the identity).  Thread t keeps 16 entries of row i = t / 4 in
+// registers (columns (t % 4) + 4q); the pivot row and its reciprocal go
+// through a double-buffered shared row, one barrier per column; the row's
+// multiplier comes from the lane that holds column j by shuffle.  The owner
+// of the next pivot row publishes it right after its own update, so the
+// dependent chain per column is barrier, shuffle, multiply, update, store.
+// RowsLU<JQ> handles columns 4JQ .. 4JQ+3 (register indices compile-time).
+template <int JQ>
+struct RowsLU {
+  static __device__ __forceinline__ void run(double (&v)[16], double (*prow)[kRP], double* rinv, int i, int sub,
+                                             int lane) {
+#pragma unroll 1
+    for (int s = 0; s < 4; ++s) {
+      const int j = 4 * JQ + s;
+      __syncthreads();
+      const double* pr = prow[j & 1];
+      const double r = rinv[j & 1];
+      const double a = __shfl_sync(0xffffffffu, v[JQ], (lane & ~3) | s);
+      if (i > j) {
+        const double l = a * r;
+        if (sub == s) v[JQ] = l;
+        if (sub > s) v[JQ] = fma(-l, pr[sub + 4 * JQ], v[JQ]);
+#pragma unroll
+        for (int q = JQ + 1; q < 16; ++q) v[q] = fma(-l, pr[sub + 4 * q], v[q]);
+      }
+      if (i == j + 1) {
+        // Row j + 1 is final: publish it and its pivot's reciprocal (the
+        // pivot is column j + 1: register JQ, or JQ + 1 after s = 3).
+#pragma unroll
+        for (int q = JQ; q < 16; ++q) prow[(j + 1) & 1][sub + 4 * q] = v[q];
+        if (sub == ((j + 1) & 3)) rinv[(j + 1) & 1] = pivot_rcp(s == 3 ? v[JQ < 15 ? JQ + 1 : 15] : v[JQ]);
+      }
+    }
+    RowsLU<JQ + 1>::run(v, prow, rinv, i, sub, lane);
+  }
+};
+template <>
+struct RowsLU<16> {
+  static __device__ __forceinline__ void run(double (&)[16], double (*)[kRP], double*, int, int, int) {}
+};
+static_assert(kRP == 64 && kRThreads == 256, "diag_lu: four threads per row, 16 entries each");
+
 __device__ void diag_lu(double* D, const double* A, int m, int k0, int nb) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // Rows/columns past nb are padded with the identity.
+  __shared__ double prow[2][kRP];
+  __shared__ double rinv[2];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int i = tid >> 2, sub = tid & 3;
+  double v[16];
 #pragma unroll
-  for (int e = tid; e < kRP * kRP; e += kRThreads) {
-    const int i = e / kRP, c = e - i * kRP;
-    D[i * kRS + c] = (i < nb && c < nb) ? A[static_cast<size_t>(k0 + i) * m + k0 + c] : (i == c ? 1.0 : 0.0);
+  for (int q = 0; q < 16; ++q) {
+    const int c = sub + 4 * q;
+    v[q] = (i < nb && c < nb) ? __ldcg(A + static_cast<size_t>(k0 + i) * m + k0 + c) : (i == c ? 1.0 : 0.0);
   }
-  __syncthreads();
-  if (warp == 0) warp_lu32(D, 0, lane);
-  __syncthreads();
-  if (warp == 0) {
-    // U12 = L11^{-1} D12: lane = column kHB + lane.
-    double x[kHB];
+  if (i == 0) {
 #pragma unroll
-    for (int r = 0; r < kHB; ++r) x[r] = D[r * kRS + kHB + lane];
-#pragma unroll
-    for (int j = 0; j < kHB; ++j)
-#pragma unroll
-      for (int r = j + 1; r < kHB; ++r) x[r] = fma(-D[r * kRS + j], x[j], x[r]);
-#pragma unroll
-    for (int r = 0; r < kHB; ++r) D[r * kRS + kHB + lane] = x[r];
-  } else if (warp == 1) {
-    // L21 = D21 U11^{-1}: lane = row kHB + lane; the pivot reciprocals are
-    // formed first, off the substitution's dependent chain.
-    double x[kHB];
-    const double rdl = 1.0 / D[lane * kRS + lane];
-#pragma unroll
-    for (int c = 0; c < kHB; ++c) x[c] = D[(kHB + lane) * kRS + c];
-#pragma unroll
-    for (int j = 0; j < kHB; ++j) {
-      x[j] *= __shfl_sync(0xffffffffu, rdl, j);
-#pragma unroll
-      for (int c = j + 1; c < kHB; ++c) x[c] = fma(-x[j], D[j * kRS + c], x[c]);
-    }
-#pragma unroll
-    for (int c = 0; c < kHB; ++c) D[(kHB + lane) * kRS + c] = x[c];
+    for (int q = 0; q < 16; ++q) prow[0][sub + 4 * q] = v[q];
+    if (sub == 0) rinv[0] = pivot_rcp(v[0]);
   }
-  __syncthreads();
-  {
-    // D22 -= L21 U12: thread = row r, columns cb + 8b.
-    const int r = tid >> 3, cb = tid & 7;
-    double acc[4];
+  RowsLU<0>::run(v, prow, rinv, i, sub, lane);
 #pragma unroll
-    for (int b = 0; b < 4; ++b) acc[b] = D[(kHB + r) * kRS + kHB + cb + 8 * b];
-#pragma unroll 8
-    for (int q = 0; q < kHB; ++q) {
-      const double l = D[(kHB + r) * kRS + q];
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[b] = fma(-l, D[q * kRS + kHB + cb + 8 * b], acc[b]);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int b = 0; b < 4; ++b) D[(kHB + r) * kRS + kHB + cb + 8 * b] = acc[b];
-  }
-  __syncthreads();
-  if (warp == 0) warp_lu32(D, kHB, lane);
+  for (int q = 0; q < 16; ++q) D[i * kRS + sub + 4 * q] = v[q];
   __syncthreads();
 }
 
-// Panel of one step, fused: every CTA of a unit factors the diagonal block
-// itself (diag_lu, redundantly: the CTAs run side by side, so the
-// factorisation adds no time to the step's dependent chain), then solves its
-// strip.  Row chunks: rows o0 .. o0+w of L21 from x U11 = a.  Column chunks:
-// columns o0 .. o0+w of U12 from L11 x = b.  Thread (line = tid / 4,
-// quarter qq) holds entries 16qq .. 16qq+15 of its row (column) in
-// registers; the factor's row j of U (column j of L) is staged padded in
-// shared memory.  Chunk 0 checks the pivots and leaves the factored block in
-// dp.dscratch (slot = the unit's index in the step); the step's update (part
-// a) copies it into the arena once every CTA here has read the unfactored
-// block.  A unit with nothing left to solve gets one CTA for that.
-constexpr size_t kRPanelSmem =
-    (static_cast<size_t>(kRP) * kRS + static_cast<size_t>(kRP) * kPadRow + kRP) * sizeof(double);
-
-__global__ void __launch_bounds__(kRThreads) k_rpanel(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
-  extern __shared__ double psm[];
-  double* D = psm;                    // kRP x kRS
-  double* T = D + kRP * kRS;          // kRP x kPadRow (16-byte aligned: kRP * kRS is even)
-  double* rd = T + kRP * kPadRow;     // kRP
-  int a = 0;
-  while (a + 1 < nact && dp.rstep_strip_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
-  const int u = dp.rstep_unit[ubase + a];
-  const int ch = blockIdx.x - dp.rstep_strip_pref[ubase + a];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const int nb = min(kRP, m - k0);
-  const int base = k0 + nb;
-  const int chunks = (m - base + kRP - 1) / kRP;
-  const bool rowc = ch < chunks;
-  const int o0 = base + (rowc ? ch : ch - chunks) * kRP;
-  const int w = max(0, min(kRP, m - o0));
-  double* A = dp.lu + dp.lu_off[u];
-  const int tid = threadIdx.x, lane = tid & 31;
-  const int line = tid >> 2, qq = tid & 3;
-  // The strip's entries go to registers first (their loads overlap the LU).
-  double x[16];
+// Strip entries of one thread: line = tid / 4 of the strip at o0 (a row of
+// L21 for a row strip, a column of U12 for a column strip), entries
+// 16qq .. 16qq+15 with qq = tid % 4; zero past nb or past the strip's w lines.
+__device__ __forceinline__ void strip_load(const double* A, int m, int k0, int nb, int o0, int w, bool rowc,
+                                           double (&x)[16]) {
+  const int tid = threadIdx.x, line = tid >> 2, qq = tid & 3;
   const bool live = line < w;
 #pragma unroll
   for (int t = 0; t < 16; ++t) {
     const int q = 16 * qq + t;
     double v = 0.0;
     if (live && q < nb)
-      v = rowc ? A[static_cast<size_t>(o0 + line) * m + k0 + q] : A[static_cast<size_t>(k0 + q) * m + o0 + line];
+      v = rowc ? __ldcg(A + static_cast<size_t>(o0 + line) * m + k0 + q)
+               : __ldcg(A + static_cast<size_t>(k0 + q) * m + o0 + line);
     x[t] = v;
   }
-  diag_lu(D, A, m, k0, nb);
-  __syncthreads();
-  if (ch == 0) {
-    if (tid < nb) {
-      const double d = D[tid * kRS + tid];
-      if (!(fabs(d) > 0.0) || !isfinite(d)) {
-        if (atomicCAS(dp.status, 0, kFailReusedPivot) == 0) dp.status[1] = u;
-      }
-    }
-    double* out = dp.dscratch + static_cast<size_t>(a) * kRP * kRP;
-#pragma unroll 4
-    for (int e = tid; e < kRP * kRP; e += kRThreads) out[e] = D[(e / kRP) * kRS + (e % kRP)];
-  }
+}
+
+// Solves one strip against the factored diagonal block D (stride kRS,
+// identity past nb) and stores it: row strips x U11 = a, column strips
+// L11 x = b.  Thread (line, quarter qq) holds its 16 entries in x; the
+// factor's row j of U (column j of L) is staged padded in shared memory T
+// (kRP x kPadRow), the pivot reciprocals in rd.
+__device__ __forceinline__ void strip_solve(const double* D, double* T, double* rd, double* A, int m, int k0,
+                                            int nb, int o0, int w, bool rowc, double (&x)[16]) {
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int line = tid >> 2, qq = tid & 3;
   // T[j][18q + t]: rows: U[j][16q + t]; columns: L[16q + t][j].
   for (int e = tid; e < kRP * kRP; e += kRThreads) {
     const int j = e / kRP, c = e - j * kRP;
@@ -921,7 +867,7 @@ __global__ void __launch_bounds__(kRThreads) k_rpanel(DevPlan dp, int32_t k0, in
       }
     }
   }
-  if (live) {
+  if (line < w) {
 #pragma unroll
     for (int t = 0; t < 16; ++t) {
       const int q = 16 * qq + t;
@@ -931,6 +877,56 @@ __global__ void __launch_bounds__(kRThreads) k_rpanel(DevPlan dp, int32_t k0, in
       }
     }
   }
+}
+
+// Panel of one step, fused: every CTA of a unit factors the diagonal block
+// itself (diag_lu, redundantly: the CTAs run side by side, so the
+// factorisation adds no time to the step's dependent chain), then solves its
+// strip (strip_solve).  Row chunks: rows o0 .. o0+w of L21; column chunks:
+// columns o0 .. o0+w of U12.  Chunk 0 checks the pivots and leaves the
+// factored block in dp.dscratch (slot = the unit's index in the step); the
+// step's update (part a) copies it into the arena once every CTA here has
+// read the unfactored block.  A unit with nothing left to solve gets one CTA
+// for that.
+constexpr size_t kRPanelSmem =
+    (static_cast<size_t>(kRP) * kRS + static_cast<size_t>(kRP) * kPadRow + kRP) * sizeof(double);
+
+__global__ void __launch_bounds__(kRThreads) k_rpanel(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact) {
+  extern __shared__ double psm[];
+  double* D = psm;                    // kRP x kRS
+  double* T = D + kRP * kRS;          // kRP x kPadRow (16-byte aligned: kRP * kRS is even)
+  double* rd = T + kRP * kPadRow;     // kRP
+  int a = 0;
+  while (a + 1 < nact && dp.rstep_strip_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
+  const int u = dp.rstep_unit[ubase + a];
+  const int ch = blockIdx.x - dp.rstep_strip_pref[ubase + a];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int nb = min(kRP, m - k0);
+  const int base = k0 + nb;
+  const int chunks = (m - base + kRP - 1) / kRP;
+  const bool rowc = ch < chunks;
+  const int o0 = base + (rowc ? ch : ch - chunks) * kRP;
+  const int w = max(0, min(kRP, m - o0));
+  double* A = dp.lu + dp.lu_off[u];
+  const int tid = threadIdx.x;
+  // The strip's entries go to registers first (their loads overlap the LU).
+  double x[16];
+  strip_load(A, m, k0, nb, o0, w, rowc, x);
+  diag_lu(D, A, m, k0, nb);
+  __syncthreads();
+  if (ch == 0) {
+    if (tid < nb) {
+      const double d = D[tid * kRS + tid];
+      if (!(fabs(d) > 0.0) || !isfinite(d)) {
+        if (atomicCAS(dp.status, 0, kFailReusedPivot) == 0) dp.status[1] = u;
+      }
+    }
+    double* out = dp.dscratch + static_cast<size_t>(a) * kRP * kRP;
+#pragma unroll 4
+    for (int e = tid; e < kRP * kRP; e += kRThreads) out[e] = D[(e / kRP) * kRS + (e % kRP)];
+  }
+  strip_solve(D, T, rd, A, m, k0, nb, o0, w, rowc, x);
 }
 
 // Copies the factored diagonal block of step k0 (left by k_rpanel in
@@ -943,11 +939,60 @@ __device__ __forceinline__ void place_diag(const DevPlan& dp, double* A, int m, 
   }
 }
 
+// C -= L U for the kRTileM x kRTileN tile at (i0, j0) of a row-major m x m
+// unit: L = columns k0 .. k0+nb of rows i0.., U = rows k0 .. k0+nb of
+// columns j0.. (rows and columns past m skipped).  rsm: kRGemmSmem bytes.
+// Thread (ty, tx) accumulates rows i0 + 4ty + i, columns j0 + 8b + tx.
+__device__ __forceinline__ void rgemm_tile(double* rsm, double* A, int m, int k0, int nb, int i0, int j0) {
+  double* As = rsm;                      // kRTileM x kRAS
+  double* Bs = rsm + kRTileM * kRAS;     // kRP x kRTileN
+  const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+#pragma unroll 8
+  for (int e = tid; e < kRTileM * kRP; e += kRThreads) {
+    const int r = e / kRP, q = e - r * kRP;
+    As[r * kRAS + q] = (i0 + r < m && q < nb) ? __ldcg(A + static_cast<size_t>(i0 + r) * m + k0 + q) : 0.0;
+  }
+#pragma unroll 8
+  for (int e = tid; e < kRP * kRTileN; e += kRThreads) {
+    const int q = e / kRTileN, c = e - q * kRTileN;
+    Bs[e] = (q < nb && j0 + c < m) ? __ldcg(A + static_cast<size_t>(k0 + q) * m + j0 + c) : 0.0;
+  }
+  __syncthreads();
+  double acc[4][8];
+  const bool cin = j0 + 7 * 8 + tx < m;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = i0 + ty * 4 + i;
+    const double* crow = A + static_cast<size_t>(r) * m + j0 + tx;
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+      acc[i][b] = (r < m && (cin || j0 + b * 8 + tx < m)) ? __ldcg(crow + b * 8) : 0.0;
+  }
+#pragma unroll 2
+  for (int k = 0; k < kRP; ++k) {
+    double x[4], y[8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) x[i] = As[(ty * 4 + i) * kRAS + k];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) y[b] = Bs[k * kRTileN + b * 8 + tx];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int b = 0; b < 8; ++b) acc[i][b] = fma(-x[i], y[b], acc[i][b]);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = i0 + ty * 4 + i;
+    double* crow = A + static_cast<size_t>(r) * m + j0 + tx;
+#pragma unroll
+    for (int b = 0; b < 8; ++b)
+      if (r < m && (cin || j0 + b * 8 + tx < m)) crow[b * 8] = acc[i][b];
+  }
+}
+
 __global__ void __launch_bounds__(kRThreads, 2) k_rgemm(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
                                                         int32_t part) {
   extern __shared__ double rsm[];
-  double* As = rsm;                      // kRTileM x kRAS
-  double* Bs = rsm + kRTileM * kRAS;     // kRP x kRTileN
   const int32_t* pref = part ? dp.rstep_gb_pref : dp.rstep_ga_pref;
   int a = 0;
   while (a + 1 < nact && pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
@@ -976,50 +1021,131 @@ __global__ void __launch_bounds__(kRThreads, 2) k_rgemm(DevPlan dp, int32_t k0, 
     ti = 1 + t / (ntj - 1);
     tj = 1 + t % (ntj - 1);
   }
-  const int i0 = base + ti * kRTileM, j0 = base + tj * kRTileN;
-  double* A = dp.lu + dp.lu_off[u];
-  const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
-#pragma unroll 8
-  for (int e = tid; e < kRTileM * kRP; e += kRThreads) {
-    const int r = e / kRP, q = e - r * kRP;
-    As[r * kRAS + q] = (i0 + r < m && q < nb) ? A[static_cast<size_t>(i0 + r) * m + k0 + q] : 0.0;
-  }
-#pragma unroll 8
-  for (int e = tid; e < kRP * kRTileN; e += kRThreads) {
-    const int q = e / kRTileN, c = e - q * kRTileN;
-    Bs[e] = (q < nb && j0 + c < m) ? A[static_cast<size_t>(k0 + q) * m + j0 + c] : 0.0;
-  }
+  rgemm_tile(rsm, dp.lu + dp.lu_off[u], m, k0, nb, base + ti * kRTileM, base + tj * kRTileN);
+}
+
+// ---------------------------------------------------------------------------
+// Value-only refactor as one persistent kernel over the tile task graph of
+// build_rtasks (plan.h): tiles kRP x kRP, tasks D(k), L(i, k), U(k, j) and
+// G(i, j, k) (row tiles i, i + 1 of tile column j), in the list's order.
+// A tile's version word counts the steps applied to it; a task waits for
+//   D(k):       ver(k, k) >= k
+//   L(i, k):    ver(k, k) >= k + 1 and ver(i, k) >= k
+//   U(k, j):    ver(k, k) >= k + 1 and ver(k, j) >= k
+//   G(i, j, k): ver(i, k), ver(i + 1, k), ver(k, j) >= k + 1 and
+//               ver(i, j), ver(i + 1, j) >= k
+// and sets its output tiles to k + 1.  CTAs take tasks by ticket (word 0 of
+// the array, an atomic counter).  A task waits only for tasks earlier in the
+// list, whose tickets running CTAs took, so the smallest unfinished ticket
+// always progresses: nothing assumes that the CTAs are co-resident.  Waits
+// are bounded (wait_ready); one that runs out records kFailRefactorSync and
+// publishes kAbortFlag on the task's outputs, so that its dependents stop at
+// once.  Matrix entries are read with ld.global.cg (from L2): a line that
+// another SM rewrote is never served stale from this SM's L1.  The
+// arithmetic per tile is that of k_rpanel / k_rgemm (diag_lu, strip_solve,
+// rgemm_tile), so both schedules give bit-identical factors.
+static_assert(kRTileM == 2 * kRP && kRTileN == kRP, "an update task covers two row tiles of one tile column");
+constexpr size_t kRDagSmem = kRGemmSmem > kRPanelSmem ? kRGemmSmem : kRPanelSmem;
+
+__device__ __forceinline__ void rdag_publish(int32_t* f, int32_t v) {
+  __threadfence();
   __syncthreads();
-  // The C tile: rows i0 + ty*4 + i, columns j0 + 8b + tx.
-  double acc[4][8];
-  const bool cin = j0 + 7 * 8 + tx < m;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = i0 + ty * 4 + i;
-    const double* crow = A + static_cast<size_t>(r) * m + j0 + tx;
-#pragma unroll
-    for (int b = 0; b < 8; ++b)
-      acc[i][b] = (r < m && (cin || j0 + b * 8 + tx < m)) ? crow[b * 8] : 0.0;
-  }
-#pragma unroll 2
-  for (int k = 0; k < kRP; ++k) {
-    double x[4], y[8];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) x[i] = As[(ty * 4 + i) * kRAS + k];
-#pragma unroll
-    for (int b = 0; b < 8; ++b) y[b] = Bs[k * kRTileN + b * 8 + tx];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int b = 0; b < 8; ++b) acc[i][b] = fma(-x[i], y[b], acc[i][b]);
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int r = i0 + ty * 4 + i;
-    double* crow = A + static_cast<size_t>(r) * m + j0 + tx;
-#pragma unroll
-    for (int b = 0; b < 8; ++b)
-      if (r < m && (cin || j0 + b * 8 + tx < m)) crow[b * 8] = acc[i][b];
+  if (threadIdx.x == 0) atomicExch(f, v);
+}
+
+__global__ void __launch_bounds__(kRThreads, 2) k_rdag(DevPlan dp, const int4* __restrict__ tasks, int32_t ntasks,
+                                                       int32_t* __restrict__ words) {
+  extern __shared__ double gsm[];
+  __shared__ int s_tk, s_ok;
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) s_tk = atomicAdd(words, 1);
+    __syncthreads();
+    const int tk = s_tk;
+    if (tk >= ntasks) break;
+    const int4 tsk = __ldg(tasks + tk);
+    const int u = tsk.x, k = tsk.y, i = tsk.z >> 16, j = tsk.z & 0xffff;
+    int32_t* ver = words + tsk.w;
+    const int s = dp.ustart[u];
+    const int m = dp.ustart[u + 1] - s;
+    const int nt = (m + kRP - 1) / kRP;
+    double* A = dp.lu + dp.lu_off[u];
+    const int k0 = k * kRP, nb = min(kRP, m - k0);
+    int32_t* kk = ver + k * nt + k;
+    if (i == k && j == k) {
+      // D(k): factor tile (k, k) in place.
+      if (tid == 0) s_ok = wait_ready(kk, k);
+      __syncthreads();
+      if (s_ok) {
+        double* D = gsm;
+        diag_lu(D, A, m, k0, nb);
+        if (tid < nb) {
+          const double d = D[tid * kRS + tid];
+          if (!(fabs(d) > 0.0) || !isfinite(d)) {
+            if (atomicCAS(dp.status, 0, kFailReusedPivot) == 0) dp.status[1] = u;
+          }
+        }
+        for (int e = tid; e < nb * nb; e += kRThreads) {
+          const int r = e / nb, c = e - r * nb;
+          A[static_cast<size_t>(k0 + r) * m + k0 + c] = D[r * kRS + c];
+        }
+        rdag_publish(kk, k + 1);
+      } else if (tid == 0) {
+        atomicCAS(dp.status, 0, kFailRefactorSync);
+        atomicExch(kk, kAbortFlag);
+      }
+    } else if (i == k || j == k) {
+      // L(i, k) (row strip) or U(k, j) (column strip).
+      const bool rowc = j == k;
+      const int o = rowc ? i : j;
+      int32_t* out = rowc ? ver + i * nt + k : ver + k * nt + j;
+      if (tid == 0) s_ok = wait_ready(kk, k + 1) && wait_ready(out, k);
+      __syncthreads();
+      if (s_ok) {
+        double* D = gsm;                   // kRP x kRS
+        double* T = D + kRP * kRS;         // kRP x kPadRow
+        double* rd = T + kRP * kPadRow;    // kRP
+        const int o0 = o * kRP, w = min(kRP, m - o0);
+        double x[16];
+        strip_load(A, m, k0, nb, o0, w, rowc, x);
+        for (int e = tid; e < kRP * kRP; e += kRThreads) {
+          const int r = e / kRP, c = e - r * kRP;
+          D[r * kRS + c] = (r < nb && c < nb) ? __ldcg(A + static_cast<size_t>(k0 + r) * m + k0 + c)
+                                              : (r == c ? 1.0 : 0.0);
+        }
+        __syncthreads();
+        strip_solve(D, T, rd, A, m, k0, nb, o0, w, rowc, x);
+        rdag_publish(out, k + 1);
+      } else if (tid == 0) {
+        atomicCAS(dp.status, 0, kFailRefactorSync);
+        atomicExch(out, kAbortFlag);
+      }
+    } else {
+      // G(i, j, k): row tiles i, i + 1 of tile column j.
+      const bool two = i + 1 < nt;
+      int32_t* c0 = ver + i * nt + j;
+      int32_t* c1 = two ? c0 + nt : c0;
+      if (tid == 0) {
+        bool ok = wait_ready(ver + i * nt + k, k + 1) && wait_ready(ver + k * nt + j, k + 1) && wait_ready(c0, k);
+        if (two) ok = ok && wait_ready(ver + (i + 1) * nt + k, k + 1) && wait_ready(c1, k);
+        s_ok = ok;
+      }
+      __syncthreads();
+      if (s_ok) {
+        rgemm_tile(gsm, A, m, k0, nb, i * kRP, j * kRP);
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) {
+          atomicExch(c0, k + 1);
+          if (two) atomicExch(c1, k + 1);
+        }
+      } else if (tid == 0) {
+        atomicCAS(dp.status, 0, kFailRefactorSync);
+        atomicExch(c0, kAbortFlag);
+        if (two) atomicExch(c1, kAbortFlag);
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -1230,6 +1356,8 @@ cudaError_t large_setup() {
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_rpanel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kRPanelSmem));
     if (err == cudaSuccess)
+      err = cudaFuncSetAttribute(k_rdag, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kRDagSmem));
+    if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_trsv_tiles<true, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(trsv_smem<16>()));
     if (err == cudaSuccess)
@@ -1350,6 +1478,28 @@ cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cu
   // Join.
   if ((e = cudaEventRecord(ev_b, sb)) != cudaSuccess) return e;
   if ((e = cudaStreamWaitEvent(sa, ev_b, 0)) != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t large_refactor_dag(const DevPlan& dp, const Plan& p, const int32_t* d_tasks, int32_t* d_words,
+                               cudaStream_t stream, int32_t* launches) {
+  cudaError_t e = large_setup();
+  if (e != cudaSuccess) return e;
+  if (p.rtasks <= 0) return cudaErrorInvalidValue;
+  static int grid_max = 0;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    int dev = 0, nsm = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rdag, kRThreads, kRDagSmem);
+    grid_max = std::max(1, nsm * std::max(1, per_sm));
+  });
+  if ((e = cudaMemsetAsync(d_words, 0, static_cast<size_t>(p.rt_words) * sizeof(int32_t), stream)) != cudaSuccess)
+    return e;
+  const int grid = std::min(grid_max, p.rtasks);
+  k_rdag<<<grid, kRThreads, kRDagSmem, stream>>>(dp, reinterpret_cast<const int4*>(d_tasks), p.rtasks, d_words);
+  ++*launches;
   return cudaGetLastError();
 }
 

@@ -26,14 +26,20 @@ cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_larg
 cudaError_t large_scatter_reuse(const DevPlan& dp, const Plan& p, const double* d_vals, const int32_t* d_large_units,
                                 cudaStream_t stream);
 
-// Enqueues the solve of the large units of one level (d_units / h_units: the
-// level's list, single-CTA units first).  xp is the permuted solution.
 // Value-only refactor of all large units with the stored pivot order (rows
 // already scattered in that order).  Work is queued on sa and sb (forked from
 // and joined back into sa with the two events); zero or non-finite pivots set
 // the reused-pivot status.
 cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cudaStream_t sb, cudaEvent_t ev_a,
                            cudaEvent_t ev_b, int32_t* launches, int32_t prec);
+
+// The same refactor as one persistent kernel over the tile task graph of
+// build_rtasks (p.rtask, uploaded to d_tasks; p.rtasks > 0).  d_words holds
+// p.rt_words words (ticket and tile versions), zeroed here on the stream.
+// Zero or non-finite pivots set the reused-pivot status; a wait that runs out
+// sets kFailRefactorSync.
+cudaError_t large_refactor_dag(const DevPlan& dp, const Plan& p, const int32_t* d_tasks, int32_t* d_words,
+                               cudaStream_t stream, int32_t* launches);
 
 // Forward and backward solves of the large units of one level (two
 // launches).  d_sync holds large_sync_words(p) zeroed words per solve sweep;

@@ -2,6 +2,8 @@
 #include "plan.h"
 
 #include <algorithm>
+#include <array>
+#include <climits>
 #include <cmath>
 
 namespace bdlu {
@@ -15,6 +17,80 @@ static double lu_flops(int64_t m) {
     f += r + 2.0 * r * r;
   }
   return f;
+}
+
+int64_t build_rtasks(const std::vector<int32_t>& units, const std::vector<int32_t>& sizes, int64_t max_tasks,
+                     std::vector<int32_t>& tasks, int32_t& words) {
+  tasks.clear();
+  words = 0;
+  const size_t nu = units.size();
+  std::vector<int64_t> nt(nu), vbase(nu);
+  int64_t total = 0, steps = 0, w = 1;
+  for (size_t q = 0; q < nu; ++q) {
+    nt[q] = (sizes[q] + kRPanel - 1) / kRPanel;
+    if (nt[q] > 65535) return -1;
+    vbase[q] = w;
+    w += nt[q] * nt[q];
+    steps = std::max(steps, nt[q]);
+    // Per step k: 1 D, 2 (nt - k - 1) strips, ceil((nt - k - 1) / 2) (nt - k - 1) updates.
+    for (int64_t k = 0; k < nt[q]; ++k) {
+      const int64_t r = nt[q] - k - 1;
+      total += 1 + 2 * r + (r + 1) / 2 * r;
+    }
+  }
+  if (nu == 0 || total > max_tasks || w > INT32_MAX) return -1;
+  tasks.reserve(static_cast<size_t>(total) * 4);
+  auto push = [&](size_t q, int64_t k, int64_t i, int64_t j) {
+    tasks.push_back(units[q]);
+    tasks.push_back(static_cast<int32_t>(k));
+    tasks.push_back(static_cast<int32_t>((i << 16) | j));
+    tasks.push_back(static_cast<int32_t>(vbase[q]));
+  };
+  // Step k's panel: D, then the strips of step k + 1's panel, then the rest.
+  auto panel = [&](int64_t k) {
+    for (size_t q = 0; q < nu; ++q)
+      if (nt[q] > k) push(q, k, k, k);
+    for (size_t q = 0; q < nu; ++q) {
+      for (int64_t t = k + 1; t < nt[q]; ++t) {
+        push(q, k, t, k);
+        push(q, k, k, t);
+      }
+    }
+  };
+  // Step k's updates of step k + 1's panel: the diagonal pair first, then
+  // row pair k + 1 and tile column k + 1 alternately.
+  auto critical = [&](int64_t k) {
+    for (size_t q = 0; q < nu; ++q) {
+      if (nt[q] <= k + 1) continue;
+      push(q, k, k + 1, k + 1);
+      for (int64_t t = 1;; ++t) {
+        const bool row = k + 1 + t < nt[q], col = k + 1 + 2 * t < nt[q];
+        if (!row && !col) break;
+        if (row) push(q, k, k + 1, k + 1 + t);
+        if (col) push(q, k, k + 1 + 2 * t, k + 1);
+      }
+    }
+  };
+  // Step k's other updates (row pairs from k + 3, tile columns from k + 2),
+  // by the step at which their tiles join a panel.
+  std::vector<std::array<int64_t, 3>> rest;
+  auto others = [&](int64_t k) {
+    for (size_t q = 0; q < nu; ++q) {
+      rest.clear();
+      for (int64_t i = k + 3; i < nt[q]; i += 2)
+        for (int64_t j = k + 2; j < nt[q]; ++j) rest.push_back({std::min(i, j), i, j});
+      std::sort(rest.begin(), rest.end());
+      for (const auto& r : rest) push(q, k, r[1], r[2]);
+    }
+  };
+  for (int64_t k = 0; k < steps; ++k) {
+    panel(k);
+    if (k > 0) others(k - 1);
+    critical(k);
+  }
+  if (steps > 0) others(steps - 1);
+  words = static_cast<int32_t>(w);
+  return static_cast<int64_t>(tasks.size() / 4);
 }
 
 Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max) {
@@ -245,6 +321,14 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
     p.rstep_ga_total.push_back(apre);
     p.rstep_gb_total.push_back(bpre);
     p.rmax_active = std::max(p.rmax_active, act);
+  }
+
+  {
+    std::vector<int32_t> sizes;
+    for (int32_t u : p.large_units)
+      sizes.push_back(p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)]);
+    const int64_t nt = build_rtasks(p.large_units, sizes, kRTaskMax, p.rtask, p.rt_words);
+    p.rtasks = nt > 0 ? static_cast<int32_t>(nt) : 0;
   }
 
   // Canonical CSR row pointer (original coordinates) for the residual.

@@ -87,6 +87,12 @@ struct Plan {
   std::vector<int32_t> rstep_ptr, rstep_unit;
   std::vector<int32_t> rstep_strip_pref, rstep_ga_pref, rstep_gb_pref;  // per active unit, exclusive
   std::vector<int32_t> rstep_strip_total, rstep_ga_total, rstep_gb_total;
+  // The same refactor as one tile task graph (build_rtasks): four words per
+  // task and the size of the ticket + version-word array.  Empty when the
+  // list would exceed kRTaskMax tasks.
+  std::vector<int32_t> rtask;
+  int32_t rtasks = 0;
+  int32_t rt_words = 0;
   // Canonical CSR (original coordinates) for the residual.
   std::vector<int32_t> csr_ptr;
   double factor_flops = 0.0;
@@ -101,6 +107,31 @@ constexpr int kRPanel = 64;         // panel width of the value-only refactor
 constexpr int kRTileM = 128;        // update tile of the value-only refactor: rows
 constexpr int kRTileN = 64;         //   and columns
 constexpr int kSolveTile = 64;      // row tile of the large-unit triangular solves
+
+constexpr int64_t kRTaskMax = int64_t{1} << 24;  // task-graph refactor: largest task list
+
+// Task list of the value-only refactor of large units as a tile graph.
+// Tiles are kRPanel x kRPanel; per unit of nt tiles per side and step k:
+//   D(k)       LU without pivot search of tile (k, k), in place
+//   L(i, k)    tile (i, k) <- tile (i, k) U(k, k)^{-1}, i > k
+//   U(k, j)    tile (k, j) <- L(k, k)^{-1} tile (k, j), j > k
+//   G(i, j, k) row tiles i and i + 1 (if it exists) of tile column j
+//              -= L(i.., k) U(k, j), for the row pairs k+1, k+3, ... and
+//              every j > k
+// A task is four words: unit, k, (i << 16) | j, and the base of the unit's
+// version words (tile (i, j) at base + i * nt + j; word 0 of the array is
+// the ticket counter).  The kind follows from i, j and k (D: i = j = k,
+// L: j = k < i, U: i = k < j, G: i, j > k).  Version word of a tile = steps
+// applied to it: G(i, j, k) and the final D/L/U of step k leave k + 1.
+// Order, per step k: D, L and U of step k (the tiles of step k + 1's panel
+// first); the updates of step k - 1 that do not touch step k + 1's panel,
+// soonest-needed tiles first; then step k's updates of row pair k + 1 and
+// tile column k + 1 (step k + 1's panel).  Every task's inputs come from
+// tasks earlier in the list.  units: unit ids, sizes: their rows.  Returns
+// the task count, or -1 if a unit has more than 65535 tiles per side or the
+// list would exceed max_tasks (the list is then left empty).
+int64_t build_rtasks(const std::vector<int32_t>& units, const std::vector<int32_t>& sizes, int64_t max_tasks,
+                     std::vector<int32_t>& tasks, int32_t& words);
 
 Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max);
 

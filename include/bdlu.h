@@ -161,6 +161,12 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  *     FP32 accuracy), then FP64.  stats.precision and stats.refine_iters
  *     report the level and the refinement steps.  Device-pointer solves run
  *     "refine_iters" steps only.
+ *   "refactor_schedule": order of the FP64 value-only refactor of blocks
+ *     above the shared-memory size.  0 (default): a chain of per-step
+ *     launches (panel, then trailing update, one step of lookahead).  1: one
+ *     persistent kernel works through the block's tile task graph (diagonal
+ *     LU, strip solves, trailing updates; each task starts when its input
+ *     tiles are ready).  Both give bit-identical factors.
  * Returns BDLU_OK, or BDLU_INVALID_DIMENSION for an unknown key. */
 int bdlu_set_option(bdlu_solver* h, const char* key, double value);
 
