@@ -506,6 +506,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_trsv_tiles(DevPlan dp, con
   double* xs = Ts + kTile * kTS;       // this tile's unknowns [i * kRC + c]
   double* xj = xs + kTile * kRC;       // finished tile's unknowns
   __shared__ int s_tk, s_ok;
+  __shared__ double rdg[kTile];        // backward sweep: reciprocals of the diagonal block's pivots
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_tk = atomicAdd(ticket, 1);
   __syncthreads();
@@ -630,6 +631,9 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_trsv_tiles(DevPlan dp, con
       const int e = tid + kSolveThreads * k;
       const int i = e / kTile, c = e - i * kTile;
       Ts[i * kTS + c] = nxt[k];
+      // The backward sweep multiplies by the pivots' reciprocals, formed
+      // here in parallel: no division on its dependent chain.
+      if (!kFwd && i == c) rdg[i] = 1.0 / nxt[k];
     }
     __syncthreads();
     // Each warp sweeps right-hand side `warp` and, when more than kWarps are
@@ -659,9 +663,9 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_trsv_tiles(DevPlan dp, con
           }
         } else {
           for (int rr = w - 1; rr >= 0; --rr) {
-            const double d = Ts[rr * kTS + rr];
-            const double x0 = __shfl_sync(0xffffffffu, rr < 32 ? a0 : b0, rr & 31) / d;
-            const double x1 = __shfl_sync(0xffffffffu, rr < 32 ? a1 : b1, rr & 31) / d;
+            const double rd = rdg[rr];
+            const double x0 = __shfl_sync(0xffffffffu, rr < 32 ? a0 : b0, rr & 31) * rd;
+            const double x1 = __shfl_sync(0xffffffffu, rr < 32 ? a1 : b1, rr & 31) * rd;
             if (lane == rr) {
               a0 = x0;
               a1 = x1;
@@ -690,8 +694,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_trsv_tiles(DevPlan dp, con
         }
       } else {
         for (int rr = w - 1; rr >= 0; --rr) {
-          const double d = Ts[rr * kTS + rr];
-          const double x0 = __shfl_sync(0xffffffffu, rr < 32 ? a0 : b0, rr & 31) / d;
+          const double x0 = __shfl_sync(0xffffffffu, rr < 32 ? a0 : b0, rr & 31) * rdg[rr];
           if (lane == rr) a0 = x0;
           if (lane + 32 == rr) b0 = x0;
           if (lane < rr) a0 = fma(-Ts[lane * kTS + rr], x0, a0);
