@@ -301,8 +301,15 @@ __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int3
     }
     if (!staged && pass == 0 && tid == 0) atomicCAS(dp.status, 0, kFailSync);
   }
+  if (!__syncthreads_and(staged)) {
+    if (tid == 0) atomicCAS(dp.status, 0, kFailSync);
+    return;
+  }
+  // Reciprocals of the pivots, formed in parallel: the backward sweep
+  // multiplies, with no division on its dependent chain.
+  __shared__ double rdiag[32 * kSlots];
+  for (int i = tid; i < m; i += kThreads) rdiag[i] = 1.0 / T[i * m + i];
   __syncthreads();
-  if (!staged) return;
   for (int t = 0; t < nmine; ++t) {
     const int c = warp + t * kWarps;
     if (t > 0) form(c);
@@ -328,8 +335,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int3
       for (int jj = jtop; jj >= 0; --jj) {
         const int j = 32 * kk + jj;
         const double* col = T + j * m;
-        const double rd = 1.0 / col[j];
-        const double xr = __shfl_sync(0xffffffffu, a[kk], jj) * rd;
+        const double xr = __shfl_sync(0xffffffffu, a[kk], jj) * rdiag[j];
         if (lane == jj) a[kk] = xr;
 #pragma unroll
         for (int k = 0; k <= kk; ++k) {
