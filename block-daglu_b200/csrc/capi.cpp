@@ -108,9 +108,22 @@ int upload_values(bdlu_solver* h, const double* vals, bool device, cudaStream_t 
 
 }  // namespace
 
+int bdlu_sync_host_values(bdlu_solver* h) {
+  if (!h->host_vals_stale) return BDLU_OK;
+  if (!h->engine) return fail(h, BDLU_BACKEND_UNAVAILABLE, "the device holding the current values was released");
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess)
+    e = cudaMemcpy(h->coo.val.data(), h->engine->values_buffer(), static_cast<size_t>(h->coo.nnz()) * sizeof(double),
+                   cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail(h, BDLU_BACKEND_UNAVAILABLE, std::string("value download: ") + cudaGetErrorString(e));
+  h->host_vals_stale = false;
+  return BDLU_OK;
+}
+
 // Analysis of an already validated canonical matrix under route `mode`
 // (solver.cpp:820-1182): signatures, decomposition, device plan and upload.
 int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf* btf) {
+  if (const int st = bdlu_sync_host_values(h)) return st;
   h->sig = bdlu::matrix_sig(h->n, h->coo);
   h->sig2 = bdlu::matrix_sig2(h->n, h->coo);
   h->value_sig = bdlu::matrix_value_sig(h->coo);
@@ -159,8 +172,10 @@ int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cud
   if (!vals || nnz != h->coo.nnz()) return fail(h, BDLU_INVALID_INDEX, "value count does not match the analysed pattern");
   for (int64_t k = 0; k < nnz; ++k)
     if (!std::isfinite(vals[k])) return fail(h, BDLU_NON_FINITE_VALUE, "matrix contains NaN or infinity");
-  std::memcpy(h->coo.val.data(), vals, static_cast<size_t>(nnz) * sizeof(double));
+  // No host copy here (10 MB per million entries): the device buffer holds
+  // the values; coo.val is refreshed from it when something reads it.
   if (const int st = upload_values(h, vals, false, stream)) return st;
+  h->host_vals_stale = true;
   return do_factor(h, stream, h->reuse_pivots);
 }
 
@@ -169,6 +184,7 @@ int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cud
 int bdlu_device_restore(bdlu_solver* h) {
   if (!h->decomposed) return fail(h, BDLU_NOT_PREPARED, "analyze must succeed before a device upload");
   if (h->engine) return BDLU_OK;
+  if (h->host_vals_stale) return fail(h, BDLU_BACKEND_UNAVAILABLE, "values were not saved before the device release");
   try {
     const bdlu::Plan plan = bdlu::build_plan(h->coo, h->dec, bdlu::small_unit_max());
     h->engine = std::make_unique<bdlu::Engine>();
@@ -191,6 +207,8 @@ int bdlu_device_restore(bdlu_solver* h) {
 }
 
 void bdlu_device_release(bdlu_solver* h) {
+  // Keep the current values on the host for the next upload.
+  if (bdlu_sync_host_values(h) != BDLU_OK) h->decomposed = false;
   h->engine.reset();
   h->factored = false;
   h->exported = false;
@@ -315,6 +333,7 @@ int bdlu_set_coo(bdlu_solver* h, const int32_t* rows, const int32_t* cols, const
   if (nnz < 0 || (nnz > 0 && (!rows || !cols || !vals))) return fail(h, BDLU_INVALID_INDEX, "invalid COO arrays");
   try {
     h->engine.reset();
+    h->host_vals_stale = false;
     h->in_rows.assign(rows, rows + nnz);
     h->in_cols.assign(cols, cols + nnz);
     h->in_vals.assign(vals, vals + nnz);
@@ -349,7 +368,9 @@ int bdlu_factor(bdlu_solver* h) {
   clear_error(h);
   if (!h->decomposed) return fail(h, BDLU_NOT_PREPARED, "analyze must succeed before factor");
   if (!h->engine) return fail(h, BDLU_BACKEND_UNAVAILABLE, "analysis was run without a device (analysis_only)");
-  if (const int st = upload_values(h, h->coo.val.data(), false, nullptr)) return st;
+  // After refactors the device buffer already holds the current values.
+  if (!h->host_vals_stale)
+    if (const int st = upload_values(h, h->coo.val.data(), false, nullptr)) return st;
   return do_factor(h, nullptr, false);
 }
 
@@ -365,6 +386,7 @@ int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nn
   if (!d_vals || nnz != h->coo.nnz()) return fail(h, BDLU_INVALID_INDEX, "value count does not match the analysed pattern");
   auto s = static_cast<cudaStream_t>(stream);
   if (const int st = upload_values(h, d_vals, true, s)) return st;
+  h->host_vals_stale = true;
   std::string err;
   if (!h->engine->factor_async(h->engine->values_buffer(), s, err, h->reuse_pivots))
     return fail(h, BDLU_BACKEND_UNAVAILABLE, err);

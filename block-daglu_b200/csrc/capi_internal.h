@@ -38,6 +38,10 @@ struct bdlu_solver {
   // Error state (solver.h:122-123).
   int last_error = BDLU_OK;
   std::string last_message;
+  // The device value buffer holds newer values than coo.val (refactors
+  // upload without a host copy; bdlu_sync_host_values fetches them when the
+  // host copy is read).
+  bool host_vals_stale = false;
   // Stats of the last solve.
   int32_t last_refine = 0;
   double last_residual = 0.0;
@@ -65,6 +69,11 @@ int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf*
 // synchronisation as bdlu_refactor_values / bdlu_solve.
 int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream);
 int bdlu_solve_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream);
+
+// Brings coo.val up to date from the engine's value buffer after refactors
+// that skipped the host copy (synchronises the device).  Returns a status
+// code and sets the handle's error.
+int bdlu_sync_host_values(bdlu_solver* h);
 
 // Device residency of an analysed handle: release frees every device
 // allocation (the host analysis stays); restore uploads again; bytes is the

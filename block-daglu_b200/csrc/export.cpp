@@ -45,6 +45,7 @@ int ensure_factored(bdlu_solver* h) {
 int bdlu_build_export(bdlu_solver* h) {
   if (h->exported) return BDLU_OK;
   if (const int st = ensure_factored(h)) return st;
+  if (const int st = bdlu_sync_host_values(h)) return st;
   bdlu::Engine& eng = *h->engine;
   const bdlu::Plan& p = eng.plan();
   const auto& d = h->dec;
@@ -185,6 +186,7 @@ int32_t bdlu_get_block_lu(bdlu_solver* h, int32_t b, double* lu_rowmajor, int32_
   // below other units.
   if (!h) return -BDLU_NOT_PREPARED;
   if (!h->factored) return -BDLU_NOT_PREPARED;
+  if (const int st = bdlu_sync_host_values(h)) return -st;
   const auto& d = h->dec;
   if (b < 0 || b >= d.nblocks) return -BDLU_INVALID_INDEX;
   bdlu::Engine& eng = *h->engine;
