@@ -98,6 +98,19 @@ int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   return fail(h, BDLU_FACTORIZATION_FAILED, err);
 }
 
+// True if no entry is NaN or infinite: branch-free over the whole array (no
+// early exit, so the loop vectorises).  One thread: helper threads lost to
+// busy OpenMP workers of the calling process in measurements.
+bool all_finite(const double* v, int64_t n) {
+  uint64_t bad = 0;
+  for (int64_t k = 0; k < n; ++k) {
+    uint64_t x;
+    std::memcpy(&x, v + k, sizeof(x));
+    bad |= static_cast<uint64_t>(((x >> 52) & 0x7ff) == 0x7ff);
+  }
+  return bad == 0;
+}
+
 int upload_values(bdlu_solver* h, const double* vals, bool device, cudaStream_t stream) {
   const size_t bytes = static_cast<size_t>(h->engine->nnz()) * sizeof(double);
   const cudaError_t e = cudaMemcpyAsync(h->engine->values_buffer(), vals, bytes,
@@ -164,18 +177,40 @@ int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf*
   return BDLU_OK;
 }
 
-int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream) {
+// Host values to the engine's value buffer: they travel to a device staging
+// buffer while the host checks them (the copy overlaps the check for pinned
+// buffers) and move to the value buffer only if every entry is finite.  No
+// host copy is kept (10 MB per million entries): coo.val is refreshed from
+// the device when something reads it.
+static int stage_host_values(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream) {
+  std::string err;
+  double* stg = h->engine->value_staging(err);
+  if (!stg) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+  const size_t bytes = static_cast<size_t>(nnz) * sizeof(double);
+  cudaError_t e = cudaMemcpyAsync(stg, vals, bytes, cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return fail(h, BDLU_BACKEND_UNAVAILABLE, std::string("value upload: ") + cudaGetErrorString(e));
+  if (!all_finite(vals, nnz)) {
+    cudaStreamSynchronize(stream);  // the staging copy ends before the error returns
+    return fail(h, BDLU_NON_FINITE_VALUE, "matrix contains NaN or infinity");
+  }
+  e = cudaMemcpyAsync(h->engine->values_buffer(), stg, bytes, cudaMemcpyDeviceToDevice, stream);
+  if (e != cudaSuccess) return fail(h, BDLU_BACKEND_UNAVAILABLE, std::string("value upload: ") + cudaGetErrorString(e));
+  h->host_vals_stale = true;
+  return BDLU_OK;
+}
+
+static int refactor_checks(bdlu_solver* h, const double* vals, int64_t nnz) {
   if (!h) return BDLU_NOT_PREPARED;
   clear_error(h);
   if (!h->decomposed) return fail(h, BDLU_NOT_PREPARED, "analyze must succeed before refactor");
   if (!h->engine) return fail(h, BDLU_BACKEND_UNAVAILABLE, "analysis was run without a device (analysis_only)");
   if (!vals || nnz != h->coo.nnz()) return fail(h, BDLU_INVALID_INDEX, "value count does not match the analysed pattern");
-  for (int64_t k = 0; k < nnz; ++k)
-    if (!std::isfinite(vals[k])) return fail(h, BDLU_NON_FINITE_VALUE, "matrix contains NaN or infinity");
-  // No host copy here (10 MB per million entries): the device buffer holds
-  // the values; coo.val is refreshed from it when something reads it.
-  if (const int st = upload_values(h, vals, false, stream)) return st;
-  h->host_vals_stale = true;
+  return BDLU_OK;
+}
+
+int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream) {
+  if (const int st = refactor_checks(h, vals, nnz)) return st;
+  if (const int st = stage_host_values(h, vals, nnz, stream)) return st;
   return do_factor(h, stream, h->reuse_pivots);
 }
 
@@ -226,9 +261,8 @@ int bdlu_solve_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStre
   if (!h->factored) return fail(h, BDLU_NOT_PREPARED, "factor must succeed before solve");
   if (!B || nrhs < 1 || ldb < h->n) return fail(h, BDLU_INVALID_RHS, "right-hand side size does not match matrix dimension");
   for (int32_t k = 0; k < nrhs; ++k)
-    for (int32_t i = 0; i < h->n; ++i)
-      if (!std::isfinite(B[static_cast<size_t>(k) * ldb + i]))
-        return fail(h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
+    if (!all_finite(B + static_cast<size_t>(k) * ldb, h->n))
+      return fail(h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
   std::string err;
   double* d_B = h->engine->rhs_buffer(nrhs, err);
   if (!d_B) return fail(h, BDLU_SOLVE_FAILED, err);
@@ -412,7 +446,18 @@ int bdlu_solve_device(bdlu_solver* h, double* d_B, int32_t ldb, int32_t nrhs, vo
 }
 
 int bdlu_refactor_solve(bdlu_solver* h, const double* vals, int64_t nnz, double* B, int32_t ldb, int32_t nrhs) {
-  if (const int st = bdlu_refactor_values(h, vals, nnz)) return st;
+  // The factor is queued without its own status wait: the solve reads the
+  // status after its first sweep and redoes a refactor whose reused pivot
+  // order met a zero pivot (with pivoting), or reports a zero pivot.
+  if (const int st = refactor_checks(h, vals, nnz)) return st;
+  if (const int st = stage_host_values(h, vals, nnz, nullptr)) return st;
+  std::string err;
+  h->engine->set_precision(h->mixed ? h->prec_level : 0);
+  h->engine->set_refactor_schedule(h->refactor_schedule);
+  if (!h->engine->factor_async(h->engine->values_buffer(), nullptr, err, h->reuse_pivots))
+    return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+  h->factored = true;
+  h->exported = false;
   return bdlu_solve(h, B, ldb, nrhs);
 }
 

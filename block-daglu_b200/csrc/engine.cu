@@ -532,6 +532,7 @@ void Engine::release() {
   d_norms_ = nullptr;
   d_rtask_ = nullptr;
   d_rwords_ = nullptr;
+  d_vals_stage_ = nullptr;
   work_nrhs_ = 0;
   dp_ = DevPlan{};
 }
@@ -796,6 +797,12 @@ size_t Engine::device_bytes() const {
   size_t b = 0;
   for (const auto& a : allocs_) b += a.second;
   return b;
+}
+
+double* Engine::value_staging(std::string& err) {
+  if (!d_vals_stage_ && !alloc_dev(allocs_, static_cast<size_t>(std::max<int64_t>(plan_.nnz, 1)), &d_vals_stage_, err))
+    return nullptr;
+  return d_vals_stage_;
 }
 
 double* Engine::rhs_buffer(int32_t nrhs, std::string& err) {

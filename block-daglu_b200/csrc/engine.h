@@ -101,6 +101,9 @@ class Engine {
   bool last_residual(cudaStream_t stream, SolveResidual& out, std::string& err);
 
   double* values_buffer() { return d_vals_; }
+  // Device buffer of nnz doubles for host values in flight (allocated at the
+  // first call; counted by device_bytes).
+  double* value_staging(std::string& err);
   // Device buffer of n * nrhs doubles for host-API right-hand sides.
   double* rhs_buffer(int32_t nrhs, std::string& err);
   int64_t nnz() const { return plan_.nnz; }
@@ -134,6 +137,7 @@ class Engine {
   DevPlan dp_{};
   std::vector<std::pair<void*, size_t>> allocs_;  // device allocations and their bytes
   double* d_vals_ = nullptr;
+  double* d_vals_stage_ = nullptr;
   int32_t* d_status_ = nullptr;
   // Solve work space, grown to the largest nrhs seen.
   int32_t work_nrhs_ = 0;
