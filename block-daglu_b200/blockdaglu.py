@@ -102,6 +102,7 @@ def load_library(path=LIB_PATH):
         "bdlu_merge_block_boundaries": (ctypes.c_int32, [_i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p]),
         "bdlu_get_decomposition": (ctypes.c_int, [vp, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]),
         "bdlu_get_block_lu": (ctypes.c_int32, [vp, ctypes.c_int32, _f64p, _i32p]),
+        "bdlu_matrix_signatures": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64)]),
         "bdlu_batch_create": (vp, []),
         "bdlu_batch_destroy": (None, [vp]),
         "bdlu_batch_add": (ctypes.c_int32, [vp, _i32p, _i32p, _f64p, ctypes.c_int64, ctypes.c_int32]),
@@ -287,6 +288,13 @@ class Solver:
         if rc != 0:
             raise RuntimeError("decomposition unavailable (analyze first)")
         return dict(P=P, Q=Q, R=R, off_ptr=optr, off_col=ocol, off_src=osrc, level=lev)
+
+    def signatures(self):
+        """(sig, sig2, value_sig) of the canonical matrix after analyze."""
+        out = (ctypes.c_uint64 * 3)()
+        if self._lib.bdlu_matrix_signatures(self._h, out) != 0:
+            return None
+        return tuple(int(v) for v in out)
 
     def block_lu(self, b):
         """Dense LU (row-major m*m) and pivots of merged block b, as the reference's micro-kernel stores them."""

@@ -142,8 +142,11 @@ int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf*
   h->value_sig = bdlu::matrix_value_sig(h->coo);
   h->mode = mode;
   // The GPU engine runs the block route under AUTO; "klu" forces the global
-  // route, which here means one diagonal block with partial pivoting.
+  // route, which here means one diagonal block with partial pivoting.  AUTO
+  // still takes the reference's route decision so selected_mode() reports
+  // what the reference would select (solver.cpp:846-861).
   h->global_route = (h->mode == BDLU_MODE_KLU);
+  h->auto_picked_klu = (h->mode == BDLU_MODE_AUTO) && !bdlu::auto_choose_block(h->n, h->coo);
   h->decomposed = false;
   h->factored = false;
   h->exported = false;
@@ -386,6 +389,7 @@ int bdlu_set_coo(bdlu_solver* h, const int32_t* rows, const int32_t* cols, const
   h->exported = false;
   h->mode = BDLU_MODE_AUTO;
   h->global_route = false;
+  h->auto_picked_klu = false;
   return BDLU_OK;
 }
 
@@ -473,7 +477,9 @@ int bdlu_last_error(const bdlu_solver* h, char* buf, int64_t len) {
 
 int32_t bdlu_n(const bdlu_solver* h) { return h ? h->n : 0; }
 
-const char* bdlu_selected_mode(const bdlu_solver* h) { return (h && h->global_route) ? "KLU" : "BLOCK"; }
+const char* bdlu_selected_mode(const bdlu_solver* h) {
+  return (h && (h->global_route || h->auto_picked_klu)) ? "KLU" : "BLOCK";
+}
 
 int64_t bdlu_canonical_pattern(const bdlu_solver* h, int32_t* rows, int32_t* cols) {
   if (!h || !h->validated) return 0;
@@ -481,6 +487,14 @@ int64_t bdlu_canonical_pattern(const bdlu_solver* h, int32_t* rows, int32_t* col
   if (rows) std::memcpy(rows, h->coo.row.data(), static_cast<size_t>(nnz) * sizeof(int32_t));
   if (cols) std::memcpy(cols, h->coo.col.data(), static_cast<size_t>(nnz) * sizeof(int32_t));
   return nnz;
+}
+
+int bdlu_matrix_signatures(const bdlu_solver* h, uint64_t* sigs) {
+  if (!h || !sigs || !h->decomposed) return BDLU_NOT_PREPARED;
+  sigs[0] = h->sig;
+  sigs[1] = h->sig2;
+  sigs[2] = h->value_sig;
+  return BDLU_OK;
 }
 
 int bdlu_get_stats(const bdlu_solver* h, bdlu_stats* out) {

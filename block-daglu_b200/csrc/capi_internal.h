@@ -26,6 +26,10 @@ struct bdlu_solver {
   uint64_t sig = 0, sig2 = 0, value_sig = 0;
   int mode = BDLU_MODE_AUTO;
   bool global_route = false;  // "KLU": one block, no BTF
+  // AUTO's route decision (solver.cpp:846-861, auto_choose_block): reported
+  // by selected_mode() like the reference's; the numerics stay
+  // block-structured either way.
+  bool auto_picked_klu = false;
   bdlu::Decomposition dec;
   std::unique_ptr<bdlu::Engine> engine;
   // Options.

@@ -7,9 +7,9 @@
 // inside another framework's step that must not grow the device footprint.
 // The handle-based API (bdlu_create / bdlu_analyze / ...) allocates its
 // per-pattern device structures; this entry point instead keeps its scratch
-// (LU factors, pivots, a status word) in one file-scope static device array
+// (LU factors, pivots, per-matrix failure flags, a status word) in one file-scope static device array
 // that is part of the library image: every GPU that loads the library holds
-// it (about 8.3 MiB) until the process exits.
+// it (about 8.5 MiB) until the process exits.
 //
 // It is a variant of the engine's dense-unit path: the factor kernel is the
 // same partial-pivoting LU as k_lu_small in engine.cu (first strict maximum,
@@ -30,12 +30,14 @@ namespace {
 constexpr int kNaMaxM = 128;                      // rows of one matrix
 constexpr long long kNaLuDoubles = 1LL << 20;     // batch * m * m <= 1,048,576 (8 MiB)
 constexpr long long kNaPivInts = 1LL << 16;       // batch * m <= 65,536
-constexpr long long kNaScratchDoubles = kNaLuDoubles + kNaPivInts / 2 + 32;
+constexpr long long kNaFlagInts = kNaPivInts;      // one failure flag per matrix (batch <= batch * m)
+constexpr long long kNaScratchDoubles = kNaLuDoubles + kNaPivInts / 2 + kNaFlagInts / 2 + 32;
 constexpr int kNaThreads = 256;
 constexpr int kNaMaxDevices = 64;
 
-// The scratch: [0, kNaLuDoubles) factors, then pivots (int32), then two
-// int32 status words.  Host code must not use this name as an address.
+// The scratch: [0, kNaLuDoubles) factors, then pivots (int32), then one
+// failure flag per matrix (int32), then two int32 status words.  Host code
+// must not use this name as an address.
 static __device__ __align__(256) double g_noalloc_scratch[kNaScratchDoubles];
 
 std::mutex g_na_mu;
@@ -59,8 +61,10 @@ __device__ __forceinline__ void na_warp_pivot(double& best, int& bi, int none) {
 }
 
 // One CTA per matrix: the matrix in shared memory, factors to the scratch.
+// Every matrix writes its failure flag (0 or 1), so the flags need no
+// clearing between calls.
 __global__ void __launch_bounds__(kNaThreads) k_noalloc_lu(const double* __restrict__ A, int m, double* lu,
-                                                           int32_t* piv_all, int32_t* status) {
+                                                           int32_t* piv_all, int32_t* failed, int32_t* status) {
   extern __shared__ double S[];
   __shared__ double s_best[kNaThreads / 32];
   __shared__ int s_bi[kNaThreads / 32];
@@ -100,8 +104,12 @@ __global__ void __launch_bounds__(kNaThreads) k_noalloc_lu(const double* __restr
     }
     __syncthreads();
     const int p = s_piv;
-    if (s_pbest == 0.0) {
-      if (tid == 0 && atomicCAS(status, 0, 1) == 0) status[1] = blockIdx.x;
+    // A zero or NaN pivot magnitude fails the matrix.
+    if (!(s_pbest > 0.0)) {
+      if (tid == 0) {
+        failed[blockIdx.x] = 1;
+        if (atomicCAS(status, 0, 1) == 0) status[1] = blockIdx.x;
+      }
       return;
     }
     if (tid == 0) piv[k] = p;
@@ -127,14 +135,18 @@ __global__ void __launch_bounds__(kNaThreads) k_noalloc_lu(const double* __restr
   }
   double* out = lu + blockIdx.x * mm;
   for (int i = tid; i < mm; i += kNaThreads) out[i] = S[i];
+  if (tid == 0) failed[blockIdx.x] = 0;
 }
 
 // One CTA per (matrix, right-hand side).  B and X may be the same buffer.
+// A matrix whose factorisation failed is skipped: its X block is not written.
 __global__ void __launch_bounds__(kNaThreads) k_noalloc_solve(const double* __restrict__ lu_all,
-                                                              const int32_t* __restrict__ piv_all, int m, int nrhs,
+                                                              const int32_t* __restrict__ piv_all,
+                                                              const int32_t* __restrict__ failed, int m, int nrhs,
                                                               const double* B, double* X) {
   __shared__ double x[kNaMaxM];
   const int mat = blockIdx.x / nrhs, col = blockIdx.x - (blockIdx.x / nrhs) * nrhs;
+  if (failed[mat] != 0) return;  // CTA-uniform
   const long long base = (static_cast<long long>(mat) * nrhs + col) * m;
   const double* LU = lu_all + static_cast<long long>(mat) * m * m;
   const int32_t* piv = piv_all + static_cast<long long>(mat) * m;
@@ -223,13 +235,16 @@ extern "C" int bdlu_dense_batch_solve_noalloc(const double* d_A, int32_t m, int3
   auto* s = static_cast<cudaStream_t>(stream);
   double* lu = base;
   auto* piv = reinterpret_cast<int32_t*>(base + kNaLuDoubles);
-  auto* status = reinterpret_cast<int32_t*>(base + kNaLuDoubles + kNaPivInts / 2);
+  auto* failed = reinterpret_cast<int32_t*>(base + kNaLuDoubles + kNaPivInts / 2);
+  auto* status = reinterpret_cast<int32_t*>(base + kNaLuDoubles + kNaPivInts / 2 + kNaFlagInts / 2);
   // The scratch keeps the previous call's contents; only the status words
-  // must start at zero (factors and pivots are fully rewritten).
+  // must start at zero (factors, pivots and failure flags are rewritten for
+  // every matrix of the call before the solve reads them).
   cudaError_t e = cudaMemsetAsync(status, 0, 2 * sizeof(int32_t), s);
   if (e == cudaSuccess) {
-    k_noalloc_lu<<<batch, kNaThreads, static_cast<size_t>(m) * m * sizeof(double), s>>>(d_A, m, lu, piv, status);
-    k_noalloc_solve<<<batch * nrhs, kNaThreads, 0, s>>>(lu, piv, m, nrhs, d_B, d_X);
+    k_noalloc_lu<<<batch, kNaThreads, static_cast<size_t>(m) * m * sizeof(double), s>>>(d_A, m, lu, piv, failed,
+                                                                                         status);
+    k_noalloc_solve<<<batch * nrhs, kNaThreads, 0, s>>>(lu, piv, failed, m, nrhs, d_B, d_X);
     e = cudaGetLastError();
   }
   int32_t h_status[2] = {0, 0};

@@ -271,7 +271,7 @@ int bdlu_server_last_error(const bdlu_server* s, char* buf, int64_t len);
  * implicit synchronisation, code called back inside another framework's step):
  * solves A_i X_i = B_i for `batch` dense m x m matrices with the engine's
  * dense-block partial-pivoting LU, using only the caller's buffers and a
- * static device scratch built into the library (about 8.3 MiB, held on every
+ * static device scratch built into the library (about 8.5 MiB, held on every
  * GPU that loads the library until exit).  No cudaMalloc, cudaFree or other
  * allocating call is made.
  *   d_A: batch matrices, each m*m column-major, contiguous (not modified).
@@ -279,10 +279,12 @@ int bdlu_server_last_error(const bdlu_server* s, char* buf, int64_t len);
  *   be the same buffer as B.
  * Limits: m <= 128, batch*m*m <= 1048576, batch*m <= 65536; larger sizes
  * return BDLU_INVALID_DIMENSION with a message.  A singular matrix returns
- * BDLU_FACTORIZATION_FAILED (X is then unspecified).  Uses the calling
+ * BDLU_FACTORIZATION_FAILED (a zero or NaN pivot); the X block of every
+ * matrix that failed is left unwritten (with X the same buffer as B it still
+ * holds B) and the other matrices are solved.  Uses the calling
  * thread's current device; the call waits for `stream` before returning.
  * The first call on a device resolves the scratch's address and sets a kernel
- * attribute; make that first call before any stream capture.  Every call on a
+ * attribute, so make it before any stream capture begins.  Every call on a
  * device shares the one scratch, so calls whose work overlaps on the GPU (other
  * streams, other host threads) race and must be serialised by the caller.
  * msg (may be NULL) receives an error message of at most msg_len bytes. */
@@ -311,6 +313,12 @@ int bdlu_get_decomposition(const bdlu_solver* h, int32_t* P, int32_t* Q, int32_t
  * micro-kernel, ubtf_block_solver.cpp:1450-1498): m*m values row-major and m
  * LAPACK-style pivots.  Returns m, or -(status). */
 int32_t bdlu_get_block_lu(bdlu_solver* h, int32_t b, double* lu_rowmajor, int32_t* piv);
+
+/* Pattern and value signatures of the canonical matrix after analyze
+ * (compute_matrix_sig, compute_matrix_sig2, compute_matrix_value_sig,
+ * blockdaglu/src/solver.cpp:96-136): sigs[0..2].  The serving loop keys its
+ * resident patterns by them. */
+int bdlu_matrix_signatures(const bdlu_solver* h, uint64_t* sigs);
 
 /* ---- Seeded synthetic systems --------------------------------------------- */
 enum bdlu_synth_family { BDLU_SYNTH_BLOCK = 0, BDLU_SYNTH_CIRCUIT = 1, BDLU_SYNTH_PRECISION = 3 };

@@ -30,7 +30,8 @@ def load():
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(os.path.join(HERE, "bdlu_oracle.c")):
+    srcs = ("bdlu_oracle.c", "btf_oracle.c", "synth_oracle.c")
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(os.path.join(HERE, f)) for f in srcs):
         build()
     lib = ctypes.CDLL(LIB)
     vp = ctypes.c_void_p
@@ -51,6 +52,13 @@ def load():
         "or_nblocks": (ctypes.c_int32, [vp]),
         "or_offdiag_nnz": (ctypes.c_int32, [vp]),
         "or_get_offdiag": (None, [vp, _i32p, _i32p, _f64p]),
+        "or_btf_order": (ctypes.c_int32, [ctypes.c_int32, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]),
+        "or_synth_create": (vp, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+        "or_synth_free": (None, [vp]),
+        "or_synth_n": (ctypes.c_int32, [vp]),
+        "or_synth_nnz": (ctypes.c_int64, [vp]),
+        "or_synth_copy": (None, [vp, _i32p, _i32p, _f64p, _f64p, _f64p]),
+        "or_synth_perturb": (None, [vp, ctypes.c_uint64, _f64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -99,6 +107,140 @@ def metrics(rows, cols, vals, x, b, x_true=None, n=None):
     lib.or_metrics(int(n if n is not None else len(xx)), len(r), _p32(r), _p32(c), _p64(v), _p64(xx), _p64(bb), _p64(xt),
                    _p64(out))
     return float(out[0]), float(out[1]), float(out[2])
+
+
+def btf_order(n, col_ptr, row_ind):
+    """The oracle's block triangular form (btf_oracle.c), SuiteSparse btf_order
+    conventions: (nblocks, P, Q, R, nmatch)."""
+    lib = load()
+    ap = np.ascontiguousarray(col_ptr, np.int32)
+    ai = np.ascontiguousarray(row_ind, np.int32)
+    P, Q, R = np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n + 1, np.int32)
+    nm = np.zeros(1, np.int32)
+    nb = lib.or_btf_order(int(n), _p32(ap), _p32(ai), _p32(P), _p32(Q), _p32(R), _p32(nm))
+    if nb < 0:
+        raise MemoryError("or_btf_order failed")
+    return nb, P, Q, R[: nb + 1].copy(), int(nm[0])
+
+
+FAMILY_BLOCK, FAMILY_CIRCUIT = 0, 1
+
+
+def config_seed(config, instance=0):
+    """Seeds of the synthetic configurations: 20261203 + 1000*config + instance."""
+    return 20261203 + 1000 * config + instance
+
+
+class Synth:
+    """Seeded synthetic system from the oracle's generator (synth_oracle.c):
+    canonical COO, x_true, b; same draws as the benchmark's generator."""
+
+    def __init__(self, family, seed, n, param=0, nrhs=1):
+        self._lib = load()
+        self._s = self._lib.or_synth_create(int(family), int(seed), int(n), int(param), int(nrhs))
+        if not self._s:
+            raise ValueError("unknown synthetic family %r" % family)
+        self.n = self._lib.or_synth_n(self._s)
+        self.nnz = self._lib.or_synth_nnz(self._s)
+        self.nrhs = max(1, int(nrhs))
+        self.rows = np.empty(self.nnz, np.int32)
+        self.cols = np.empty(self.nnz, np.int32)
+        self.vals = np.empty(self.nnz, np.float64)
+        self.x_true = np.empty((self.n, self.nrhs), np.float64, order="F")
+        self.b = np.empty((self.n, self.nrhs), np.float64, order="F")
+        self._lib.or_synth_copy(self._s, _p32(self.rows), _p32(self.cols), _p64(self.vals), _p64(self.x_true),
+                                _p64(self.b))
+
+    def perturbed(self, seed):
+        out = np.empty(self.nnz, np.float64)
+        self._lib.or_synth_perturb(self._s, int(seed), _p64(out))
+        return out
+
+    def __del__(self):
+        s, self._s = getattr(self, "_s", None), None
+        if s and getattr(self, "_lib", None) is not None:
+            self._lib.or_synth_free(s)
+
+
+_ref = None
+
+
+def load_reference():
+    """The reference's own sources built under _ref (make -C oracle ref)."""
+    global _ref
+    if _ref is not None:
+        return _ref
+    if not os.path.exists(REF_LIB):
+        raise FileNotFoundError(REF_LIB)
+    lib = ctypes.CDLL(REF_LIB)
+    vp = ctypes.c_void_p
+    sig = {
+        "ref_solver_create": (vp, []),
+        "ref_solver_destroy": (None, [vp]),
+        "ref_solver_set_coo": (ctypes.c_int, [vp, _i32p, _i32p, _f64p, ctypes.c_int64, ctypes.c_int32]),
+        "ref_solver_analyze": (ctypes.c_int, [vp]),
+        "ref_solver_factor": (ctypes.c_int, [vp]),
+        "ref_solver_solve": (ctypes.c_int, [vp, _f64p, ctypes.c_int32]),
+        "ref_solver_mode": (ctypes.c_char_p, [vp]),
+        "ref_solver_error": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_int64]),
+        "btf_standin_inject": (None, [ctypes.c_int32, _i32p, _i32p, _i32p, ctypes.c_int32, ctypes.c_int32]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _ref = lib
+    return lib
+
+
+def inject_reference_btf(n, P=None, Q=None, R=None, nmatch=None):
+    """Makes the reference build's btf_order return (P, Q, R) for order-n
+    patterns (parity tests start both sides from one ordering); with P None
+    the injection is cleared and the oracle's own BTF runs again."""
+    lib = load_reference()
+    if P is None:
+        lib.btf_standin_inject(-1, None, None, None, 0, 0)
+        return
+    p, q, r = (np.ascontiguousarray(a, np.int32) for a in (P, Q, R))
+    lib.btf_standin_inject(int(n), _p32(p), _p32(q), _p32(r), len(r) - 1, int(n if nmatch is None else nmatch))
+
+
+class RefSolver:
+    """blockdaglu::Solver of the reference build (set_matrix / analyze / factor /
+    solve_in_place / selected_mode), for parity tests and the CPU baseline."""
+
+    def __init__(self):
+        self._lib = load_reference()
+        self._h = self._lib.ref_solver_create()
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            self._lib.ref_solver_destroy(h)
+
+    def set_matrix(self, rows, cols, vals, n=-1):
+        r = np.ascontiguousarray(rows, np.int32)
+        c = np.ascontiguousarray(cols, np.int32)
+        v = np.ascontiguousarray(vals, np.float64)
+        return self._lib.ref_solver_set_coo(self._h, _p32(r), _p32(c), _p64(v), len(r), int(n)) == 0
+
+    def analyze(self):
+        return self._lib.ref_solver_analyze(self._h) == 0
+
+    def factor(self):
+        return self._lib.ref_solver_factor(self._h) == 0
+
+    def solve_in_place(self, b):
+        assert b.dtype == np.float64 and b.flags.c_contiguous
+        return self._lib.ref_solver_solve(self._h, _p64(b), len(b)) == 0
+
+    def selected_mode(self):
+        return self._lib.ref_solver_mode(self._h).decode()
+
+    def last_error_message(self):
+        buf = ctypes.create_string_buffer(512)
+        self._lib.ref_solver_error(self._h, buf, 512)
+        return buf.value.decode()
 
 
 class System:

@@ -1,7 +1,14 @@
 // C entry points into the reference's own code (compiled from its sources
-// under /root/reference by oracle/Makefile into oracle/_ref/libbdlu_ref.so).
+// where they lie, by oracle/Makefile, into oracle/_ref/libbdlu_ref.so).
 // Test infrastructure only: tests and bench.py's reference arm call these to
 // run the reference's Solver, decomposition, block factor and block solve.
+//
+// blockdaglu/src/solver.cpp is compiled as part of this translation unit
+// (included unmodified) so that its file-local helpers -- the pattern and
+// value signatures and the canonicalisation -- can be called for parity
+// checks; the library contains it once.
+#include "solver.cpp"
+
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -41,6 +48,25 @@ int ref_solver_solve(void* h, double* b, int32_t n) {
 }
 
 const char* ref_solver_mode(void* h) { return static_cast<Solver*>(h)->selected_mode(); }
+
+// validate_and_canonicalize_matrix, then compute_matrix_sig / sig2 /
+// value_sig (solver.cpp:96-136, :642-722) on the canonical COO.  Returns 0,
+// or the SolverError code of a rejected input.
+int ref_matrix_sigs(const int32_t* r, const int32_t* c, const double* v, int64_t nnz, int32_t dim, int32_t* n_out,
+                    uint64_t* sigs) {
+  CooMatrix m;
+  m.reserve(static_cast<size_t>(nnz));
+  for (int64_t k = 0; k < nnz; ++k) m.emplace_back(r[k], c[k], v[k]);
+  int32_t n = 0;
+  blockdaglu::SolverError err = blockdaglu::SolverError::None;
+  std::string msg;
+  if (!blockdaglu::validate_and_canonicalize_matrix(m, dim, n, err, msg)) return static_cast<int>(err);
+  if (n_out) *n_out = n;
+  sigs[0] = blockdaglu::compute_matrix_sig(n, m);
+  sigs[1] = blockdaglu::compute_matrix_sig2(n, m);
+  sigs[2] = blockdaglu::compute_matrix_value_sig(m);
+  return 0;
+}
 
 int ref_solver_error(void* h, char* buf, int64_t len) {
   auto* s = static_cast<Solver*>(h);

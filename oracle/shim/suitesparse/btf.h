@@ -1,9 +1,10 @@
 /*
  * Stand-in declaration of SuiteSparse btf_order (blockdaglu/src/btf_dynamic.h:
  * 19-28 calling convention) for compiling the reference's sources as an
- * oracle.  btf_standin.c forwards to the engine's btf_order so both sides of a
- * parity test start from the same permutation (SuiteSparse's own traversal
- * order is not available here).
+ * oracle.  btf_standin.c runs the oracle's own block triangular form
+ * (oracle/btf_oracle.c), or an ordering a parity test injected so both sides
+ * start from the same permutation (SuiteSparse's own traversal order is not
+ * available here).
  */
 #ifndef BDLU_SHIM_BTF_H_
 #define BDLU_SHIM_BTF_H_

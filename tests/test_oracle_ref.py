@@ -7,6 +7,7 @@ import subprocess
 
 import numpy as np
 import pytest
+import scipy.sparse as sp
 
 import blockdaglu as bd
 import oracle
@@ -65,7 +66,17 @@ def test_oracle_and_engine_analysis_equal_reference(monkeypatch, family, seed, n
     monkeypatch.setenv("USERALGO_BLOCK_SCHED", "level")
     g = bd.Synth(family, seed, n)
     lib = ref_lib()
-    run = lib.ref_decompose(p32(g.rows), p32(g.cols), p64(g.vals), g.nnz, g.n)
+    # The reference build's btf_order is the oracle's own BTF; here it is
+    # handed the engine's ordering of the same pattern (n < 50,000: no small
+    # entries dropped) so both sides start from one permutation.
+    a = sp.csc_matrix((np.ones(g.nnz), (g.rows, g.cols)), shape=(g.n, g.n))
+    a.sort_indices()
+    nb_e, P_e, Q_e, R_e, nm_e = bd.btf_order(g.n, a.indptr, a.indices)
+    oracle.inject_reference_btf(g.n, P_e, Q_e, R_e, nm_e)
+    try:
+        run = lib.ref_decompose(p32(g.rows), p32(g.cols), p64(g.vals), g.nnz, g.n)
+    finally:
+        oracle.inject_reference_btf(g.n)
     assert run
     try:
         nb, noff = lib.ref_nblocks(run), lib.ref_offdiag_nnz(run)
@@ -111,3 +122,40 @@ def test_oracle_and_engine_analysis_equal_reference(monkeypatch, family, seed, n
         assert oracle.metrics(g.rows, g.cols, g.vals, xo, g.b[:, 0])[0] <= 1e-12
     finally:
         lib.ref_run_free(run)
+
+
+@pytest.mark.parametrize("family,seed,n,mode", [
+    (bd.FAMILY_BLOCK, bd.config_seed(0), 2000, "KLU"),
+    (bd.FAMILY_CIRCUIT, bd.config_seed(1, 3), 20000, "KLU"),
+    (bd.FAMILY_CIRCUIT, bd.config_seed(1, 4), 60000, "BLOCK"),
+    (bd.FAMILY_BLOCK, bd.config_seed(2, 7), 45000, "KLU"),
+])
+def test_auto_route_and_signatures_equal_reference(monkeypatch, family, seed, n, mode):
+    """selected_mode() under AUTO and the three matrix signatures, engine vs the
+    reference's own code (solver.cpp:96-136, :448-506, :846-861).  The
+    reference build analyses with the oracle's BTF; no engine code there."""
+    monkeypatch.delenv("BLOCKDAGLU_MODE", raising=False)
+    monkeypatch.delenv("USERALGO_MODE", raising=False)
+    g = oracle.Synth(family, seed, n)
+    # Shuffled input order with a duplicate pair, so canonicalisation matters.
+    rng = np.random.default_rng(n)
+    perm = rng.permutation(g.nnz)
+    rows = np.concatenate([g.rows[perm], g.rows[:1]])
+    cols = np.concatenate([g.cols[perm], g.cols[:1]])
+    vals = np.concatenate([g.vals[perm], [g.vals[0] * 0.5]])
+    vals[np.argsort(perm)[0]] = g.vals[0] * 0.5
+    lib = oracle.load_reference()
+    lib.ref_matrix_sigs.restype = ctypes.c_int
+    lib.ref_matrix_sigs.argtypes = [_i32p, _i32p, _f64p, ctypes.c_int64, ctypes.c_int32,
+                                    ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_uint64)]
+    sigs = (ctypes.c_uint64 * 3)()
+    nref = ctypes.c_int32()
+    assert lib.ref_matrix_sigs(p32(rows), p32(cols), p64(vals), len(rows), -1, ctypes.byref(nref), sigs) == 0
+    s = bd.Solver()
+    s.set_option("analysis_only", 1)
+    assert s.set_matrix((rows, cols, vals), -1) and s.analyze(), s.last_error_message()
+    assert s.n() == nref.value == g.n
+    assert s.signatures() == tuple(int(v) for v in sigs)
+    ref = oracle.RefSolver()
+    assert ref.set_matrix(rows, cols, vals, -1) and ref.analyze(), ref.last_error_message()
+    assert s.selected_mode() == ref.selected_mode() == mode

@@ -56,13 +56,15 @@ def handle_solution(A, B):
     return np.stack([X[i * m:(i + 1) * m] for i in range(batch)])
 
 
-def device_call(fn, A, B, torch, in_place=False):
+def device_call(fn, A, B, torch, in_place=False, fill=None):
     batch, m, _ = A.shape
     nrhs = B.shape[2]
     # Column-major per matrix / per RHS block, matrices contiguous.
     dA = torch.from_numpy(np.ascontiguousarray(A.transpose(0, 2, 1))).cuda()
     dB = torch.from_numpy(np.ascontiguousarray(B.transpose(0, 2, 1))).cuda()
     dX = dB if in_place else torch.empty_like(dB)
+    if fill is not None and not in_place:
+        dX.fill_(fill)
     msg = ctypes.create_string_buffer(256)
     stream = torch.cuda.current_stream().cuda_stream
     rc = fn(dA.data_ptr(), m, batch, dB.data_ptr(), dX.data_ptr(), nrhs, stream, msg, 256)
@@ -96,12 +98,42 @@ def test_noalloc_rejects_sizes_beyond_limit(cuda_device):
     assert rc == bd.SolverError.InvalidDimension and "1048576" in msg
 
 
-def test_noalloc_singular_matrix_reported(cuda_device):
+def test_noalloc_at_exact_limits(cuda_device):
+    """m = 128 (128 KiB of dynamic shared memory per matrix) with
+    batch * m * m exactly 1,048,576; one entry more is refused, and so is
+    batch * m above 65,536 while batch * m * m stays within its limit."""
     import torch
     fn = noalloc_fn()
-    A = np.zeros((2, 4, 4))
-    A[0] = np.eye(4)
-    A[1, :, 0] = 1.0  # rank 1
-    B = np.ones((2, 4, 1))
+    rng = np.random.default_rng(128)
+    A, B = random_batch(rng, 64, 128, 2)
+    rc, msg, X = device_call(fn, A, B, torch)
+    assert rc == bd.SolverError.None_, msg
+    assert close_vec(X, np.linalg.solve(A, B), 1e-9)
+    A, B = random_batch(rng, 8193, 8, 1)  # 8193 * 8 = 65544 rows; 524352 factor entries
     rc, msg, _ = device_call(fn, A, B, torch)
+    assert rc == bd.SolverError.InvalidDimension and "65536" in msg
+
+
+def test_noalloc_singular_matrix_reported(cuda_device):
+    """A failed matrix is reported, its X block is left unwritten and the
+    other matrices of the batch are still solved; a NaN pivot counts as a
+    failure."""
+    import torch
+    fn = noalloc_fn()
+    A = np.zeros((3, 4, 4))
+    A[0] = np.eye(4) * 2.0
+    A[1, :, 0] = 1.0  # rank 1
+    A[2] = np.eye(4)
+    B = np.ones((3, 4, 2))
+    rc, msg, X = device_call(fn, A, B, torch, fill=-7.0)
     assert rc == bd.SolverError.FactorizationFailed and "matrix 1" in msg
+    assert np.all(X[1] == -7.0)
+    assert np.array_equal(X[0], B[0] / 2.0) and np.array_equal(X[2], B[2])
+    rc, msg, X = device_call(fn, A, B, torch, in_place=True)
+    assert rc == bd.SolverError.FactorizationFailed
+    assert np.array_equal(X[1], B[1])
+    A[1] = np.eye(4)
+    A[1, 2, 2] = np.nan
+    rc, msg, X = device_call(fn, A, B, torch, fill=-7.0)
+    assert rc == bd.SolverError.FactorizationFailed and "matrix 1" in msg
+    assert np.all(X[1] == -7.0)
