@@ -174,50 +174,149 @@ def step_inputs(g, k):
     return v, b
 
 
-def cpu_baseline_port(g):
-    """Oracle port on the host: one full refactor + solve of the same system."""
+def host_cpu():
+    """(usable cores, CPU model) of this host."""
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        cores = os.cpu_count() or 1
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return cores, model
+
+
+def oracle_module():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import blockdaglu as bd
     import oracle
-    s = bd.Solver()
-    s.set_option("analysis_only", 1)
-    assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze()
-    d = s.decomposition()
+    return oracle
+
+
+def oracle_circuit_system():
+    """The circuit-200k system from the oracle's own generator (identical to the
+    engine arm's; checked by tests/test_oracle_synth.py)."""
+    oracle = oracle_module()
+    return oracle.Synth(oracle.FAMILY_CIRCUIT, oracle.config_seed(CONFIG_INDEX), N_ROWS)
+
+
+def reference_route(g, steps, warm, threads, nrhs_of=None, step_inputs_fn=None):
+    """The reference's BLOCK route (its own solver.cpp / ubtf_block_solver.cpp
+    built under oracle/_ref, SuiteSparse stand-ins) as a caller of its API runs
+    a value change: set_matrix(new values) + analyze + factor +
+    solve_in_place, on one Solver.  threads: USERALGO_THREADS (None: the
+    reference's own default policy).  Returns per-phase means in seconds."""
+    oracle = oracle_module()
+    if threads:
+        os.environ["USERALGO_THREADS"] = str(threads)
+    else:
+        os.environ.pop("USERALGO_THREADS", None)
+    os.environ.pop("USERALGO_MODE", None)
+    os.environ.pop("BLOCKDAGLU_MODE", None)
+    s = oracle.RefSolver()
+    rec, worst = [], 0.0
+    fn = step_inputs_fn or step_inputs
+    for k in range(warm + steps):
+        v, b = fn(g, k)
+        t0 = time.perf_counter()
+        ok = s.set_matrix(g.rows, g.cols, v, g.n) and s.analyze()
+        t1 = time.perf_counter()
+        ok = ok and s.factor()
+        t2 = time.perf_counter()
+        x = np.ascontiguousarray(b, np.float64).copy()
+        ok = ok and s.solve_in_place(x)
+        t3 = time.perf_counter()
+        if not ok:
+            raise RuntimeError("reference route failed: " + s.last_error_message())
+        if k >= warm:
+            rec.append((t1 - t0, t2 - t1, t3 - t2))
+            worst = max(worst, oracle.metrics(g.rows, g.cols, v, x, b)[0])
+    os.environ.pop("USERALGO_THREADS", None)
+    mean = [statistics.mean(r[i] for r in rec) for i in range(3)]
+    return {"analyze_s": mean[0], "factor_s": mean[1], "solve_s": mean[2], "step_s": sum(mean),
+            "factor_solve_s": mean[1] + mean[2], "steps": len(rec), "residual_inf_max": worst,
+            "mode": s.selected_mode()}
+
+
+def port_step(g):
+    """The oracle's C restatement (bdlu_oracle.c), one thread: one factor + solve
+    of the system under the oracle's own BTF ordering."""
+    oracle = oracle_module()
+    import scipy.sparse as sp
     v, b = step_inputs(g, 0)
     t0 = time.perf_counter()
-    ref = oracle.System(g.n, g.rows, g.cols, v, d["P"], d["Q"], d["R"])
+    a = sp.csc_matrix((np.ones(g.nnz), (g.rows, g.cols)), shape=(g.n, g.n))
+    a.sort_indices()
+    nb, P, Q, R, _ = oracle.btf_order(g.n, a.indptr, a.indices)
+    Q = np.where(Q < -1, -Q - 2, Q)
+    R = oracle.merge_block_boundaries(R, g.n)
+    ref = oracle.System(g.n, g.rows, g.cols, v, P, Q, R)
     ok = ref.factor()
     x = ref.solve(b)
     dt = time.perf_counter() - t0
-    resid = oracle.metrics(g.rows, g.cols, v, x, b)[0]
-    return {"value": 1.0 / dt, "unit": METRIC, "cores": 1, "kind": "port",
-            "sample": "1 value-only refactor + 1-RHS solve of the full %s system by the oracle "
-                      "(reference dense micro-kernel on every merged block, reverse block solve, "
-                      "single thread): %.1f s, residual %.1e%s" % (WORKLOAD, dt, resid, "" if ok else ", FAILED")}
+    return dt, oracle.metrics(g.rows, g.cols, v, x, b)[0], ok
+
+
+def cpu_baseline_reference(g):
+    """cpu_baseline of the engine arm: one timed value change of the circuit-200k
+    system through the reference's BLOCK route on all host cores, after one
+    untimed step."""
+    cores, model = host_cpu()
+    r = reference_route(g, 1, 1, cores)
+    return {"value": 1.0 / r["step_s"], "unit": METRIC, "cores": cores, "kind": "reference",
+            "sample": "1 timed value change (set_matrix + analyze + factor + 1-RHS solve, after 1 untimed) of the "
+                      "full %s system by the reference's BLOCK route built under oracle/_ref (its own solver.cpp and "
+                      "ubtf_block_solver.cpp; KLU and BTF are stand-ins: SuiteSparse is unavailable on this box), "
+                      "USERALGO_THREADS=%d on %s: analyze %.2f s, factor %.2f s, solve %.3f s, residual %.1e"
+                      % (WORKLOAD, cores, model, r["analyze_s"], r["factor_s"], r["solve_s"], r["residual_inf_max"])}
 
 
 def run_reference(args, rank, world):
-    """The reference's CPU route on the same workload (rank 0 only)."""
+    """The reference's CPU route on the circuit-200k workload (rank 0 only):
+    all host cores for the line's value, the reference's default thread
+    policy and the oracle's one-thread restatement beside it."""
     if rank != 0:
         return
-    g = circuit_system()
-    steps = max(1, min(args.steps, 2))
+    cores, model = host_cpu()
+    g = oracle_circuit_system()
+    steps = max(1, min(args.steps, 3))
     warm = 1 if args.warmup > 0 else 0
-    times = []
-    for k in range(warm + steps):
-        base = cpu_baseline_port(g)
-        if k >= warm:
-            times.append(1.0 / base["value"])
-    t = statistics.mean(times)
+    allc = reference_route(g, steps, warm, cores)
+    dflt = reference_route(g, 1, 0, None)
+    port_s, port_res, port_ok = port_step(g)
+    t = allc["step_s"]
     line = {"metric": METRIC, "value": 1.0 / t, "unit": METRIC, "n_gpus": args.gpus, "steps": steps,
             "warmup": warm, "ms_per_step": 1000.0 * t, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "n": g.n, "nnz": int(g.nnz), "nrhs": 1},
             "impl": "reference",
-            "cpu_baseline": {"value": 1.0 / t, "unit": METRIC, "cores": 1, "kind": "port",
-                             "sample": "%d timed full refactor+solve steps (of --steps %d, bounded to keep the run "
-                                       "within minutes) by the oracle port; SuiteSparse KLU is unavailable on this "
-                                       "box" % (steps, args.steps)},
+            "same_steps": steps == args.steps and warm == args.warmup,
+            "same_steps_reason": None if steps == args.steps else
+            "each reference step takes seconds on the host: %d timed steps of --steps %d keep the run within minutes"
+            % (steps, args.steps),
+            "cpu_baseline": {"value": 1.0 / t, "unit": METRIC, "cores": cores, "kind": "reference",
+                             "sample": "%d timed value changes (set_matrix + analyze + factor + 1-RHS solve) of the "
+                                       "full system by the reference's BLOCK route built under oracle/_ref (its own "
+                                       "solver.cpp and ubtf_block_solver.cpp; KLU and BTF are stand-ins: SuiteSparse "
+                                       "is unavailable on this box), USERALGO_THREADS=%d on %s"
+                                       % (steps, cores, model)},
+            "reference_phases_s": {k: allc[k] for k in ("analyze_s", "factor_s", "solve_s")},
+            "reference_factor_solve_only": {"value": 1.0 / allc["factor_solve_s"], "unit": METRIC},
+            "reference_default_threads": {"value": 1.0 / dflt["step_s"], "unit": METRIC,
+                                          "factor_solve_only": 1.0 / dflt["factor_solve_s"],
+                                          "threads": "reference default (solver.cpp:366-390)"},
+            "reference_selected_mode": allc["mode"],
+            "residual_inf_max": allc["residual_inf_max"],
+            "port": {"value": 1.0 / port_s, "unit": METRIC, "cores": 1, "kind": "port",
+                     "sample": "the oracle's C restatement (bdlu_oracle.c, reference dense micro-kernel on every "
+                               "merged block, reverse block solve) under the oracle's BTF: one factor + solve, "
+                               "%.1f s, residual %.1e%s" % (port_s, port_res, "" if port_ok else ", FAILED")},
+            "host": {"cores": cores, "cpu_model": model},
             "e2e": {"value": 1.0 / t, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -773,7 +872,7 @@ def main():
                                    "(MEASURED_PEAKS.json has no FP64 figure)"}
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_port(g)
+        cpu = cpu_baseline_reference(oracle_circuit_system())
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",

@@ -130,6 +130,7 @@ def load_library(path=LIB_PATH):
         "bdlu_server_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
         "bdlu_server_reset_stats": (ctypes.c_int, [vp]),
         "bdlu_server_last_error": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_int64]),
+        "bdlu_server_set_option": (ctypes.c_int, [vp, ctypes.c_char_p, ctypes.c_double]),
         "bdlu_synth_create": (vp, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
         "bdlu_synth_destroy": (None, [vp]),
         "bdlu_synth_n": (ctypes.c_int32, [vp]),
@@ -480,6 +481,10 @@ class Server:
         st = ServerStats()
         self._lib.bdlu_server_get_stats(self._s, ctypes.byref(st))
         return st.as_dict()
+
+    def set_option(self, key, value):
+        """Server-wide option for every pattern ("precision": 0, 1 or 2)."""
+        return self._lib.bdlu_server_set_option(self._s, key.encode(), float(value)) == 0
 
     def reset_stats(self):
         self._lib.bdlu_server_reset_stats(self._s)

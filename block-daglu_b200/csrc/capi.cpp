@@ -80,6 +80,7 @@ int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
   h->engine->set_refactor_schedule(h->refactor_schedule);
+  h->engine->set_wait_limit(h->wait_limit);
   for (int attempt = 0; attempt < 2; ++attempt) {
     const bool r = reuse && attempt == 0;
     if (!h->engine->factor_async(h->engine->values_buffer(), stream, err, r))
@@ -458,6 +459,7 @@ int bdlu_refactor_solve(bdlu_solver* h, const double* vals, int64_t nnz, double*
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
   h->engine->set_refactor_schedule(h->refactor_schedule);
+  h->engine->set_wait_limit(h->wait_limit);
   if (!h->engine->factor_async(h->engine->values_buffer(), nullptr, err, h->reuse_pivots))
     return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
   h->factored = true;
@@ -550,17 +552,27 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
     if (h->engine) h->engine->set_refactor_schedule(h->refactor_schedule);
     return BDLU_OK;
   }
+  if (k == "wait_limit") {
+    // Polls a bounded wait between tiles makes before the solve (or the tile
+    // graph refactor) gives up with an error status; 0 restores the default
+    // (about half a second).  Shorter limits exist to exercise that error
+    // path on purpose.
+    if (value < 0.0 || value > 2147483647.0) return BDLU_INVALID_DIMENSION;
+    h->wait_limit = static_cast<int32_t>(value);
+    if (h->engine) h->engine->set_wait_limit(h->wait_limit);
+    return BDLU_OK;
+  }
   if (k == "analysis_only") {
     h->analysis_only = value != 0.0;
     return BDLU_OK;
   }
   if (k == "precision") {
     // 0: FP64 throughout; 1: mixed (tensor-core trailing updates of large
-    // blocks, FP64 refinement, ladder TF32 -> 3xTF32 -> FP64).  Takes effect
-    // at the next factor; switching restarts the ladder at TF32.
-    if (value != 0.0 && value != 1.0) return BDLU_INVALID_DIMENSION;
-    h->mixed = value == 1.0;
-    h->prec_level = 1;
+    // blocks, FP64 refinement, ladder TF32 -> 3xTF32 -> FP64); 2: mixed with
+    // the ladder starting at 3xTF32.  Takes effect at the next factor.
+    if (value != 0.0 && value != 1.0 && value != 2.0) return BDLU_INVALID_DIMENSION;
+    h->mixed = value != 0.0;
+    h->prec_level = value == 2.0 ? 2 : 1;
     return BDLU_OK;
   }
   return BDLU_INVALID_DIMENSION;

@@ -39,6 +39,7 @@ struct bdlu_solver {
   bool mixed = false;         // "precision" = 1: tensor-core updates + FP64 refinement
   int32_t prec_level = 1;     // mixed route's current level: 1 TF32, 2 3xTF32, 0 FP64 (sticky)
   int32_t refactor_schedule = 0;  // 0 step chain, 1 tile task graph (Engine::set_refactor_schedule)
+  int32_t wait_limit = 0;         // polls of a bounded wait between tiles (0: default; Engine::set_wait_limit)
   // Error state (solver.h:122-123).
   int last_error = BDLU_OK;
   std::string last_message;

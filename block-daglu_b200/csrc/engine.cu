@@ -19,6 +19,7 @@
 #include "engine.h"
 
 #include "device_util.cuh"
+#include "tc_update.cuh"
 #include "large.h"
 
 #include <cuda_runtime.h>
@@ -50,6 +51,17 @@ __global__ void k_gather(DevPlan dp, const double* __restrict__ vals, int64_t nc
 }
 
 __global__ void k_set_i32(int32_t* p, int32_t v) { *p = v; }
+
+// Start of a solve: the right-hand-side count for the captured sweep, and a
+// solve-wait failure left by the previous solve cleared (factor failures
+// stay until the next factor).
+__global__ void k_solve_begin(int32_t* nrhs_word, int32_t nrhs, int32_t* status) {
+  *nrhs_word = nrhs;
+  if (status[0] == kFailSync) {
+    status[0] = 0;
+    status[1] = 0;
+  }
+}
 
 // ---------------------------------------------------------------------------
 // Dense LU of one unit in shared memory (column-major, leading dimension m).
@@ -576,6 +588,7 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   d.n = plan.n;
   d.nunits = plan.nunits;
   d.nnz = plan.nnz;
+  d.wait_limit = kWaitLimitDefault;
   if (!upload_vec(allocs_, dec.P, &d.P, err)) return false;
   if (!upload_vec(allocs_, dec.Q, &d.Q, err)) return false;
   if (!upload_vec(allocs_, plan.ustart, &d.ustart, err)) return false;
@@ -760,6 +773,10 @@ int Engine::factor_status(cudaStream_t stream, std::string& err) {
     err = "reused pivot order met a zero pivot in diagonal block " + std::to_string(st[1]);
     return 2;
   }
+  if (st[0] == kFailTensorSync) {
+    err = "tensor-core update: a bounded wait for the tensor cores ran out";
+    return -1;
+  }
   if (st[0] == kFailRefactorSync) {
     // Only the tile-graph refactor (stored pivot order) sets this; the
     // caller redoes the factor with pivoting, which does not use it.
@@ -871,7 +888,7 @@ bool Engine::solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_
   // The sweep's kernels read the right-hand-side count from d_nrhs_, so one
   // graph per tile-kernel width (up to 8 and up to 16 right-hand sides per
   // pass), captured on the current work buffers, serves every count.
-  k_set_i32<<<1, 1, 0, stream>>>(d_nrhs_, nrhs);
+  k_solve_begin<<<1, 1, 0, stream>>>(d_nrhs_, nrhs, d_status_);
   const int wide = nrhs > 8 ? 1 : 0;
   if (solve_exec_b0_ != d_b0_) {
     for (auto& ge : solve_exec_)

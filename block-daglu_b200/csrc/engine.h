@@ -45,7 +45,14 @@ struct DevPlan {
   double* sdiag;
   double* cpl_val;
   int32_t* status;  // [0] failure code (0 = ok), [1] failing unit
+  // Polls a bounded wait between tiles makes before it gives up (solve
+  // sweeps of large units, tile-graph refactor): kWaitLimitDefault, or a
+  // shorter limit set through the "wait_limit" option to make waits run out
+  // on purpose in tests.
+  int32_t wait_limit;
 };
+
+constexpr int32_t kWaitLimitDefault = 1 << 22;  // ~0.5 s with the poll back-off
 
 struct SolveResidual {
   double resid_inf;   // |b - Ax|_inf
@@ -97,6 +104,14 @@ class Engine {
   // chain (panel and update launches on two graph branches), 1 one
   // persistent kernel over the tile task graph (when the plan has one).
   void set_refactor_schedule(int32_t s) { schedule_ = s; }
+  // Bound of the waits between tiles (polls; <= 0 restores the default).
+  // Captured graphs hold the old bound, so they are dropped.
+  void set_wait_limit(int32_t polls) {
+    const int32_t v = polls > 0 ? polls : kWaitLimitDefault;
+    if (v == dp_.wait_limit) return;
+    dp_.wait_limit = v;
+    drop_graphs();
+  }
   // Residual norms of the last solve (synchronises the stream), worst column.
   bool last_residual(cudaStream_t stream, SolveResidual& out, std::string& err);
 

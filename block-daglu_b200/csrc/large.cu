@@ -44,6 +44,7 @@
 
 #include "device_util.cuh"
 #include "large.h"
+#include "tc_update.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -461,7 +462,6 @@ __global__ void k_scatter_large_perm(DevPlan dp, const double* __restrict__ vals
 // Right-hand sides per pass: kernels exist for 8 and 16 (the 16-wide one
 // reads each factor block once for up to 16 right-hand sides; the 8-wide one
 // keeps fewer registers and a shorter tile chain for few right-hand sides).
-constexpr int kSpinLimit = 1 << 22;       // polls of a flag (~0.5 s with the back-off)
 constexpr int32_t kAbortFlag = 1 << 30;
 constexpr int kTLoads = kTile * kTile / kSolveThreads;  // block entries each thread stages
 template <int kRC>
@@ -469,8 +469,9 @@ constexpr size_t trsv_smem() {
   return (static_cast<size_t>(kTile) * kTS + 2 * static_cast<size_t>(kTile) * kRC) * sizeof(double);
 }
 
-__device__ __forceinline__ bool wait_ready(const int32_t* f, int32_t need) {
-  for (int it = 0; it < kSpinLimit; ++it) {
+// Waits until *f >= need, at most `limit` polls (DevPlan::wait_limit).
+__device__ __forceinline__ bool wait_ready(const int32_t* f, int32_t need, int32_t limit) {
+  for (int it = 0; it < limit; ++it) {
     const int32_t v = *reinterpret_cast<const volatile int32_t*>(f);
     if (v >= need) {
       __threadfence();
@@ -581,7 +582,7 @@ __global__ void __launch_bounds__(kSolveThreads, 2) k_trsv_tiles(DevPlan dp, con
       } else {
         load_block(LU, m, t0, w, t0, w, tid, nxt);
       }
-      if (tid == 0) s_ok = wait_ready(rdy + J, need) ? 1 : 0;
+      if (tid == 0) s_ok = wait_ready(rdy + J, need, dp.wait_limit) ? 1 : 0;
       __syncthreads();
       if (!s_ok) {
         ok = false;
@@ -1068,7 +1069,7 @@ __global__ void __launch_bounds__(kRThreads, 2) k_rdag(DevPlan dp, const int4* _
     int32_t* kk = ver + k * nt + k;
     if (i == k && j == k) {
       // D(k): factor tile (k, k) in place.
-      if (tid == 0) s_ok = wait_ready(kk, k);
+      if (tid == 0) s_ok = wait_ready(kk, k, dp.wait_limit);
       __syncthreads();
       if (s_ok) {
         double* D = gsm;
@@ -1093,7 +1094,7 @@ __global__ void __launch_bounds__(kRThreads, 2) k_rdag(DevPlan dp, const int4* _
       const bool rowc = j == k;
       const int o = rowc ? i : j;
       int32_t* out = rowc ? ver + i * nt + k : ver + k * nt + j;
-      if (tid == 0) s_ok = wait_ready(kk, k + 1) && wait_ready(out, k);
+      if (tid == 0) s_ok = wait_ready(kk, k + 1, dp.wait_limit) && wait_ready(out, k, dp.wait_limit);
       __syncthreads();
       if (s_ok) {
         double* D = gsm;                   // kRP x kRS
@@ -1120,8 +1121,10 @@ __global__ void __launch_bounds__(kRThreads, 2) k_rdag(DevPlan dp, const int4* _
       int32_t* c0 = ver + i * nt + j;
       int32_t* c1 = two ? c0 + nt : c0;
       if (tid == 0) {
-        bool ok = wait_ready(ver + i * nt + k, k + 1) && wait_ready(ver + k * nt + j, k + 1) && wait_ready(c0, k);
-        if (two) ok = ok && wait_ready(ver + (i + 1) * nt + k, k + 1) && wait_ready(c1, k);
+        const int32_t lim = dp.wait_limit;
+        bool ok = wait_ready(ver + i * nt + k, k + 1, lim) && wait_ready(ver + k * nt + j, k + 1, lim) &&
+                  wait_ready(c0, k, lim);
+        if (two) ok = ok && wait_ready(ver + (i + 1) * nt + k, k + 1, lim) && wait_ready(c1, k, lim);
         s_ok = ok;
       }
       __syncthreads();
@@ -1144,139 +1147,29 @@ __global__ void __launch_bounds__(kRThreads, 2) k_rdag(DevPlan dp, const int4* _
 }
 
 // ---------------------------------------------------------------------------
-// Tensor-core trailing updates for the mixed-precision route: a 128 x 64 tile
-// C -= L U with TF32 operands and FP32 accumulation (mma.sync m16n8k8), the
-// operands rounded from the FP64 storage while staged in shared memory.  With
-// split3, each operand is split a = hi + lo (both TF32, lo = tf32(a - hi)) and
+// Tensor-core trailing updates for the mixed-precision route (tc_update.cuh):
+// tcgen05.mma kind::tf32 with the accumulator in tensor memory, operands
+// rounded to TF32 from the FP64 storage while staged in shared memory.  With
+// split3 each operand is split a = hi + lo (both TF32, lo = tf32(a - hi)) and
 // C -= hi hi + hi lo + lo hi ("3xTF32", a published way to reach about FP32
-// accuracy on TF32 units).  The panels, pivot search and storage stay FP64;
-// FP64 iterative refinement on the host side recovers the accuracy.
-// 256 threads: 8 warps in a 4 x 2 grid of 32 x 32 warp tiles (2 x 4 mma tiles).
-constexpr int kTM = 128;
-constexpr int kTN = 64;
-constexpr int kTBS = kTN + 8;  // B stage row stride (words): conflict-free fragment loads
-
-template <int K>
-constexpr int tf32_smem_words() {
-  return 2 * (kTM * (K + 4) + K * kTBS);
+// accuracy on TF32 units).  Panels, pivot search and storage stay FP64; FP64
+// iterative refinement recovers the accuracy.  A CTA allocates its
+// accumulator columns only once it knows it has a tile, and frees them on
+// every path out.
+__device__ __forceinline__ uint8_t* tc_align(uint8_t* p) {
+  return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~static_cast<uintptr_t>(1023));
 }
 
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
+constexpr size_t kRTcSmem = tc_smem_bytes<kRP, kRTileN>();
+constexpr size_t kGTcSmem = tc_smem_bytes<kPanel, kGT>();
+static_assert(kRTileM == kTcM && kGT == kTcM && kRThreads == kTcThreads, "tile shapes of the tensor-core update");
 
-__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// C = A[i0 : i0+128, j0 : j0+64] -= A[i0 :, k0 : k0+kk] * A[k0 : k0+kk, j0 :]
-// on a row-major m x m block (kk <= K; rows/columns past m are skipped).
-template <int K>
-__device__ void tile_update_tf32(double* A, int m, int i0, int j0, int k0, int kk, bool split3, uint32_t* sm) {
-  constexpr int kAS = K + 4;  // A stage row stride (words)
-  uint32_t* Ah = sm;
-  uint32_t* Bh = Ah + kTM * kAS;
-  uint32_t* Al = Bh + K * kTBS;
-  uint32_t* Bl = Al + kTM * kAS;
-  const int tid = threadIdx.x;
-  for (int e = tid; e < kTM * K; e += blockDim.x) {
-    const int r = e / K, q = e - r * K;
-    const double v = (i0 + r < m && q < kk) ? A[static_cast<size_t>(i0 + r) * m + k0 + q] : 0.0;
-    const float f = static_cast<float>(v);
-    const uint32_t h = to_tf32(f);
-    Ah[r * kAS + q] = h;
-    if (split3) Al[r * kAS + q] = to_tf32(f - __uint_as_float(h));
-  }
-  for (int e = tid; e < K * kTN; e += blockDim.x) {
-    const int q = e / kTN, c = e - q * kTN;
-    const double v = (q < kk && j0 + c < m) ? A[static_cast<size_t>(k0 + q) * m + j0 + c] : 0.0;
-    const float f = static_cast<float>(v);
-    const uint32_t h = to_tf32(f);
-    Bh[q * kTBS + c] = h;
-    if (split3) Bl[q * kTBS + c] = to_tf32(f - __uint_as_float(h));
-  }
-  __syncthreads();
-  const int lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
-  const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
-  float acc[2][4][4];
-#pragma unroll
-  for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-    for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-      for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0f;
-#pragma unroll 2
-  for (int ks = 0; ks < K; ks += 8) {
-    uint32_t af[2][4], bf[4][2];
-#pragma unroll
-    for (int mi = 0; mi < 2; ++mi) {
-      const int r = wm + mi * 16 + g;
-      af[mi][0] = Ah[r * kAS + ks + t4];
-      af[mi][1] = Ah[(r + 8) * kAS + ks + t4];
-      af[mi][2] = Ah[r * kAS + ks + t4 + 4];
-      af[mi][3] = Ah[(r + 8) * kAS + ks + t4 + 4];
-    }
-#pragma unroll
-    for (int ni = 0; ni < 4; ++ni) {
-      const int c = wn + ni * 8 + g;
-      bf[ni][0] = Bh[(ks + t4) * kTBS + c];
-      bf[ni][1] = Bh[(ks + t4 + 4) * kTBS + c];
-    }
-#pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) mma_tf32(acc[mi][ni], af[mi], bf[ni]);
-    if (split3) {
-      uint32_t al[2][4], bl[4][2];
-#pragma unroll
-      for (int mi = 0; mi < 2; ++mi) {
-        const int r = wm + mi * 16 + g;
-        al[mi][0] = Al[r * kAS + ks + t4];
-        al[mi][1] = Al[(r + 8) * kAS + ks + t4];
-        al[mi][2] = Al[r * kAS + ks + t4 + 4];
-        al[mi][3] = Al[(r + 8) * kAS + ks + t4 + 4];
-      }
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
-        const int c = wn + ni * 8 + g;
-        bl[ni][0] = Bl[(ks + t4) * kTBS + c];
-        bl[ni][1] = Bl[(ks + t4 + 4) * kTBS + c];
-      }
-#pragma unroll
-      for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni) {
-          mma_tf32(acc[mi][ni], af[mi], bl[ni]);
-          mma_tf32(acc[mi][ni], al[mi], bf[ni]);
-        }
-    }
-  }
-  // acc[mi][ni][2h + b]: row wm + 16mi + g + 8h, column wn + 8ni + 2t4 + b.
-#pragma unroll
-  for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int r = i0 + wm + mi * 16 + g + 8 * h;
-      if (r >= m) continue;
-      double* row = A + static_cast<size_t>(r) * m;
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
-        const int c = j0 + wn + ni * 8 + 2 * t4;
-        if (c < m) row[c] -= static_cast<double>(acc[mi][ni][2 * h]);
-        if (c + 1 < m) row[c + 1] -= static_cast<double>(acc[mi][ni][2 * h + 1]);
-      }
-    }
-}
-
-// Value-only refactor update (k_rgemm's tiles) on tensor cores.
-__global__ void __launch_bounds__(kRThreads) k_rgemm_tf32(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
-                                                          int32_t part, int32_t split3) {
-  extern __shared__ uint32_t tsm[];
+// Value-only refactor update (k_rgemm's 128 x 64 tiles, K = 64).
+__global__ void __launch_bounds__(kTcThreads) k_rgemm_tc(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
+                                                         int32_t part, int32_t split3) {
+  extern __shared__ uint8_t tc_dyn_r[];
+  __shared__ uint32_t s_tmem;
+  __shared__ __align__(8) uint64_t s_bar;
   const int32_t* pref = part ? dp.rstep_gb_pref : dp.rstep_ga_pref;
   int a = 0;
   while (a + 1 < nact && pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
@@ -1290,7 +1183,7 @@ __global__ void __launch_bounds__(kRThreads) k_rgemm_tf32(DevPlan dp, int32_t k0
   const int ntj = (rest + kRTileN - 1) / kRTileN;
   if (part == 0 && t == 0) {
     place_diag(dp, dp.lu + dp.lu_off[u], m, k0, nb, a);
-    if (rest <= 0) return;
+    if (rest <= 0) return;  // no tile: nothing allocated yet
   }
   int ti, tj;
   if (part == 0) {
@@ -1305,14 +1198,20 @@ __global__ void __launch_bounds__(kRThreads) k_rgemm_tf32(DevPlan dp, int32_t k0
     ti = 1 + t / (ntj - 1);
     tj = 1 + t % (ntj - 1);
   }
-  tile_update_tf32<kRP>(dp.lu + dp.lu_off[u], m, base + ti * kRTileM, base + tj * kRTileN, k0, nb, split3 != 0, tsm);
+  const uint32_t tmem = tc_tmem_alloc<kRTileN>(&s_tmem, &s_bar);
+  uint32_t parity = 0;
+  const bool ok = tile_update_tc<kRP, kRTileN>(dp.lu + dp.lu_off[u], m, base + ti * kRTileM, base + tj * kRTileN, k0,
+                                               nb, split3 != 0, tc_align(tc_dyn_r), tmem, &s_bar, parity);
+  if (!ok && threadIdx.x == 0) atomicCAS(dp.status, 0, kFailTensorSync);
+  tc_tmem_free<kRTileN>(tmem);
 }
 
-// First-factor update (k_gemm_rm's 128 x 128 tiles, panel depth kPanel) on
-// tensor cores: two 128 x 64 halves.
-__global__ void __launch_bounds__(kRThreads) k_gemm_rm_tf32(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
-                                                            int32_t split3) {
-  extern __shared__ uint32_t tsm[];
+// First-factor update (k_gemm_rm's 128 x 128 tiles, K = kPanel).
+__global__ void __launch_bounds__(kTcThreads) k_gemm_rm_tc(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
+                                                           int32_t split3) {
+  extern __shared__ uint8_t tc_dyn_g[];
+  __shared__ uint32_t s_tmem;
+  __shared__ __align__(8) uint64_t s_bar;
   int a = 0;
   while (a + 1 < nact && dp.step_gemm_pref[ubase + a + 1] <= static_cast<int>(blockIdx.x)) ++a;
   const int u = dp.step_unit[ubase + a];
@@ -1324,10 +1223,12 @@ __global__ void __launch_bounds__(kRThreads) k_gemm_rm_tf32(DevPlan dp, int32_t 
   const int rest = m - base;
   const int nt = (rest + kGT - 1) / kGT;
   const int ti = tile % nt, tj = tile / nt;
-  double* A = dp.lu + dp.lu_off[u];
-  tile_update_tf32<kPanel>(A, m, base + ti * kGT, base + tj * kGT, k0, nb, split3 != 0, tsm);
-  __syncthreads();
-  tile_update_tf32<kPanel>(A, m, base + ti * kGT, base + tj * kGT + kTN, k0, nb, split3 != 0, tsm);
+  const uint32_t tmem = tc_tmem_alloc<kGT>(&s_tmem, &s_bar);
+  uint32_t parity = 0;
+  const bool ok = tile_update_tc<kPanel, kGT>(dp.lu + dp.lu_off[u], m, base + ti * kGT, base + tj * kGT, k0, nb,
+                                              split3 != 0, tc_align(tc_dyn_g), tmem, &s_bar, parity);
+  if (!ok && threadIdx.x == 0) atomicCAS(dp.status, 0, kFailTensorSync);
+  tc_tmem_free<kGT>(tmem);
 }
 
 int cluster_size_for(int rows) {
@@ -1364,11 +1265,9 @@ cudaError_t large_setup() {
       err = cudaFuncSetAttribute(k_trsv_tiles<false, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(trsv_smem<8>()));
     if (err == cudaSuccess)
-      err = cudaFuncSetAttribute(k_rgemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 tf32_smem_words<kRP>() * 4);
+      err = cudaFuncSetAttribute(k_rgemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kRTcSmem));
     if (err == cudaSuccess)
-      err = cudaFuncSetAttribute(k_gemm_rm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 tf32_smem_words<kPanel>() * 4);
+      err = cudaFuncSetAttribute(k_gemm_rm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kGTcSmem));
     if (err == cudaSuccess)
       err = cudaFuncSetAttribute(k_large_perm, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 4 * 1024);
   });
@@ -1410,8 +1309,8 @@ cudaError_t large_factor(const DevPlan& dp, const Plan& p, const int32_t* d_larg
     *launches += 2;
     if (p.step_gemm_total[static_cast<size_t>(st)] > 0) {
       if (prec > 0)
-        k_gemm_rm_tf32<<<p.step_gemm_total[static_cast<size_t>(st)], kRThreads, tf32_smem_words<kPanel>() * 4, stream>>>(
-            dp, k0, ub, na, prec == 2);
+        k_gemm_rm_tc<<<p.step_gemm_total[static_cast<size_t>(st)], kTcThreads, kGTcSmem, stream>>>(dp, k0, ub, na,
+                                                                                                  prec == 2);
       else
         k_gemm_rm<<<p.step_gemm_total[static_cast<size_t>(st)], kGThreads, kGemmSmem, stream>>>(dp, k0, ub, na);
       ++*launches;
@@ -1456,15 +1355,14 @@ cudaError_t large_refactor(const DevPlan& dp, const Plan& p, cudaStream_t sa, cu
     if ((e = cudaEventRecord(ev_a, sa)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(sb, ev_a, 0)) != cudaSuccess) return e;
     const int32_t gb = p.rstep_gb_total[static_cast<size_t>(st)];
-    constexpr size_t kTfSmem = tf32_smem_words<kRP>() * 4;
     if (gb > 0) {
-      if (prec > 0) k_rgemm_tf32<<<gb, kRThreads, kTfSmem, sb>>>(dp, k0, ub, na, 1, prec == 2);
+      if (prec > 0) k_rgemm_tc<<<gb, kTcThreads, kRTcSmem, sb>>>(dp, k0, ub, na, 1, prec == 2);
       else k_rgemm<<<gb, kRThreads, kRGemmSmem, sb>>>(dp, k0, ub, na, 1);
       ++*launches;
     }
     const int32_t ga = p.rstep_ga_total[static_cast<size_t>(st)];
     if (ga > 0) {
-      if (prec > 0) k_rgemm_tf32<<<ga, kRThreads, kTfSmem, sa>>>(dp, k0, ub, na, 0, prec == 2);
+      if (prec > 0) k_rgemm_tc<<<ga, kTcThreads, kRTcSmem, sa>>>(dp, k0, ub, na, 0, prec == 2);
       else k_rgemm<<<ga, kRThreads, kRGemmSmem, sa>>>(dp, k0, ub, na, 0);
       ++*launches;
     }

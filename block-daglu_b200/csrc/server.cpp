@@ -81,6 +81,7 @@ struct bdlu_server {
   int64_t completed = 0, failed = 0;
   std::string last_message;
   int last_error = BDLU_OK;
+  double precision = 0.0;  // "precision" option of every pattern's handle
 };
 
 namespace {
@@ -281,6 +282,10 @@ int32_t bdlu_server_add_pattern(bdlu_server* s, const int32_t* rows, const int32
   if (st == BDLU_OK) st = bdlu_set_option(p->h, "analysis_only", 1);
   if (st == BDLU_OK) st = bdlu_analyze(p->h);
   if (st == BDLU_OK) st = bdlu_set_option(p->h, "analysis_only", 0);
+  if (st == BDLU_OK) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    st = bdlu_set_option(p->h, "precision", s->precision);
+  }
   if (st != BDLU_OK) {
     char buf[512];
     bdlu_last_error(p->h, buf, sizeof(buf));
@@ -389,6 +394,19 @@ int bdlu_server_reset_stats(bdlu_server* s) {
   s->t_last = 0.0;
   s->peak_running = s->running;
   s->evictions = 0;
+  return BDLU_OK;
+}
+
+int bdlu_server_set_option(bdlu_server* s, const char* key, double value) {
+  if (!s || !key) return BDLU_NOT_PREPARED;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->queue.empty() || s->running > 0) return sfail(s, BDLU_NOT_PREPARED, "requests are queued or running");
+  const std::string k(key);
+  if (k != "precision" || (value != 0.0 && value != 1.0 && value != 2.0))
+    return sfail(s, BDLU_INVALID_DIMENSION, "unknown server option or value");
+  for (auto& p : s->patterns)
+    if (const int st = bdlu_set_option(p->h, "precision", value)) return sfail(s, st, "precision option refused");
+  s->precision = value;
   return BDLU_OK;
 }
 

@@ -263,6 +263,11 @@ int bdlu_server_drain(bdlu_server* s);
 int bdlu_server_get_stats(bdlu_server* s, bdlu_server_stats* out);
 int bdlu_server_reset_stats(bdlu_server* s);
 int bdlu_server_last_error(const bdlu_server* s, char* buf, int64_t len);
+/* Server-wide option, applied to every pattern (present and added later)
+ * with bdlu_set_option's meaning: "precision" (0 FP64, 1 mixed with FP64
+ * refinement, 2 mixed starting at 3xTF32).  Only while no request is queued
+ * or running (else BDLU_NOT_PREPARED). */
+int bdlu_server_set_option(bdlu_server* s, const char* key, double value);
 
 /* ---- Dense batch solve without allocation -----------------------------------
  * No counterpart in the reference.  For callers that must not allocate

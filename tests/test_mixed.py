@@ -30,8 +30,35 @@ def _solver(g, mixed):
 
 def test_precision_option_values():
     s = bd.Solver()
-    assert s.set_option("precision", 0) and s.set_option("precision", 1)
-    assert not s.set_option("precision", 2)
+    assert s.set_option("precision", 0) and s.set_option("precision", 1) and s.set_option("precision", 2)
+    assert not s.set_option("precision", 3)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("level,tol,agree", [(2, 1e-5, 1000), (1, 3e-2, 100)])
+def test_tensor_core_update_matches_fp64_factors(cuda_device, monkeypatch, level, tol, agree):
+    """The tcgen05 trailing update against the FP64 update on the same unit:
+    MODE=klu makes one 1,200-row unit whose first factor runs 37 panel steps
+    of tensor-core updates.  Where both factorisations chose the same pivots
+    (a diagonally weighted block: nearly all of them), the factors agree to
+    the accuracy of the tensor-core arithmetic: 3xTF32 (level 2) to about
+    FP32 rounding, TF32 (level 1) to about TF32 rounding.  A wrong operand
+    layout or descriptor would put O(1) errors into every updated entry."""
+    monkeypatch.setenv("BLOCKDAGLU_MODE", "klu")
+    g = bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(0, 35), 1200, 24)
+    lus = []
+    for prec in (0, level):
+        s = bd.Solver()
+        assert s.set_option("precision", prec)
+        assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze() and s.factor(), s.last_error_message()
+        assert s.stats()["max_unit"] == 1200
+        lus.append(s.block_lu(0))
+    (lu64, piv64), (lumx, pivmx) = lus
+    same = np.flatnonzero(np.cumprod(piv64 == pivmx))  # columns before the first pivot difference
+    assert len(same) > agree, len(same)
+    k = len(same)
+    scale = np.max(np.abs(lu64))
+    assert np.max(np.abs(lu64[:k, :k] - lumx[:k, :k])) <= tol * scale
 
 
 @pytest.mark.gpu
