@@ -56,7 +56,7 @@ sys.path[:0] = [os.path.join(ROOT, "block-daglu_b200")]
 
 import numpy as np  # noqa: E402
 
-WORKLOAD = "circuit-200k"
+CIRCUIT_WORKLOAD = "circuit-200k"
 METRIC = "refactor+solves/s"
 N_ROWS = 200000
 CONFIG_INDEX = 1
@@ -65,8 +65,10 @@ BATCH_WORKLOAD = "batch-256"
 BATCH_METRIC = "system factor+solves/s"
 BATCH_SYSTEMS, BATCH_NRHS, BATCH_CONFIG = 256, 8, 2
 SERVE_WORKLOAD = "serve-64"
+WORKLOAD = SERVE_WORKLOAD  # the default: served vs plain FP64 GPU throughput and latency
 SERVE_METRIC = "refactor+solves/s"
 SERVE_PATTERNS, SERVE_CONFIG, SERVE_BUDGET = 64, 4, 150 << 30
+REF_SERVE_MAX_BLOCK = 4000
 PREC_WORKLOAD = "precision-200"
 PREC_METRIC = "factor+16-rhs solves/s"
 PREC_BLOCKS, PREC_CONFIG, PREC_NRHS = 200, 3, 16
@@ -79,13 +81,17 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default=WORKLOAD, choices=[WORKLOAD, BATCH_WORKLOAD, SERVE_WORKLOAD, PREC_WORKLOAD])
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=[SERVE_WORKLOAD, CIRCUIT_WORKLOAD, BATCH_WORKLOAD, PREC_WORKLOAD])
     ap.add_argument("--blocks", type=int, default=PREC_BLOCKS, help="precision-200: number of large blocks")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve-64: Poisson arrival rate (requests/s)")
-    ap.add_argument("--duration", type=float, default=5.0, help="serve-64: seconds of open-loop arrivals")
-    ap.add_argument("--slots", type=int, default=8, help="serve-64: concurrent request slots")
-    ap.add_argument("--refactor-schedule", type=int, default=0, choices=[0, 1],
-                    help="circuit-200k: large-block refactor as a step chain (0) or one tile task graph (1)")
+    ap.add_argument("--duration", type=float, default=2.0, help="serve-64: seconds of open-loop arrivals")
+    ap.add_argument("--slots", type=int, default=16, help="serve-64: concurrent request slots")
+    ap.add_argument("--precision", type=int, default=0, choices=[0, 1, 2],
+                    help="serve-64: 0 FP64, 1 mixed (tensor-core updates + FP64 refinement), 2 mixed from 3xTF32")
+    ap.add_argument("--refactor-schedule", type=int, default=None, choices=[0, 1],
+                    help="circuit-200k: large-block refactor as a step chain (0) or one tile task graph (1); "
+                         "default: the autotuner's choice")
     return ap.parse_args()
 
 
@@ -216,7 +222,7 @@ def reference_route(g, steps, warm, threads, nrhs_of=None, step_inputs_fn=None):
         os.environ["USERALGO_THREADS"] = str(threads)
     else:
         os.environ.pop("USERALGO_THREADS", None)
-    os.environ.pop("USERALGO_MODE", None)
+    os.environ["USERALGO_MODE"] = "block"
     os.environ.pop("BLOCKDAGLU_MODE", None)
     s = oracle.RefSolver()
     rec, worst = [], 0.0
@@ -237,6 +243,7 @@ def reference_route(g, steps, warm, threads, nrhs_of=None, step_inputs_fn=None):
             rec.append((t1 - t0, t2 - t1, t3 - t2))
             worst = max(worst, oracle.metrics(g.rows, g.cols, v, x, b)[0])
     os.environ.pop("USERALGO_THREADS", None)
+    os.environ.pop("USERALGO_MODE", None)
     mean = [statistics.mean(r[i] for r in rec) for i in range(3)]
     return {"analyze_s": mean[0], "factor_s": mean[1], "solve_s": mean[2], "step_s": sum(mean),
             "factor_solve_s": mean[1] + mean[2], "steps": len(rec), "residual_inf_max": worst,
@@ -273,7 +280,7 @@ def cpu_baseline_reference(g):
                       "full %s system by the reference's BLOCK route built under oracle/_ref (its own solver.cpp and "
                       "ubtf_block_solver.cpp; KLU and BTF are stand-ins: SuiteSparse is unavailable on this box), "
                       "USERALGO_THREADS=%d on %s: analyze %.2f s, factor %.2f s, solve %.3f s, residual %.1e"
-                      % (WORKLOAD, cores, model, r["analyze_s"], r["factor_s"], r["solve_s"], r["residual_inf_max"])}
+                      % (CIRCUIT_WORKLOAD, cores, model, r["analyze_s"], r["factor_s"], r["solve_s"], r["residual_inf_max"])}
 
 
 def run_reference(args, rank, world):
@@ -293,7 +300,7 @@ def run_reference(args, rank, world):
     line = {"metric": METRIC, "value": 1.0 / t, "unit": METRIC, "n_gpus": args.gpus, "steps": steps,
             "warmup": warm, "ms_per_step": 1000.0 * t, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n": g.n, "nnz": int(g.nnz), "nrhs": 1},
+            "config": {"workload": CIRCUIT_WORKLOAD, "n": g.n, "nnz": int(g.nnz), "nrhs": 1},
             "impl": "reference",
             "same_steps": steps == args.steps and warm == args.warmup,
             "same_steps_reason": None if steps == args.steps else
@@ -321,14 +328,17 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def batch_systems(count=BATCH_SYSTEMS):
-    """The batch workload's systems: block generator, n log-uniform in [1e3, 5e4]."""
-    import blockdaglu as bd
-    rng = np.random.default_rng(bd.config_seed(BATCH_CONFIG))
+def batch_systems(count=BATCH_SYSTEMS, gen=None):
+    """The batch workload's systems: block generator, n log-uniform in [1e3, 5e4].
+    gen: the generator module (the engine package, or the oracle for the CPU
+    baseline and the reference arm; both draw the same systems)."""
+    if gen is None:
+        import blockdaglu as gen
+    rng = np.random.default_rng(gen.config_seed(BATCH_CONFIG))
     out = []
     for i in range(count):
         n = int(np.exp(rng.uniform(np.log(1000.0), np.log(50000.0))))
-        out.append(bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(BATCH_CONFIG, i), n))
+        out.append(gen.Synth(gen.FAMILY_BLOCK, gen.config_seed(BATCH_CONFIG, i), n))
     return out
 
 
@@ -340,30 +350,42 @@ def batch_step_inputs(systems, k):
     return vals, B
 
 
-def batch_cpu_sample(systems, sample=4):
-    """Oracle port on the first `sample` systems (factor + 8-rhs solve), scaled to systems/s."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import blockdaglu as bd
-    import oracle
-    vals, B = batch_step_inputs(systems[:sample], 0)
-    t_all, off, voff = 0.0, 0, 0
-    for g in systems[:sample]:
-        s = bd.Solver()
-        s.set_option("analysis_only", 1)
-        assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze()
-        d = s.decomposition()
-        v = vals[voff:voff + g.nnz]
-        t0 = time.perf_counter()
-        ref = oracle.System(g.n, g.rows, g.cols, v, d["P"], d["Q"], d["R"])
-        ref.factor()
-        for j in range(BATCH_NRHS):
-            ref.solve(np.ascontiguousarray(B[off:off + g.n, j]))
-        t_all += time.perf_counter() - t0
-        off += g.n
-        voff += g.nnz
-    return {"value": sample / t_all, "unit": BATCH_METRIC, "cores": 1, "kind": "port",
-            "sample": "the first %d systems of the batch (n = %s), each factored and solved for %d rhs by the "
-                      "oracle on one thread: %.2f s" % (sample, [g.n for g in systems[:sample]], BATCH_NRHS, t_all)}
+def batch_cpu_sample(sample=4):
+    """The reference's BLOCK route (oracle/_ref, all host cores) on the first
+    `sample` systems of the batch's step 0: per system set_matrix + analyze +
+    factor + one solve_in_place per right-hand side (its API is single-RHS),
+    after one untimed pass; scaled to systems/s."""
+    oracle = oracle_module()
+    cores, model = host_cpu()
+    systems = batch_systems(BATCH_SYSTEMS, oracle)[:sample]
+    vals, B = batch_step_inputs(systems, 0)
+    os.environ["USERALGO_THREADS"] = str(cores)
+    os.environ["USERALGO_MODE"] = "block"  # n < 50,000: AUTO would take the global KLU route (stand-in only)
+    t_all = 0.0
+    for rep in range(2):
+        voff = off = 0
+        t_rep = 0.0
+        for g in systems:
+            s = oracle.RefSolver()
+            v = vals[voff:voff + g.nnz]
+            t0 = time.perf_counter()
+            ok = s.set_matrix(g.rows, g.cols, v, g.n) and s.analyze() and s.factor()
+            for j in range(BATCH_NRHS):
+                x = np.ascontiguousarray(B[off:off + g.n, j])
+                ok = ok and s.solve_in_place(x)
+            t_rep += time.perf_counter() - t0
+            if not ok:
+                raise RuntimeError("reference route failed: " + s.last_error_message())
+            off += g.n
+            voff += g.nnz
+        t_all = t_rep
+    os.environ.pop("USERALGO_THREADS", None)
+    os.environ.pop("USERALGO_MODE", None)
+    return {"value": sample / t_all, "unit": BATCH_METRIC, "cores": cores, "kind": "reference",
+            "sample": "the first %d systems of the batch (n = %s), each through the reference's BLOCK route built "
+                      "under oracle/_ref (set_matrix + analyze + factor + %d single-RHS solves, USERALGO_THREADS=%d on "
+                      "%s), second of two passes: %.2f s" % (sample, [g.n for g in systems], BATCH_NRHS, cores, model,
+                                                             t_all)}
 
 
 def run_batch(args, rank, world):
@@ -371,8 +393,7 @@ def run_batch(args, rank, world):
     if args.impl == "reference":
         if rank != 0:
             return
-        systems = batch_systems()
-        base = batch_cpu_sample(systems)
+        base = batch_cpu_sample()
         line = {"metric": BATCH_METRIC, "value": base["value"], "unit": BATCH_METRIC, "n_gpus": args.gpus,
                 "steps": 1, "warmup": 0, "ms_per_step": 1000.0 * BATCH_SYSTEMS / base["value"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -508,7 +529,7 @@ def run_batch(args, rank, world):
         roofline = {"bound": "tensor", "achieved": achieved, "peak": dgemm, "unit": "TFLOP/s", "frac": achieved / dgemm,
                     "traffic": None, "kernel": "dense block LU of all systems' blocks (k_lu_small), FP64",
                     "peak_source": "FP64 pipe: torch.matmul float64 8192^3 measured in this run"}
-    cpu = batch_cpu_sample(systems) if (world == 1 and not args.no_cpu_baseline) else None
+    cpu = batch_cpu_sample() if (world == 1 and not args.no_cpu_baseline) else None
     line = {
         "metric": BATCH_METRIC, "value": value, "unit": BATCH_METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -528,11 +549,100 @@ def run_batch(args, rank, world):
         dist.destroy_process_group()
 
 
-def serve_patterns(count=SERVE_PATTERNS):
-    import blockdaglu as bd
-    rng = np.random.default_rng(bd.config_seed(SERVE_CONFIG))
+def serve_patterns(count=SERVE_PATTERNS, gen=None):
+    """The serving workload's patterns: circuit generator, n log-uniform in
+    [5e3, 3e5] (gen: engine package or oracle, same draws)."""
+    if gen is None:
+        import blockdaglu as gen
+    rng = np.random.default_rng(gen.config_seed(SERVE_CONFIG))
     sizes = [int(np.exp(rng.uniform(np.log(5000.0), np.log(300000.0)))) for _ in range(count)]
-    return [bd.Synth(bd.FAMILY_CIRCUIT, bd.config_seed(SERVE_CONFIG, i), n) for i, n in enumerate(sizes)]
+    return [gen.Synth(gen.FAMILY_CIRCUIT, gen.config_seed(SERVE_CONFIG, i), n) for i, n in enumerate(sizes)]
+
+
+def serve_reference_sample(args, budget_s):
+    """The reference serving the closed-loop request stream the way its API
+    allows: one Solver per pattern, each request set_matrix(new values) +
+    analyze + factor + one solve_in_place per right-hand side, one request at
+    a time, on all host cores (oracle/_ref).  A bounded sample: requests in
+    stream order until about `budget_s` seconds of work, skipping requests
+    whose pattern has a diagonal block above REF_SERVE_MAX_BLOCK rows (the
+    dense KLU stand-in takes minutes on those), so the sample overstates the
+    reference's throughput.  Returns the cpu_baseline dict."""
+    import scipy.sparse as sp
+    oracle = oracle_module()
+    cores, model = host_cpu()
+    patterns = serve_patterns(SERVE_PATTERNS, oracle)
+    closed = serve_requests(patterns, max(args.steps, 1) * 64, 11)
+    os.environ["USERALGO_THREADS"] = str(cores)
+    # The BLOCK route: under AUTO the reference sends n < 50,000 to its global
+    # KLU route, which the dense KLU stand-in cannot run at these sizes.
+    os.environ["USERALGO_MODE"] = "block"
+    solvers, done, skipped, t_total, worst = {}, 0, 0, 0.0, 0.0
+    max_block = {}
+    for k, v, B in closed:
+        g = patterns[k]
+        if k not in max_block:
+            a = sp.csc_matrix((np.ones(g.nnz), (g.rows, g.cols)), shape=(g.n, g.n))
+            a.sort_indices()
+            _, _, _, R, _ = oracle.btf_order(g.n, a.indptr, a.indices)
+            max_block[k] = int(np.max(np.diff(R)))
+        if max_block[k] > REF_SERVE_MAX_BLOCK:
+            skipped += 1
+            continue
+        s = solvers.setdefault(k, oracle.RefSolver())
+        t0 = time.perf_counter()
+        ok = s.set_matrix(g.rows, g.cols, v, g.n) and s.analyze() and s.factor()
+        xs = []
+        for j in range(B.shape[1]):
+            if not ok:
+                break
+            x = np.ascontiguousarray(B[:, j])
+            ok = s.solve_in_place(x)
+            xs.append(x)
+        dt = time.perf_counter() - t0
+        if not ok:
+            raise RuntimeError("reference route failed: " + s.last_error_message())
+        t_total += dt
+        done += 1
+        worst = max(worst, max(oracle.metrics(g.rows, g.cols, v, x, B[:, j])[0] for j, x in enumerate(xs)))
+        if t_total > budget_s and done >= 2:
+            break
+    os.environ.pop("USERALGO_THREADS", None)
+    os.environ.pop("USERALGO_MODE", None)
+    value = done / t_total
+    sample = ("%d requests of the closed-loop stream in order (%d skipped: their pattern has a diagonal block above "
+              "%d rows, which the dense KLU stand-in factors in minutes; the sample overstates the reference's "
+              "throughput), each set_matrix + analyze + factor + single-RHS solves through the reference's BLOCK "
+              "route built under oracle/_ref (own solver.cpp / ubtf_block_solver.cpp, KLU and BTF stand-ins; "
+              "USERALGO_MODE=block: AUTO would send n < 50,000 to the global KLU route, which the stand-in cannot "
+              "run), one Solver per pattern, one request at a time, USERALGO_THREADS=%d on %s: %.1f s, worst "
+              "residual %.1e" % (done, skipped, REF_SERVE_MAX_BLOCK, cores, model, t_total, worst))
+    return {"value": value, "unit": SERVE_METRIC, "cores": cores, "kind": "reference", "sample": sample,
+            "requests": done, "seconds": t_total, "residual_inf_max": worst}
+
+
+def run_serve_reference(args):
+    """serve-64 reference arm: the sampled request stream (about a minute) and
+    the circuit-200k value change, both through the reference build."""
+    cores, model = host_cpu()
+    base = serve_reference_sample(args, 60.0)
+    circ = reference_route(oracle_circuit_system(), 1, 1, cores)
+    value = base["value"]
+    line = {"metric": SERVE_METRIC, "value": value, "unit": SERVE_METRIC, "n_gpus": args.gpus,
+            "steps": base["requests"], "warmup": 0, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": SERVE_WORKLOAD, "patterns": SERVE_PATTERNS},
+            "impl": "reference", "same_steps": False,
+            "same_steps_reason": "a bounded sample of the request stream (about a minute of host work)",
+            "residual_inf_max": base["residual_inf_max"],
+            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "circuit_200k": {"value": 1.0 / circ["step_s"], "unit": METRIC,
+                             "factor_solve_only": 1.0 / circ["factor_solve_s"],
+                             "phases_s": {k: circ[k] for k in ("analyze_s", "factor_s", "solve_s")},
+                             "sample": "1 timed value change after 1 untimed, USERALGO_THREADS=%d" % cores},
+            "host": {"cores": cores, "cpu_model": model},
+            "e2e": {"value": value, "unit": SERVE_METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
 
 
 def serve_requests(patterns, count, seed, nvals=3):
@@ -548,47 +658,119 @@ def serve_requests(patterns, count, seed, nvals=3):
     return out
 
 
+def serve_roofline_time(st, nnz, n, nrhs, p_flops, bw):
+    """t_roof of one request: max(F / P, B / BW) with F = dense-block LU flops +
+    2 * dense entries * nrhs (solve), B = values in (8 nnz) + factor write and
+    read (8 + 8 per dense entry, the read once per 16 right-hand sides) +
+    12 * coupling entries + 32 bytes per row and right-hand side."""
+    passes = (nrhs + 15) // 16
+    F = st["factor_flops"] + 2.0 * st["dense_entries"] * nrhs
+    B = 8.0 * nnz + 8.0 * st["dense_entries"] * (1 + passes) + 12.0 * st["nnz_offdiag"] + 32.0 * n * nrhs
+    return max(F / p_flops, B / bw)
+
+
 def run_serve(args, rank, world):
-    """serve-64: open-loop and closed-loop serving vs the plain FP64 path."""
+    """serve-64: the served engine against the plain FP64 GPU path on one
+    request stream.  `value`: closed loop with device-resident requests (values
+    and right-hand sides already in HBM); `e2e`: the same stream through host
+    buffers (bdlu_server_submit); open-loop Poisson arrivals for p50 / p99;
+    the plain path runs the same requests one at a time, one Solver per
+    pattern, through bdlu_refactor_solve with host buffers."""
     import concurrent.futures as cf
-    import blockdaglu as bd
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps({"impl": "reference", "metric": SERVE_METRIC, "unavailable":
-                              "serve-64 has no CPU reference arm; the reference serves one request at a time per "
-                              "Solver (see the circuit-200k reference arm for its per-request cost)"}), flush=True)
+            run_serve_reference(args)
         return
-    if world > 1 and rank != 0:
-        return
+    import torch
+    import blockdaglu as bd
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    cores, _ = host_cpu()
     patterns = serve_patterns()
     srv = bd.Server(SERVE_BUDGET, args.slots)
+    assert srv.set_option("precision", args.precision), srv.last_error_message()
     t0 = time.perf_counter()
-    with cf.ThreadPoolExecutor(8) as ex:
+    with cf.ThreadPoolExecutor(max(1, min(8, cores))) as ex:
         ids = list(ex.map(lambda g: srv.add_pattern((g.rows, g.cols, g.vals), g.n), patterns))
     analyze_s = time.perf_counter() - t0
     assert all(i >= 0 for i in ids), srv.last_error_message()
-    order = {pid: k for k, pid in enumerate(ids)}
-    # Warm-up: two requests per pattern (upload and first factor with
-    # pivoting, then the first value-only refactor, which captures its graph).
-    warm = [(k, patterns[k].vals, np.asfortranarray(np.ones((patterns[k].n, 1))))
-            for _ in range(2) for k in range(len(patterns))]
-    for (k, v, B) in warm:
+    closed = serve_requests(patterns, max(args.steps, 1) * 64, 11)
+    # Warm-up: per pattern an upload + first factor, a refactor with 1 and
+    # with 16 right-hand sides (both solve graphs captured), and one
+    # device-resident request.
+    warm = [(k, patterns[k].vals, np.asfortranarray(np.ones((patterns[k].n, nr))))
+            for nr in (1, 1, 16) for k in range(len(patterns))]
+    for k, v, B in warm:
         srv.submit(ids[k], v, B)
     srv.drain()
-    # Closed loop: all requests queued at once (saturation throughput).
-    closed = serve_requests(patterns, max(args.steps, 1) * 64, 11)
+    # Device-resident inputs: one device copy of each value set, one device
+    # right-hand-side block per request (column-major, overwritten with X).
+    dvals = {}
+    for k, v, _ in closed:
+        if id(v) not in dvals:
+            dvals[id(v)] = torch.from_numpy(v).to(dev)
+    dB0 = [torch.from_numpy(np.ascontiguousarray(B.T)).to(dev) for _, _, B in closed]
+    wk = [(k, torch.from_numpy(patterns[k].vals).to(dev), torch.ones(1, patterns[k].n, dtype=torch.float64,
+                                                                      device=dev)) for k in range(len(patterns))]
+    for k, dv, db in wk:
+        srv.submit_device(ids[k], dv.data_ptr(), patterns[k].nnz, db.data_ptr(), patterns[k].n, 1, keep=(dv, db))
+    srv.drain()
+    del wk
+    # Closed loop, device-resident requests (value): all requests queued at
+    # once; the time runs from the first submit to the last result, between
+    # device synchronisations (the requests run on the server's worker
+    # streams, which one event pair cannot bracket).
+    dB = [b.clone() for b in dB0]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     srv.reset_stats()
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rids = [srv.submit_device(ids[k], dvals[id(v)].data_ptr(), len(v), b.data_ptr(), B.shape[0], B.shape[1])
+                for (k, v, B), b in zip(closed, dB)]
+        res = [srv.wait(r) for r in rids]
+        torch.cuda.synchronize()
+        dev_s = time.perf_counter() - t0
+    dstats = srv.stats()
+    assert all(r[0] for r in res), srv.last_error_message()
+    worst = max(r[1] for r in res)
+    # Check the device-resident solutions on the host (FP64 residual).
+    for (k, v, B), b in zip(closed[:8], dB[:8]):
+        g = patterns[k]
+        X = b.cpu().numpy().T
+        for j in range(B.shape[1]):
+            r = B[:, j].copy()
+            np.subtract.at(r, g.rows, v * X[g.cols, j])
+            arow = np.zeros(g.n)
+            np.add.at(arow, g.rows, np.abs(v))
+            worst = max(worst, float(np.max(np.abs(r)) / (arow.max() * np.max(np.abs(X[:, j])) + np.max(np.abs(B[:, j])))))
+    del dB
+    dev_s_max = max_over_ranks(dev_s, dist, dev)
+    value = world * len(closed) / dev_s_max
+    # Closed loop, host buffers (e2e): the same requests through
+    # bdlu_server_submit.
     outs = [B.copy(order="F") for _, _, B in closed]
+    srv.reset_stats()
     t0 = time.perf_counter()
     rids = [srv.submit(ids[k], v, X) for (k, v, _), X in zip(closed, outs)]
     res = [srv.wait(r) for r in rids]
-    closed_s = time.perf_counter() - t0
-    cstats = srv.stats()
+    host_s = time.perf_counter() - t0
+    hstats = srv.stats()
     assert all(r[0] for r in res), srv.last_error_message()
-    worst = max(r[1] for r in res)
-    value = len(closed) / closed_s
-    # Open loop: Poisson arrivals for --duration seconds, at --rate and at
-    # 70 % of the closed-loop throughput (a load the server can sustain).
+    worst = max(worst, max(r[1] for r in res))
+    host_s_max = max_over_ranks(host_s, dist, dev)
+    e2e = world * len(closed) / host_s_max
+
+    # Open loop: Poisson arrivals for --duration seconds at --rate, and at
+    # 70 % of the closed-loop host-buffer throughput (a load it sustains).
     def open_loop(rate, seed):
         rng = np.random.default_rng(seed)
         n_open = max(1, int(rate * args.duration))
@@ -613,52 +795,93 @@ def run_serve(args, rank, world):
                 "evictions": st["evictions"]}, max(r[1] for r in ores)
 
     open_spec, w1 = open_loop(args.rate, 17)
-    open_fit, w2 = open_loop(0.7 * value, 23)
+    open_fit, w2 = open_loop(0.7 * e2e / world, 23)
     worst = max(worst, w1, w2)
-    # Plain FP64 path: one request at a time, one Solver per pattern.
+    srv.close()
+    # Plain FP64 GPU path: one request at a time, one Solver per pattern.
     sample = closed[: min(len(closed), 192)]
     solvers = {}
-    for k in sorted({k for k, _, _ in sample}):
+    for k in sorted({k for k, _, _ in closed}):
         s = bd.Solver()
         g = patterns[k]
         assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze() and s.factor(), s.last_error_message()
         X = np.ones(g.n)
         assert s.solve_in_place(X)
+        X = np.asfortranarray(np.ones((g.n, 16)))
         assert s.refactor_values(g.vals) and s.solve_in_place(X), s.last_error_message()
         solvers[k] = s
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     for k, v, B in sample:
         X = B.copy(order="F")
         s = solvers[k]
         assert s._lib.bdlu_refactor_solve(s._h, bd._p64(v), len(v), bd._p64(X), X.shape[0], X.shape[1]) == 0, \
             s.last_error_message()
-    plain = len(sample) / (time.perf_counter() - t0)
+    plain_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    plain = world * len(sample) / plain_s
+    # Roofline of the serving loop: sum over requests of max(F/P, B/BW), the
+    # time an ideal device would need, against the wall time (value's run).
+    pstats = {k: s.stats() for k, s in solvers.items()}
     del solvers
+    peaks = measured_peaks()
+    dgemm = measured_dgemm(dev)
+    bw = peaks.get("hbm_gbs", 6650.0) * 1e9
+    t_roof = sum(serve_roofline_time(pstats[k], patterns[k].nnz, patterns[k].n, B.shape[1], dgemm * 1e12, bw)
+                 for k, _, B in closed)
+    # The plain path on the 200k-row circuit system: device-timed steps, the
+    # end-to-end call, phases and the roofline of its dominant phase.
+    circ = measure_circuit(args, world, dist, dev)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    cpu = serve_reference_sample(args, 30.0) if (world == 1 and not args.no_cpu_baseline) else None
     nrhs_mean = float(np.mean([B.shape[1] for _, _, B in closed]))
     n_mean = float(np.mean([patterns[k].n for k, _, _ in closed]))
     nnz_mean = float(np.mean([patterns[k].nnz for k, _, _ in closed]))
     line = {
-        "metric": SERVE_METRIC, "value": value, "unit": SERVE_METRIC, "n_gpus": 1, "steps": len(closed),
-        "warmup": len(warm), "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "metric": SERVE_METRIC, "value": value, "unit": SERVE_METRIC, "n_gpus": world, "steps": len(closed),
+        "warmup": len(warm) + len(patterns), "ms_per_step": 1000.0 * dev_s_max / len(closed),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == 0 else "f64 storage, tf32 tensor-core updates, f64 refinement",
+        "data": "synthetic",
         "config": {"workload": SERVE_WORKLOAD, "patterns": SERVE_PATTERNS, "slots": args.slots,
-                   "budget_bytes": SERVE_BUDGET, "rows_min_max": [min(g.n for g in patterns), max(g.n for g in patterns)],
-                   "analyze_s": analyze_s, "mode": "closed loop (all requests queued), then open loop"},
-        "e2e": {"value": value, "unit": SERVE_METRIC, "h2d_bytes_per_step": int(8 * nnz_mean + 8 * n_mean * nrhs_mean),
+                   "precision": args.precision, "budget_bytes": SERVE_BUDGET,
+                   "rows_min_max": [min(g.n for g in patterns), max(g.n for g in patterns)],
+                   "requests": len(closed), "nrhs": "U{1..16}", "analyze_s": analyze_s,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": "inputs larger than L2 (the request stream's factors and values total GBs)",
+                   "value": "closed loop, device-resident requests (bdlu_server_submit_device), first submit to "
+                            "last result between device synchronisations"},
+        "e2e": {"value": e2e, "unit": SERVE_METRIC, "h2d_bytes_per_step": int(8 * nnz_mean + 8 * n_mean * nrhs_mean),
                 "d2h_bytes_per_step": int(8 * n_mean * nrhs_mean)},
-        "served_closed_loop": {"requests": len(closed), "seconds": closed_s, "throughput": value,
-                               "p50_ms": cstats["p50_ms"], "p99_ms": cstats["p99_ms"],
-                               "peak_concurrency": cstats["peak_concurrency"]},
+        "served_device_resident": {"requests": len(closed), "seconds": dev_s, "throughput": value,
+                                   "p50_ms": dstats["p50_ms"], "p99_ms": dstats["p99_ms"],
+                                   "peak_concurrency": dstats["peak_concurrency"]},
+        "served_host_buffers": {"requests": len(closed), "seconds": host_s, "throughput": e2e,
+                                "p50_ms": hstats["p50_ms"], "p99_ms": hstats["p99_ms"],
+                                "peak_concurrency": hstats["peak_concurrency"]},
         "served_open_loop": open_spec,
         "served_open_loop_sustainable": open_fit,
-        "plain_fp64_path": {"requests": len(sample), "throughput": plain, "ratio_served_over_plain": value / plain},
+        "plain_fp64_path": {"requests": len(sample), "throughput": plain, "host_buffers": True},
+        "ratio_served_over_plain": e2e / plain,
+        "ratio_served_device_resident_over_plain": value / plain,
+        "serving_roofline": {"sum_t_roof_s": t_roof, "wall_s": dev_s, "frac": t_roof / dev_s,
+                             "peaks": {"fp64_tflops": dgemm, "hbm_gbs": bw / 1e9},
+                             "formula": "t_roof(req) = max(F/P_fp64, B/BW) summed over the closed-loop requests"},
+        "plain_circuit_200k": {"value": circ["value"], "e2e": circ["e2e"], "ms_per_step": circ["ms_per_step"],
+                               "phases_ms": circ["phases_ms"], "residual_inf_max": circ["residual_inf_max"],
+                               "gpu_launches": circ["gpu_launches"], "unit": METRIC},
         "residual_inf_max": worst,
-        "roofline": None,
-        "cpu_baseline": None,
-        "gpu_launches": None,
+        "roofline": dict(circ["roofline"], workload=CIRCUIT_WORKLOAD + " plain FP64 path (measured in this run)"),
+        "cpu_baseline": cpu,
+        "clocks": clocks.summary(),
+        "gpu_launches": int(dstats["kernel_launches"]),
+        "tuner": circ["tuner"],
     }
-    srv.close()
     print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
 
 
 def run_precision(args, rank, world):
@@ -727,36 +950,18 @@ def run_precision(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def main():
-    args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.workload == BATCH_WORKLOAD:
-        run_batch(args, rank, world)
-        return
-    if args.workload == SERVE_WORKLOAD:
-        run_serve(args, rank, world)
-        return
-    if args.workload == PREC_WORKLOAD:
-        run_precision(args, rank, world)
-        return
-    if args.impl == "reference":
-        run_reference(args, rank, world)
-        return
+def measure_circuit(args, world, dist, dev):
+    """circuit-200k on this rank: device-timed value-only refactor + 1-RHS solve
+    steps (inputs resident in HBM, L2 flushed between steps), the same steps
+    end to end through bdlu_refactor_solve with pinned host buffers, phase
+    times and the roofline of the dominant phase.  Returns a dict."""
     import torch
     import blockdaglu as bd
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream(dev)
     g = circuit_system()
     s = bd.Solver()
-    assert s.set_option("refactor_schedule", args.refactor_schedule)
+    if args.refactor_schedule is not None:
+        assert s.set_option("refactor_schedule", args.refactor_schedule)
     assert s.set_matrix((g.rows, g.cols, g.vals), g.n), s.last_error_message()
     t0 = time.perf_counter()
     assert s.analyze(), s.last_error_message()
@@ -776,7 +981,12 @@ def main():
         assert s.refactor_values_device(d_vals[k].data_ptr(), nnz, sh), s.last_error_message()
         assert s.solve_device(d_x.data_ptr(), g.n, 1, sh), s.last_error_message()
 
-    # Warm-up (untimed).
+    # Untimed: four host-buffer refactor + solve calls (the autotuner's trials
+    # of the large-unit refactor schedule), then the device-path warm-up.
+    for k in range(4):
+        v, b = inputs[k % total]
+        x = b.copy()
+        assert s.refactor_values(v) and s.solve_in_place(x), s.last_error_message()
     for k in range(args.warmup):
         d_x.copy_(d_b[k])
         device_step(k)
@@ -785,7 +995,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     step_ms, phases, resid, launches = [], [], [], []
-    with ClockSampler(local) as clocks:
+    with ClockSampler(dev.index or 0) as clocks:
         for k in range(args.warmup, total):
             flush.fill_(float(k))
             d_x.copy_(d_b[k])
@@ -797,7 +1007,7 @@ def main():
             step_ms.append(e0.elapsed_time(e1))
             phases.append(s.phase_times())
             st = s.stats()
-            launches.append(st["factor_launches"] + st["solve_launches"] + 0)
+            launches.append(st["factor_launches"] + st["solve_launches"])
             x = d_x.cpu().numpy()
             v, b = inputs[k]
             r = b.copy()
@@ -812,9 +1022,8 @@ def main():
     my_ms = max_over_ranks(sum(step_ms), dist, dev)
     ms_per_step = my_ms / args.steps
     value = world * 1000.0 / ms_per_step
-
     # End to end through the C ABI with pinned host buffers.
-    pin_v = [torch.from_numpy(v).pin_memory() for v, _ in inputs[: args.warmup + args.steps]]
+    pin_v = [torch.from_numpy(v).pin_memory() for v, _ in inputs]
     pin_b = torch.empty(g.n, dtype=torch.float64).pin_memory()
     e2e_ms = []
     for k in range(total):
@@ -827,34 +1036,11 @@ def main():
         assert ok == 0, s.last_error_message()
         if k >= args.warmup:
             e2e_ms.append(dt)
-    e2e = world * 1000.0 / statistics.mean(e2e_ms)
-
-    if rank != 0:
-        if dist:
-            dist.destroy_process_group()
-        return
-    # Roofline of the dominant phase.
+    e2e_ms_max = max_over_ranks(statistics.mean(e2e_ms), dist, dev)
+    e2e = world * 1000.0 / e2e_ms_max
     ph = {key: statistics.mean(p[key] for p in phases) for key in phases[0]}
     dominant = max(("lu_small", "lu_large", "solve"), key=lambda key: ph[key])
     peaks = measured_peaks()
-    dgemm = None
-    if dominant in ("lu_small", "lu_large"):
-        n8 = 8192
-        a = torch.randn(n8, n8, dtype=torch.float64, device=dev)
-        torch.matmul(a, a)
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        best = 1e30
-        for _ in range(3):
-            e0.record()
-            torch.matmul(a, a)
-            e1.record()
-            e1.synchronize()
-            best = min(best, e0.elapsed_time(e1))
-        dgemm = 2.0 * n8 ** 3 / (best * 1e-3) / 1e12
-        del a
-    flops_large = first["factor_flops"]  # both dense classes; split below
-    roofline = None
     if dominant == "solve":
         traffic = 8 * first["dense_entries"] + 12 * first["nnz_offdiag"] + 8 * 4 * g.n
         achieved = traffic / (ph["solve"] * 1e-3) / 1e9
@@ -863,37 +1049,107 @@ def main():
                     "traffic": None, "kernel": "solve sweep (k_solve_scalar / k_solve_dense / k_trsv_tiles levels)",
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"}
     else:
-        achieved = flops_large / (ph["lu_small"] + ph["lu_large"]) / 1e9
+        dgemm = measured_dgemm(dev)
+        achieved = first["factor_flops"] / (ph["lu_small"] + ph["lu_large"]) / 1e9
         roofline = {"bound": "tensor", "achieved": achieved, "peak": dgemm, "unit": "TFLOP/s",
-                    "frac": achieved / dgemm if dgemm else None, "traffic": None,
-                    "kernel": "dense block LU phases (k_lu_small; value-only refactor: k_rdag tile task graph, "
-                              "or k_rpanel / k_rgemm step chain), FP64",
-                    "peak_source": "FP64 pipe: torch.matmul float64 8192^3 measured in this run "
-                                   "(MEASURED_PEAKS.json has no FP64 figure)"}
+                    "frac": achieved / dgemm, "traffic": profile_traffic("k_rgemm"),
+                    "kernel": "dense block LU phases (k_lu_small; value-only refactor: k_rpanel / k_rgemm step "
+                              "chain, or k_rdag tile task graph), FP64 FMA pipe",
+                    "peak_source": "FP64: torch.matmul float64 8192^3 measured in this run (MEASURED_PEAKS.json "
+                                   "has no FP64 figure)"}
+    return {"value": value, "ms_per_step": ms_per_step, "e2e": e2e, "phases_ms": ph, "tuner": bd.tuner_report(),
+            "residual_inf_max": max(resid), "roofline": roofline, "clocks": clocks.summary(),
+            "gpu_launches": int(sum(launches)), "n": g.n, "nnz": nnz, "first": first, "analyze_s": analyze_s}
+
+
+def measured_dgemm(dev):
+    """FP64 GEMM throughput of this GPU (torch.matmul float64, 8192^3, best of 3)."""
+    import torch
+    n8 = 8192
+    a = torch.randn(n8, n8, dtype=torch.float64, device=dev)
+    torch.matmul(a, a)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e30
+    for _ in range(3):
+        e0.record()
+        torch.matmul(a, a)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a
+    return 2.0 * n8 ** 3 / (best * 1e-3) / 1e12
+
+
+def profile_traffic(kernel):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary profiles/traffic.json, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(kernel, {}).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def run_circuit(args, rank, world):
+    """circuit-200k: the plain FP64 path on the 200k-row circuit system."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    c = measure_circuit(args, world, dist, dev)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_reference(oracle_circuit_system())
+    first = c["first"]
     line = {
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": c["value"], "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": c["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": g.n, "nnz": nnz, "nrhs": 1, "nblocks": first["nblocks"],
+        "config": {"workload": CIRCUIT_WORKLOAD, "n": c["n"], "nnz": c["nnz"], "nrhs": 1, "nblocks": first["nblocks"],
                    "nunits": first["nunits"], "max_block": first["max_unit"], "unit_levels": first["unit_levels"],
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": "flushed (256 MiB write) between timed steps, outside the step window",
-                   "refactor_schedule": "step chain" if args.refactor_schedule == 0 else "task graph",
-                   "analyze_s": analyze_s},
-        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 8 * nnz + 8 * g.n, "d2h_bytes_per_step": 8 * g.n},
-        "phases_ms": ph,
-        "residual_inf_max": max(resid),
-        "roofline": roofline,
+                   "refactor_schedule": {None: "autotuned", 0: "step chain", 1: "task graph"}[args.refactor_schedule],
+                   "analyze_s": c["analyze_s"]},
+        "e2e": {"value": c["e2e"], "unit": METRIC, "h2d_bytes_per_step": 8 * c["nnz"] + 8 * c["n"],
+                "d2h_bytes_per_step": 8 * c["n"]},
+        "phases_ms": c["phases_ms"],
+        "residual_inf_max": c["residual_inf_max"],
+        "roofline": c["roofline"],
         "cpu_baseline": cpu,
-        "clocks": clocks.summary(),
-        "gpu_launches": int(sum(launches)),
+        "clocks": c["clocks"],
+        "gpu_launches": c["gpu_launches"],
+        "tuner": c["tuner"],
     }
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.workload == BATCH_WORKLOAD:
+        run_batch(args, rank, world)
+    elif args.workload == SERVE_WORKLOAD:
+        run_serve(args, rank, world)
+    elif args.workload == PREC_WORKLOAD:
+        run_precision(args, rank, world)
+    elif args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_circuit(args, rank, world)
 
 
 if __name__ == "__main__":

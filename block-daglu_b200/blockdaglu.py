@@ -59,7 +59,7 @@ class ServerStats(ctypes.Structure):
         ("completed", ctypes.c_int64), ("failed", ctypes.c_int64), ("p50_ms", ctypes.c_double),
         ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
         ("throughput", ctypes.c_double), ("resident_bytes", ctypes.c_int64), ("evictions", ctypes.c_int64),
-        ("peak_concurrency", ctypes.c_int32),
+        ("peak_concurrency", ctypes.c_int32), ("kernel_launches", ctypes.c_int64), ("factor_flops", ctypes.c_double),
     ]
 
     def as_dict(self):
@@ -103,6 +103,7 @@ def load_library(path=LIB_PATH):
         "bdlu_get_decomposition": (ctypes.c_int, [vp, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]),
         "bdlu_get_block_lu": (ctypes.c_int32, [vp, ctypes.c_int32, _f64p, _i32p]),
         "bdlu_matrix_signatures": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64)]),
+        "bdlu_tuner_report": (ctypes.c_int64, [ctypes.c_char_p, ctypes.c_int64]),
         "bdlu_batch_create": (vp, []),
         "bdlu_batch_destroy": (None, [vp]),
         "bdlu_batch_add": (ctypes.c_int32, [vp, _i32p, _i32p, _f64p, ctypes.c_int64, ctypes.c_int32]),
@@ -125,6 +126,8 @@ def load_library(path=LIB_PATH):
         "bdlu_server_pattern_bytes": (ctypes.c_int64, [vp, ctypes.c_int32]),
         "bdlu_server_submit": (ctypes.c_int64, [vp, ctypes.c_int32, _f64p, ctypes.c_int64, _f64p, ctypes.c_int32,
                                                 ctypes.c_int32]),
+        "bdlu_server_submit_device": (ctypes.c_int64, [vp, ctypes.c_int32, vp, ctypes.c_int64, vp, ctypes.c_int32,
+                                                      ctypes.c_int32]),
         "bdlu_server_wait": (ctypes.c_int, [vp, ctypes.c_int64, _f64p, _f64p]),
         "bdlu_server_drain": (ctypes.c_int, [vp]),
         "bdlu_server_get_stats": (ctypes.c_int, [vp, ctypes.POINTER(ServerStats)]),
@@ -466,6 +469,17 @@ class Server:
         self._keep[rid] = (v, B)
         return rid
 
+    def submit_device(self, pattern, d_vals, nnz, d_B, ldb, nrhs, keep=None):
+        """Device-resident request: d_vals / d_B are device pointers (ints);
+        X overwrites d_B.  `keep` holds the owning objects until wait.
+        Returns id or -1."""
+        rid = self._lib.bdlu_server_submit_device(self._s, int(pattern), int(d_vals), int(nnz), int(d_B), int(ldb),
+                                                  int(nrhs))
+        if rid < 0:
+            return -1
+        self._keep[rid] = keep
+        return rid
+
     def wait(self, rid):
         """Returns (ok, residual, latency_ms)."""
         res = np.zeros(1)
@@ -496,6 +510,16 @@ class Server:
         buf = ctypes.create_string_buffer(1024)
         self._lib.bdlu_server_last_error(self._s, buf, len(buf))
         return buf.value.decode()
+
+
+def tuner_report():
+    """The autotuner's choices on this GPU (dict; see include/bdlu.h)."""
+    import json
+    lib = load_library()
+    need = lib.bdlu_tuner_report(None, 0)
+    buf = ctypes.create_string_buffer(max(1, int(need)))
+    lib.bdlu_tuner_report(buf, len(buf))
+    return json.loads(buf.value.decode())
 
 
 def btf_order(n, col_ptr, row_ind):

@@ -19,8 +19,10 @@
 #include "capi_internal.h"
 #include "engine.h"
 #include "plan.h"
+#include "tuner.h"
 
 using bdlu::Status;
+using bdlu::Tuner;
 
 namespace {
 // Normwise residual above which a refactor that reused the pivot order is
@@ -73,13 +75,43 @@ int ensure_validated(bdlu_solver* h) {
   return BDLU_OK;
 }
 
+// Whether the refactor schedule of this handle is being tuned: FP64 route,
+// large units with a tile task graph, no schedule set by the caller.
+bool schedule_tunable(const bdlu_solver* h) {
+  return !h->schedule_user_set && !h->mixed && h->engine && Tuner::get().enabled() &&
+         !h->engine->plan().large_units.empty() && h->engine->plan().rtasks > 0;
+}
+
+// Schedule of the next value-only refactor: the caller's, the tuned one, or
+// the next trial (chain, graph, chain, graph).
+int32_t schedule_for(bdlu_solver* h) {
+  if (!schedule_tunable(h)) return h->refactor_schedule;
+  const int t = Tuner::get().refactor_schedule(h->sig);
+  if (t >= 0) return t;
+  return h->sched_trials & 1;
+}
+
+// After a refactor that reused the pivot order completed: a trial's device
+// time; after the fourth trial the faster schedule is kept for the pattern.
+void record_schedule(bdlu_solver* h, int32_t used) {
+  if (!schedule_tunable(h) || !h->engine->last_factor_reused()) return;
+  Tuner& tu = Tuner::get();
+  if (tu.refactor_schedule(h->sig) >= 0 || (h->sched_trials & 1) != used) return;
+  h->sched_ms[used] = h->engine->last_factor_ms();
+  if (++h->sched_trials == 4) {
+    const int best = h->sched_ms[1] < h->sched_ms[0] ? 1 : 0;
+    tu.set_refactor_schedule(h->sig, best, h->sched_ms[0], h->sched_ms[1]);
+  }
+}
+
 // Factor from the engine's value buffer.  reuse: large blocks keep the pivot
 // order of the last full factorisation (value-only refactor); a zero pivot
 // met that way falls back to a factorisation with pivoting.
 int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
-  h->engine->set_refactor_schedule(h->refactor_schedule);
+  const int32_t sched = schedule_for(h);
+  h->engine->set_refactor_schedule(sched);
   h->engine->set_wait_limit(h->wait_limit);
   for (int attempt = 0; attempt < 2; ++attempt) {
     const bool r = reuse && attempt == 0;
@@ -89,6 +121,7 @@ int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
     if (st == 0) {
       h->factored = true;
       h->exported = false;
+      if (r) record_schedule(h, sched);
       return BDLU_OK;
     }
     if (st == 2 && r) continue;
@@ -260,19 +293,32 @@ int64_t bdlu_device_bytes(const bdlu_solver* h) {
 }
 
 int bdlu_solve_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream) {
+  return bdlu_solve_checked_on(h, B, ldb, nrhs, stream, false);
+}
+
+int bdlu_refactor_values_device_on(bdlu_solver* h, const double* d_vals, int64_t nnz, cudaStream_t stream) {
+  if (const int st = refactor_checks(h, d_vals, nnz)) return st;
+  if (const int st = upload_values(h, d_vals, true, stream)) return st;
+  h->host_vals_stale = true;
+  return do_factor(h, stream, h->reuse_pivots);
+}
+
+int bdlu_solve_checked_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream, bool device) {
   if (!h) return BDLU_NOT_PREPARED;
   clear_error(h);
   if (!h->factored) return fail(h, BDLU_NOT_PREPARED, "factor must succeed before solve");
   if (!B || nrhs < 1 || ldb < h->n) return fail(h, BDLU_INVALID_RHS, "right-hand side size does not match matrix dimension");
-  for (int32_t k = 0; k < nrhs; ++k)
-    if (!all_finite(B + static_cast<size_t>(k) * ldb, h->n))
-      return fail(h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
+  if (!device)
+    for (int32_t k = 0; k < nrhs; ++k)
+      if (!all_finite(B + static_cast<size_t>(k) * ldb, h->n))
+        return fail(h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
   std::string err;
   double* d_B = h->engine->rhs_buffer(nrhs, err);
   if (!d_B) return fail(h, BDLU_SOLVE_FAILED, err);
   cudaError_t e = cudaMemcpy2DAsync(d_B, static_cast<size_t>(h->n) * sizeof(double), B,
                                     static_cast<size_t>(ldb) * sizeof(double), static_cast<size_t>(h->n) * sizeof(double),
-                                    static_cast<size_t>(nrhs), cudaMemcpyHostToDevice, stream);
+                                    static_cast<size_t>(nrhs),
+                                    device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("rhs upload: ") + cudaGetErrorString(e));
   const int iters = refine_iters_for(h);
   auto relres = [](const bdlu::SolveResidual& q) {
@@ -343,7 +389,8 @@ int bdlu_solve_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStre
     if (const int st = solve_once()) return st;
   }
   e = cudaMemcpy2DAsync(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
-                        static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToHost, stream);
+                        static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs),
+                        device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
   h->last_refine = iters + steps;
@@ -427,6 +474,12 @@ int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nn
   if (const int st = upload_values(h, d_vals, true, s)) return st;
   h->host_vals_stale = true;
   std::string err;
+  // No status wait here, so no schedule trial: the tuned schedule if the
+  // pattern has one, else the handle's.
+  const int tuned = schedule_tunable(h) ? Tuner::get().refactor_schedule(h->sig) : -1;
+  h->engine->set_precision(h->mixed ? h->prec_level : 0);
+  h->engine->set_refactor_schedule(tuned >= 0 ? tuned : h->refactor_schedule);
+  h->engine->set_wait_limit(h->wait_limit);
   if (!h->engine->factor_async(h->engine->values_buffer(), s, err, h->reuse_pivots))
     return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
   // Zero pivots are reported by the next synchronising call (bdlu_solve_status).
@@ -458,13 +511,16 @@ int bdlu_refactor_solve(bdlu_solver* h, const double* vals, int64_t nnz, double*
   if (const int st = stage_host_values(h, vals, nnz, nullptr)) return st;
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
-  h->engine->set_refactor_schedule(h->refactor_schedule);
+  const int32_t sched = schedule_for(h);
+  h->engine->set_refactor_schedule(sched);
   h->engine->set_wait_limit(h->wait_limit);
   if (!h->engine->factor_async(h->engine->values_buffer(), nullptr, err, h->reuse_pivots))
     return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
   h->factored = true;
   h->exported = false;
-  return bdlu_solve(h, B, ldb, nrhs);
+  const int st = bdlu_solve(h, B, ldb, nrhs);
+  if (st == BDLU_OK) record_schedule(h, sched);
+  return st;
 }
 
 int bdlu_last_error(const bdlu_solver* h, char* buf, int64_t len) {
@@ -489,6 +545,20 @@ int64_t bdlu_canonical_pattern(const bdlu_solver* h, int32_t* rows, int32_t* col
   if (rows) std::memcpy(rows, h->coo.row.data(), static_cast<size_t>(nnz) * sizeof(int32_t));
   if (cols) std::memcpy(cols, h->coo.col.data(), static_cast<size_t>(nnz) * sizeof(int32_t));
   return nnz;
+}
+
+int64_t bdlu_tuner_report(char* buf, int64_t len) {
+  try {
+    const std::string r = bdlu::Tuner::get().report();
+    if (buf && len > 0) {
+      const size_t k = std::min<size_t>(static_cast<size_t>(len - 1), r.size());
+      std::memcpy(buf, r.data(), k);
+      buf[k] = '\0';
+    }
+    return static_cast<int64_t>(r.size()) + 1;
+  } catch (...) {
+    return -1;
+  }
 }
 
 int bdlu_matrix_signatures(const bdlu_solver* h, uint64_t* sigs) {
@@ -549,6 +619,7 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
   if (k == "refactor_schedule") {
     if (value != 0.0 && value != 1.0) return BDLU_INVALID_DIMENSION;
     h->refactor_schedule = static_cast<int32_t>(value);
+    h->schedule_user_set = true;
     if (h->engine) h->engine->set_refactor_schedule(h->refactor_schedule);
     return BDLU_OK;
   }

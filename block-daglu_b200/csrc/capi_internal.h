@@ -39,6 +39,11 @@ struct bdlu_solver {
   bool mixed = false;         // "precision" = 1: tensor-core updates + FP64 refinement
   int32_t prec_level = 1;     // mixed route's current level: 1 TF32, 2 3xTF32, 0 FP64 (sticky)
   int32_t refactor_schedule = 0;  // 0 step chain, 1 tile task graph (Engine::set_refactor_schedule)
+  bool schedule_user_set = false; // refactor_schedule set by the caller: no autotuning
+  // Autotuning of the refactor schedule (tuner.h): trial refactors run
+  // chain, graph, chain, graph; the second time of each decides.
+  int32_t sched_trials = 0;
+  float sched_ms[2] = {0.0f, 0.0f};
   int32_t wait_limit = 0;         // polls of a bounded wait between tiles (0: default; Engine::set_wait_limit)
   // Error state (solver.h:122-123).
   int last_error = BDLU_OK;
@@ -74,6 +79,13 @@ int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf*
 // synchronisation as bdlu_refactor_values / bdlu_solve.
 int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream);
 int bdlu_solve_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream);
+
+// The same two steps with the values and right-hand sides in device memory
+// (the serving loop's device-resident requests): no host finiteness check;
+// the solve still reads the residual and status and applies the fallbacks,
+// and returns with B overwritten on the device and `stream` synchronised.
+int bdlu_refactor_values_device_on(bdlu_solver* h, const double* d_vals, int64_t nnz, cudaStream_t stream);
+int bdlu_solve_checked_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream, bool device);
 
 // Brings coo.val up to date from the engine's value buffer after refactors
 // that skipped the host copy (synchronises the device).  Returns a status

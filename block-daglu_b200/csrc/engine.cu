@@ -20,6 +20,7 @@
 
 #include "device_util.cuh"
 #include "tc_update.cuh"
+#include "tuner.h"
 #include "large.h"
 
 #include <cuda_runtime.h>
@@ -674,6 +675,61 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   return true;
 }
 
+void Engine::launch_lu_small(int threads, int32_t units, int32_t mb, cudaStream_t st, const double* d_vals,
+                             const int32_t* list) {
+  const size_t smem = static_cast<size_t>(mb) * mb * sizeof(double);
+  if (threads == 64) k_lu_small<64><<<units, 64, smem, st>>>(dp_, d_vals, list);
+  else if (threads == 128) k_lu_small<128><<<units, 128, smem, st>>>(dp_, d_vals, list);
+  else k_lu_small<kThreads><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
+}
+
+int Engine::lu_small_width(int32_t mb) const {
+  // The kernel needs one thread per row for its first pivot scan (m <= CTA
+  // width).  Tuned choice, else the rule it replaces: narrow CTAs for small
+  // units (more units per SM, cheaper per-column barriers).
+  const int t = Tuner::get().enabled() ? Tuner::get().lu_small_threads(mb) : 0;
+  if (t >= mb && (t == 64 || t == 128 || t == kThreads)) return t;
+  return mb <= 32 ? 64 : (mb <= 64 ? 128 : kThreads);
+}
+
+// Times every admissible CTA width of each size bucket this GPU has no
+// choice for yet, on the bucket's own units (one untimed and one timed
+// launch each; the launches write the same factors the real one writes).
+cudaError_t Engine::tune_lu_small(const double* d_vals, cudaStream_t stream) {
+  const Plan& p = plan_;
+  Tuner& tu = Tuner::get();
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaSuccess;
+  for (size_t bkt = 0; bkt < p.small_bucket_m.size() && e == cudaSuccess; ++bkt) {
+    const int32_t mb = p.small_bucket_m[bkt];
+    if (tu.lu_small_threads(mb) != 0) continue;
+    if (!e0 && ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess)) break;
+    const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
+    int widths[3], count = 0;
+    for (int t : {64, 128, kThreads})
+      if (t >= mb) widths[count++] = t;
+    float ms[3] = {0.0f, 0.0f, 0.0f};
+    int best = widths[count - 1];
+    float best_ms = 1e30f;
+    for (int c = 0; c < count && e == cudaSuccess; ++c) {
+      launch_lu_small(widths[c], q1 - q0, mb, stream, d_vals, small_list_ + q0);
+      cudaEventRecord(e0, stream);
+      launch_lu_small(widths[c], q1 - q0, mb, stream, d_vals, small_list_ + q0);
+      cudaEventRecord(e1, stream);
+      if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+      cudaEventElapsedTime(&ms[c], e0, e1);
+      if (ms[c] < best_ms) {
+        best_ms = ms[c];
+        best = widths[c];
+      }
+    }
+    if (e == cudaSuccess) tu.set_lu_small_threads(mb, best, ms, widths, count);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
 bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string& err, bool reuse_pivots) {
   const Plan& p = plan_;
   const bool reuse = reuse_pivots && have_pivots_ && !p.large_units.empty();
@@ -687,6 +743,12 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   // One launch per size bucket, shared memory sized to the bucket; the
   // buckets run side by side on the auxiliary streams (forked from and
   // joined back into `stream`), largest units first.
+  if (!p.small_bucket_m.empty() && Tuner::get().enabled()) {
+    // Tuning waits for its timing events: never inside a caller's capture.
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    BDLU_CUDA(cudaStreamIsCapturing(stream, &cap));
+    if (cap == cudaStreamCaptureStatusNone) BDLU_CUDA(tune_lu_small(d_vals, stream));
+  }
   if (!p.small_bucket_m.empty()) {
     BDLU_CUDA(cudaEventRecord(fork_ev_[0], stream));
     const size_t nbk = p.small_bucket_m.size();
@@ -695,13 +757,8 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
       cudaStream_t sb = aux_[q % kAux];
       if (q < static_cast<size_t>(kAux)) BDLU_CUDA(cudaStreamWaitEvent(sb, fork_ev_[0], 0));
       const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
-      const size_t mb = static_cast<size_t>(p.small_bucket_m[bkt]);
-      const size_t smem = mb * mb * sizeof(double);
-      // CTA width follows the unit size: narrow CTAs let more small units
-      // run per SM and make the per-column barriers cheaper.
-      if (mb <= 32) k_lu_small<64><<<q1 - q0, 64, smem, sb>>>(dp_, d_vals, small_list_ + q0);
-      else if (mb <= 64) k_lu_small<128><<<q1 - q0, 128, smem, sb>>>(dp_, d_vals, small_list_ + q0);
-      else k_lu_small<kThreads><<<q1 - q0, kThreads, smem, sb>>>(dp_, d_vals, small_list_ + q0);
+      const int32_t mb = p.small_bucket_m[bkt];
+      launch_lu_small(lu_small_width(mb), q1 - q0, mb, sb, d_vals, small_list_ + q0);
     }
     for (int q = 0; q < kAux && q < static_cast<int>(nbk); ++q) {
       BDLU_CUDA(cudaEventRecord(aux_ev_[q], aux_[q]));

@@ -139,6 +139,12 @@ class Engine {
  private:
   void release();
   bool ensure_work(int32_t nrhs, std::string& err);
+  // Shared-memory LU of one size bucket with `threads` per CTA; the width the
+  // autotuner chose for a bucket (or the default rule); the tuning itself.
+  void launch_lu_small(int threads, int32_t units, int32_t mb, cudaStream_t st, const double* d_vals,
+                       const int32_t* list);
+  int lu_small_width(int32_t mb) const;
+  cudaError_t tune_lu_small(const double* d_vals, cudaStream_t stream);
   void solve_core(const double* rhs, int32_t ldr, double* xp, const int32_t* nrhs, bool wide, cudaStream_t stream);
   void refine_core(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream);
   int32_t prec_ = 0;

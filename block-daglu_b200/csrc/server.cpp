@@ -53,6 +53,7 @@ struct Request {
   const double* vals = nullptr;
   double* B = nullptr;
   int32_t ldb = 0, nrhs = 0;
+  bool device = false;  // vals and B are device pointers (device-resident request)
   double t_submit = 0.0, t_done = 0.0;
   int status = BDLU_OK;
   double residual = 0.0;
@@ -79,6 +80,8 @@ struct bdlu_server {
   std::vector<double> latencies;
   double t_first = -1.0, t_last = 0.0;
   int64_t completed = 0, failed = 0;
+  int64_t kernel_launches = 0;
+  double factor_flops = 0.0;
   std::string last_message;
   int last_error = BDLU_OK;
   double precision = 0.0;  // "precision" option of every pattern's handle
@@ -173,22 +176,28 @@ void worker(bdlu_server* s) {
     int st = BDLU_OK;
     const int64_t reserved = p.bytes;
     if (!bdlu_engine_ready(p.h)) st = bdlu_device_restore(p.h);
-    const size_t nb = static_cast<size_t>(p.n) * static_cast<size_t>(r->nrhs);
-    double* sv = vstage.get(static_cast<size_t>(p.nnz));
-    double* sb = bstage.get(nb);
-    if (st == BDLU_OK && (!sv || !sb)) st = -1;
-    if (st == BDLU_OK) {
-      std::copy(r->vals, r->vals + p.nnz, sv);
-      for (int32_t k = 0; k < r->nrhs; ++k)
-        std::copy(r->B + static_cast<size_t>(k) * r->ldb, r->B + static_cast<size_t>(k) * r->ldb + p.n,
-                  sb + static_cast<size_t>(k) * p.n);
-      st = bdlu_refactor_values_on(p.h, sv, p.nnz, stream);
+    if (r->device) {
+      // Device-resident request: values and right-hand sides never leave HBM.
+      if (st == BDLU_OK) st = bdlu_refactor_values_device_on(p.h, r->vals, p.nnz, stream);
+      if (st == BDLU_OK) st = bdlu_solve_checked_on(p.h, r->B, r->ldb, r->nrhs, stream, true);
+    } else {
+      const size_t nb = static_cast<size_t>(p.n) * static_cast<size_t>(r->nrhs);
+      double* sv = vstage.get(static_cast<size_t>(p.nnz));
+      double* sb = bstage.get(nb);
+      if (st == BDLU_OK && (!sv || !sb)) st = -1;
+      if (st == BDLU_OK) {
+        std::copy(r->vals, r->vals + p.nnz, sv);
+        for (int32_t k = 0; k < r->nrhs; ++k)
+          std::copy(r->B + static_cast<size_t>(k) * r->ldb, r->B + static_cast<size_t>(k) * r->ldb + p.n,
+                    sb + static_cast<size_t>(k) * p.n);
+        st = bdlu_refactor_values_on(p.h, sv, p.nnz, stream);
+      }
+      if (st == BDLU_OK) st = bdlu_solve_on(p.h, sb, p.n, r->nrhs, stream);
+      if (st == BDLU_OK)
+        for (int32_t k = 0; k < r->nrhs; ++k)
+          std::copy(sb + static_cast<size_t>(k) * p.n, sb + static_cast<size_t>(k + 1) * p.n,
+                    r->B + static_cast<size_t>(k) * r->ldb);
     }
-    if (st == BDLU_OK) st = bdlu_solve_on(p.h, sb, p.n, r->nrhs, stream);
-    if (st == BDLU_OK)
-      for (int32_t k = 0; k < r->nrhs; ++k)
-        std::copy(sb + static_cast<size_t>(k) * p.n, sb + static_cast<size_t>(k + 1) * p.n,
-                  r->B + static_cast<size_t>(k) * r->ldb);
     char buf[512] = "host staging allocation failed";
     if (st > 0) bdlu_last_error(p.h, buf, sizeof(buf));
     if (st < 0) st = BDLU_BACKEND_UNAVAILABLE;
@@ -213,7 +222,9 @@ void worker(bdlu_server* s) {
       r->t_done = now_ms();
       r->done = true;
       --s->running;
+      s->kernel_launches += static_cast<int64_t>(stats.factor_launches) + stats.solve_launches;
       if (st == BDLU_OK) {
+        s->factor_flops += stats.factor_flops;
         ++s->completed;
         s->latencies.push_back(r->t_done - r->t_submit);
         s->t_last = std::max(s->t_last, r->t_done);
@@ -319,8 +330,8 @@ int64_t bdlu_server_pattern_bytes(bdlu_server* s, int32_t pattern) {
   return s->patterns[static_cast<size_t>(pattern)]->bytes;
 }
 
-int64_t bdlu_server_submit(bdlu_server* s, int32_t pattern, const double* vals, int64_t nnz, double* B, int32_t ldb,
-                           int32_t nrhs) {
+static int64_t submit_request(bdlu_server* s, int32_t pattern, const double* vals, int64_t nnz, double* B,
+                              int32_t ldb, int32_t nrhs, bool device) {
   if (!s) return -BDLU_NOT_PREPARED;
   std::lock_guard<std::mutex> lk(s->mu);
   if (pattern < 0 || pattern >= static_cast<int32_t>(s->patterns.size()))
@@ -335,6 +346,7 @@ int64_t bdlu_server_submit(bdlu_server* s, int32_t pattern, const double* vals, 
   r->B = B;
   r->ldb = ldb;
   r->nrhs = nrhs;
+  r->device = device;
   r->t_submit = now_ms();
   if (s->t_first < 0.0) s->t_first = r->t_submit;
   s->queue.push_back(r.get());
@@ -342,6 +354,16 @@ int64_t bdlu_server_submit(bdlu_server* s, int32_t pattern, const double* vals, 
   s->requests.emplace(id, std::move(r));
   s->cv_work.notify_one();
   return id;
+}
+
+int64_t bdlu_server_submit(bdlu_server* s, int32_t pattern, const double* vals, int64_t nnz, double* B, int32_t ldb,
+                           int32_t nrhs) {
+  return submit_request(s, pattern, vals, nnz, B, ldb, nrhs, false);
+}
+
+int64_t bdlu_server_submit_device(bdlu_server* s, int32_t pattern, const double* d_vals, int64_t nnz, double* d_B,
+                                  int32_t ldb, int32_t nrhs) {
+  return submit_request(s, pattern, d_vals, nnz, d_B, ldb, nrhs, true);
 }
 
 int bdlu_server_wait(bdlu_server* s, int64_t request, double* residual, double* latency_ms) {
@@ -382,6 +404,8 @@ int bdlu_server_get_stats(bdlu_server* s, bdlu_server_stats* out) {
   out->resident_bytes = s->resident_bytes;
   out->evictions = s->evictions;
   out->peak_concurrency = s->peak_running;
+  out->kernel_launches = s->kernel_launches;
+  out->factor_flops = s->factor_flops;
   return BDLU_OK;
 }
 
@@ -390,6 +414,8 @@ int bdlu_server_reset_stats(bdlu_server* s) {
   std::lock_guard<std::mutex> lk(s->mu);
   s->latencies.clear();
   s->completed = s->failed = 0;
+  s->kernel_launches = 0;
+  s->factor_flops = 0.0;
   s->t_first = -1.0;
   s->t_last = 0.0;
   s->peak_running = s->running;

@@ -247,6 +247,8 @@ typedef struct bdlu_server_stats {
   int64_t resident_bytes;   /* device bytes of resident patterns (estimates for ones being uploaded) */
   int64_t evictions;        /* patterns released to admit others */
   int32_t peak_concurrency; /* most requests running at once */
+  int64_t kernel_launches;  /* engine kernels launched by the completed requests (graph nodes counted) */
+  double factor_flops;      /* dense-block LU flops of the completed requests (one factor each) */
 } bdlu_server_stats;
 bdlu_server* bdlu_server_create(int64_t memory_budget_bytes, int32_t slots);
 void bdlu_server_destroy(bdlu_server* s);
@@ -258,6 +260,11 @@ int64_t bdlu_server_pattern_nnz(bdlu_server* s, int32_t pattern);
 int64_t bdlu_server_pattern_bytes(bdlu_server* s, int32_t pattern);
 int64_t bdlu_server_submit(bdlu_server* s, int32_t pattern, const double* vals, int64_t nnz, double* B, int32_t ldb,
                            int32_t nrhs);
+/* Device-resident request: d_vals and d_B are device pointers (the current
+ * device's memory); the values and right-hand sides never cross to the host
+ * (no host finiteness check), X overwrites d_B. */
+int64_t bdlu_server_submit_device(bdlu_server* s, int32_t pattern, const double* d_vals, int64_t nnz, double* d_B,
+                                  int32_t ldb, int32_t nrhs);
 int bdlu_server_wait(bdlu_server* s, int64_t request, double* residual, double* latency_ms);
 int bdlu_server_drain(bdlu_server* s);
 int bdlu_server_get_stats(bdlu_server* s, bdlu_server_stats* out);
@@ -324,6 +331,20 @@ int32_t bdlu_get_block_lu(bdlu_solver* h, int32_t b, double* lu_rowmajor, int32_
  * blockdaglu/src/solver.cpp:96-136): sigs[0..2].  The serving loop keys its
  * resident patterns by them. */
 int bdlu_matrix_signatures(const bdlu_solver* h, uint64_t* sigs);
+
+/* ---- Autotuner --------------------------------------------------------------
+ * No counterpart in the reference (it tunes by environment knobs,
+ * blockdaglu/src/ubtf_block_solver.cpp:35-568).  The engine times its
+ * launch-shape and schedule candidates on the GPU it runs on and keeps the
+ * faster (every candidate computes bit-identical results): the CTA width of
+ * the shared-memory LU per size bucket, and per pattern signature the
+ * value-only refactor schedule of large units (step chain or tile task graph,
+ * decided over the pattern's first four refactors that wait for their
+ * status).  Choices persist in $BDLU_TUNE_CACHE, else
+ * $HOME/.cache/bdlu/tune-<gpu>.json; BDLU_AUTOTUNE=0 disables tuning.
+ * bdlu_tuner_report writes the choices as JSON (NUL-terminated, at most len
+ * bytes) and returns the bytes needed including the NUL. */
+int64_t bdlu_tuner_report(char* buf, int64_t len);
 
 /* ---- Seeded synthetic systems --------------------------------------------- */
 enum bdlu_synth_family { BDLU_SYNTH_BLOCK = 0, BDLU_SYNTH_CIRCUIT = 1, BDLU_SYNTH_PRECISION = 3 };

@@ -11,6 +11,12 @@ for sub in ("", "block-daglu_b200", "oracle"):
         sys.path.insert(0, p)
 
 
+# The autotuner's cache goes to a per-run temporary file, not $HOME.
+if "BDLU_TUNE_CACHE" not in os.environ:
+    import tempfile
+    os.environ["BDLU_TUNE_CACHE"] = os.path.join(tempfile.mkdtemp(prefix="bdlu-tune-"), "tune.json")
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
     config.addinivalue_line("markers", "slow: long-running parity case")

@@ -123,3 +123,41 @@ def test_server_pattern_above_budget_fails(cuda_device):
     ok, _, _ = s.wait(rid)
     assert not ok and s.last_error() == bd.SolverError.BackendUnavailable
     s.close()
+
+
+@pytest.mark.gpu
+def test_server_device_resident_requests_match_host_requests(cuda_device):
+    """Requests whose values and right-hand sides already live in device
+    memory (bdlu_server_submit_device) run the same kernels as host-buffer
+    requests: the same stream gives the same solutions, alone and mixed with
+    host requests, and the mixed-precision server option keeps the bound."""
+    import torch
+    patterns = _patterns(3, 5)
+    reqs = _stream(patterns, 12, 6)
+    host, _, _ = _serve(patterns, reqs, slots=1)
+    for prec in (0, 1):
+        s = bd.Server(64 << 30, 4)
+        assert s.set_option("precision", prec)
+        for g in patterns:
+            s.add_pattern((g.rows, g.cols, g.vals), g.n)
+        dv = [torch.from_numpy(v).cuda() for _, v, _ in reqs]
+        dB = [torch.from_numpy(np.ascontiguousarray(B.T)).cuda() for _, _, B in reqs]  # (nrhs, n): column-major
+        torch.cuda.synchronize()
+        rids = []
+        for i, ((k, v, B), a, b) in enumerate(zip(reqs, dv, dB)):
+            if i % 3 == 2:   # every third request from host buffers
+                X = B.copy(order="F")
+                rids.append((s.submit(k, v, X), X))
+            else:
+                rids.append((s.submit_device(k, a.data_ptr(), len(v), b.data_ptr(), B.shape[0], B.shape[1],
+                                             keep=(a, b)), b))
+        assert all(r >= 0 for r, _ in rids), s.last_error_message()
+        for (k, v, B), (rid, out), xh in zip(reqs, rids, host):
+            ok, resid, _ = s.wait(rid)
+            assert ok and resid <= 1e-12, s.last_error_message()
+            X = out if isinstance(out, np.ndarray) else out.cpu().numpy().T
+            for j in range(B.shape[1]):
+                assert _relres(patterns[k], v, X[:, j], B[:, j]) <= 1e-12
+            if prec == 0:
+                assert np.allclose(X, xh, rtol=1e-12, atol=0.0)
+        s.close()

@@ -1,0 +1,64 @@
+"""The autotuner (include/bdlu.h, csrc/tuner.cpp): launch widths of the
+shared-memory LU per size bucket and the refactor schedule of large units per
+pattern, timed on the GPU and kept in a per-GPU JSON cache.  Every candidate
+computes bit-identical results, so the parity tests (which run with tuning
+on) already cover correctness; here the choices themselves are checked."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import blockdaglu as bd
+
+pytestmark = pytest.mark.gpu
+
+
+def test_tuner_picks_lu_small_widths(cuda_device, monkeypatch):
+    monkeypatch.delenv("BLOCKDAGLU_MODE", raising=False)
+    g = bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(0, 50), 2000)
+    s = bd.Solver()
+    assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze() and s.factor(), s.last_error_message()
+    rep = bd.tuner_report()
+    if not rep["enabled"]:
+        pytest.skip("BDLU_AUTOTUNE=0")
+    widths = {e["bucket_m"]: e for e in rep["lu_small_threads"]}
+    assert widths, rep
+    for m, e in widths.items():
+        assert e["threads"] in (64, 128, 256) and e["threads"] >= m
+        if "ms" in e:
+            assert len(e["ms"]) == len(e["widths"]) and min(e["ms"]) > 0.0
+            assert e["ms"][e["widths"].index(e["threads"])] == min(e["ms"])
+    # The choice persists in the cache file.
+    with open(rep["cache"]) as f:
+        saved = json.load(f)
+    assert {e["bucket_m"]: e["threads"] for e in saved["lu_small_threads"]} == \
+        {m: e["threads"] for m, e in widths.items()}
+
+
+def test_tuner_picks_refactor_schedule_per_pattern(cuda_device, monkeypatch):
+    # One 2,000-row large unit: its value-only refactors run the step chain
+    # and the tile task graph in turn (4 trials), then the faster stays.
+    monkeypatch.setenv("BLOCKDAGLU_MODE", "klu")
+    g = bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(0, 51), 2000, 40)
+    s = bd.Solver()
+    assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze() and s.factor(), s.last_error_message()
+    xs = []
+    for k in range(6):
+        v = g.perturbed(700 + (k % 2))
+        assert s.refactor_values(v), s.last_error_message()
+        x = g.b[:, 0].copy()
+        assert s.solve_in_place(x), s.last_error_message()
+        xs.append(x)
+    # Same values, either schedule: bit-identical solutions.
+    assert np.array_equal(xs[0], xs[2]) and np.array_equal(xs[1], xs[3]) and np.array_equal(xs[0], xs[4])
+    rep = bd.tuner_report()
+    if not rep["enabled"]:
+        pytest.skip("BDLU_AUTOTUNE=0")
+    sig = s.signatures()[0]
+    entry = [e for e in rep["refactor_schedule"] if int(e["sig"], 16) == sig]
+    assert len(entry) == 1, rep
+    e = entry[0]
+    assert e["schedule"] in (0, 1) and e["ms_chain"] > 0.0 and e["ms_graph"] > 0.0
+    assert e["schedule"] == (1 if e["ms_graph"] < e["ms_chain"] else 0)
+    assert os.path.exists(rep["cache"])
