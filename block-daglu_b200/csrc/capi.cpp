@@ -110,6 +110,7 @@ void record_schedule(bdlu_solver* h, int32_t used) {
 int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
+  h->engine->set_lu_small_width(h->lu_small_threads);
   const int32_t sched = schedule_for(h);
   h->engine->set_refactor_schedule(sched);
   h->engine->set_wait_limit(h->wait_limit);
@@ -478,6 +479,7 @@ int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nn
   // pattern has one, else the handle's.
   const int tuned = schedule_tunable(h) ? Tuner::get().refactor_schedule(h->sig) : -1;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
+  h->engine->set_lu_small_width(h->lu_small_threads);
   h->engine->set_refactor_schedule(tuned >= 0 ? tuned : h->refactor_schedule);
   h->engine->set_wait_limit(h->wait_limit);
   if (!h->engine->factor_async(h->engine->values_buffer(), s, err, h->reuse_pivots))
@@ -511,6 +513,7 @@ int bdlu_refactor_solve(bdlu_solver* h, const double* vals, int64_t nnz, double*
   if (const int st = stage_host_values(h, vals, nnz, nullptr)) return st;
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
+  h->engine->set_lu_small_width(h->lu_small_threads);
   const int32_t sched = schedule_for(h);
   h->engine->set_refactor_schedule(sched);
   h->engine->set_wait_limit(h->wait_limit);
@@ -621,6 +624,16 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
     h->refactor_schedule = static_cast<int32_t>(value);
     h->schedule_user_set = true;
     if (h->engine) h->engine->set_refactor_schedule(h->refactor_schedule);
+    return BDLU_OK;
+  }
+  if (k == "lu_small_threads") {
+    // Launch width of the shared-memory LU: 0 the autotuner's choice (or the
+    // default rule), 32 one warp per unit (units up to 64 rows), 64 / 128 /
+    // 256 threads per unit (units up to that many rows).  All give the same
+    // factors; a width a bucket cannot take falls back to the tuned one.
+    if (value != 0.0 && value != 32.0 && value != 64.0 && value != 128.0 && value != 256.0)
+      return BDLU_INVALID_DIMENSION;
+    h->lu_small_threads = static_cast<int32_t>(value);
     return BDLU_OK;
   }
   if (k == "wait_limit") {

@@ -196,6 +196,114 @@ __global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __res
 }
 
 // ---------------------------------------------------------------------------
+// Column-warp LU: one warp per unit of up to 32*R rows (the C2 "column-warp"
+// path), several units per CTA, no CTA barriers.  Lane l holds rows l,
+// l + 32, ... of the unit in registers (all columns, statically indexed: the
+// column loop is unrolled), row swaps are logical (each held row carries its
+// current position; a swap exchanges two positions), the pivot row is
+// broadcast by shuffles.  Per element the arithmetic is the micro-kernel's:
+// first strict maximum of |a| (ties to the smallest position), multipliers by
+// division, a - l*u as multiply then subtract; so the factors, pivots and row
+// order are bit-identical to k_lu_small's.
+template <int R, int W>
+__global__ void __launch_bounds__(32 * W) k_lu_warp(DevPlan dp, const double* __restrict__ vals,
+                                                    const int32_t* __restrict__ units, int32_t count) {
+  constexpr int M = 32 * R;
+  constexpr int kNone = 1 << 20;  // position of rows outside the unit
+  extern __shared__ double wsm[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int slot = blockIdx.x * W + wib;
+  if (slot >= count) return;  // warp-uniform
+  const int u = units[slot];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  double* S = wsm + static_cast<size_t>(wib) * M * M;  // staging, column-major, ld m
+  for (int i = lane; i < m * m; i += 32) S[i] = 0.0;
+  __syncwarp();
+  for (int64_t e = dp.dent_ptr[u] + lane; e < dp.dent_ptr[u + 1]; e += 32) S[dp.dent_pos[e]] = vals[dp.dent_src[e]];
+  __syncwarp();
+  double a[R][M];
+  int pos[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int row = lane + 32 * r;
+    pos[r] = row < m ? row : kNone;
+#pragma unroll
+    for (int j = 0; j < M; ++j) a[r][j] = (row < m && j < m) ? S[j * m + row] : 0.0;
+  }
+  int32_t* piv = dp.piv + s;
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    if (k >= m) break;
+    // Pivot: this lane's best row (largest |a|, smallest position), then the
+    // warp's.
+    double best = 0.0;
+    int bpos = kNone;
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const double v = fabs(a[r][k]);
+      if (pos[r] >= k && pos[r] != kNone && (bpos == kNone || v > best || (v == best && pos[r] < bpos))) {
+        best = v;
+        bpos = pos[r];
+      }
+    }
+    warp_pivot_reduce(best, bpos, kNone);
+    if (bpos == kNone || best == 0.0) {
+      if (lane == 0) report_failure(dp.status, u);
+      return;
+    }
+    const int p = bpos;
+    // Owner lane and row slot of the pivot row.
+    int oslot = -1;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (pos[r] == p) oslot = r;
+    const unsigned who = __ballot_sync(0xffffffffu, oslot >= 0);
+    const int olane = __ffs(who) - 1;
+    const int orow = __shfl_sync(0xffffffffu, oslot, olane);
+    if (lane == 0) piv[k] = p;
+    // Logical swap of positions k and p.
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      if (pos[r] == k) pos[r] = p;
+      else if (pos[r] == p) pos[r] = k;
+    }
+    const double pv = __shfl_sync(0xffffffffu, orow == 0 ? a[0][k] : a[R - 1][k], olane);
+    double l[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      l[r] = 0.0;
+      if (pos[r] > k && pos[r] != kNone) {
+        l[r] = __ddiv_rn(a[r][k], pv);
+        a[r][k] = l[r];
+      }
+    }
+#pragma unroll
+    for (int j = k + 1; j < M; ++j) {
+      if (j >= m) break;
+      const double uj = __shfl_sync(0xffffffffu, orow == 0 ? a[0][j] : a[R - 1][j], olane);
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        if (pos[r] > k && pos[r] != kNone) a[r][j] = __dsub_rn(a[r][j], __dmul_rn(l[r], uj));
+    }
+  }
+  double* out = dp.lu + dp.lu_off[u];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int row = lane + 32 * r;
+    if (row < m) {
+#pragma unroll
+      for (int j = 0; j < M; ++j)
+        if (j < m) out[static_cast<size_t>(j) * m + pos[r]] = a[r][j];
+      dp.lperm[s + pos[r]] = row;
+    }
+  }
+}
+
+constexpr int kWarpLuW1 = 4;  // units (warps) per CTA, up to 32 rows
+constexpr int kWarpLuW2 = 2;  // up to 64 rows
+
+// ---------------------------------------------------------------------------
 // Large units: value scatter into their (row-major) arena slots.
 // ---------------------------------------------------------------------------
 __global__ void k_scatter_large(DevPlan dp, const double* __restrict__ vals, const int32_t* __restrict__ units) {
@@ -641,6 +749,9 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
         attr_err = cudaFuncSetAttribute(k_lu_small<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_solve_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_lu_warp<2, kWarpLuW2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        kWarpLuW2 * 64 * 64 * static_cast<int>(sizeof(double)));
     });
     BDLU_CUDA(attr_err);
   }
@@ -678,17 +789,35 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
 void Engine::launch_lu_small(int threads, int32_t units, int32_t mb, cudaStream_t st, const double* d_vals,
                              const int32_t* list) {
   const size_t smem = static_cast<size_t>(mb) * mb * sizeof(double);
+  if (threads == 32 && mb <= 32) {
+    k_lu_warp<1, kWarpLuW1><<<(units + kWarpLuW1 - 1) / kWarpLuW1, 32 * kWarpLuW1, kWarpLuW1 * 32 * 32 * sizeof(double),
+                              st>>>(dp_, d_vals, list, units);
+    return;
+  }
+  if (threads == 32 && mb <= 64) {
+    k_lu_warp<2, kWarpLuW2><<<(units + kWarpLuW2 - 1) / kWarpLuW2, 32 * kWarpLuW2, kWarpLuW2 * 64 * 64 * sizeof(double),
+                              st>>>(dp_, d_vals, list, units);
+    return;
+  }
   if (threads == 64) k_lu_small<64><<<units, 64, smem, st>>>(dp_, d_vals, list);
   else if (threads == 128) k_lu_small<128><<<units, 128, smem, st>>>(dp_, d_vals, list);
   else k_lu_small<kThreads><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
 }
 
+// Admissible widths of a bucket of units up to mb rows: 32 (one warp per
+// unit, up to 64 rows), and CTA widths with one thread per row at least.
+static bool lu_width_ok(int t, int32_t mb) {
+  if (t == 32) return mb <= 64;
+  return (t == 64 || t == 128 || t == kThreads) && t >= mb;
+}
+
 int Engine::lu_small_width(int32_t mb) const {
-  // The kernel needs one thread per row for its first pivot scan (m <= CTA
-  // width).  Tuned choice, else the rule it replaces: narrow CTAs for small
-  // units (more units per SM, cheaper per-column barriers).
+  // A width forced for this engine, the tuned choice, else the default rule:
+  // narrow CTAs for small units (more units per SM, cheaper per-column
+  // barriers).
+  if (forced_lu_width_ != 0 && lu_width_ok(forced_lu_width_, mb)) return forced_lu_width_;
   const int t = Tuner::get().enabled() ? Tuner::get().lu_small_threads(mb) : 0;
-  if (t >= mb && (t == 64 || t == 128 || t == kThreads)) return t;
+  if (lu_width_ok(t, mb)) return t;
   return mb <= 32 ? 64 : (mb <= 64 ? 128 : kThreads);
 }
 
@@ -705,10 +834,10 @@ cudaError_t Engine::tune_lu_small(const double* d_vals, cudaStream_t stream) {
     if (tu.lu_small_threads(mb) != 0) continue;
     if (!e0 && ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess)) break;
     const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
-    int widths[3], count = 0;
-    for (int t : {64, 128, kThreads})
-      if (t >= mb) widths[count++] = t;
-    float ms[3] = {0.0f, 0.0f, 0.0f};
+    int widths[4], count = 0;
+    for (int t : {32, 64, 128, kThreads})
+      if (lu_width_ok(t, mb)) widths[count++] = t;
+    float ms[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     int best = widths[count - 1];
     float best_ms = 1e30f;
     for (int c = 0; c < count && e == cudaSuccess; ++c) {

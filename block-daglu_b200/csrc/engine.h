@@ -104,6 +104,9 @@ class Engine {
   // chain (panel and update launches on two graph branches), 1 one
   // persistent kernel over the tile task graph (when the plan has one).
   void set_refactor_schedule(int32_t s) { schedule_ = s; }
+  // Launch width of the shared-memory LU forced for this engine (32: one
+  // warp per unit; 64, 128, 256: threads per CTA; 0: the autotuner's).
+  void set_lu_small_width(int32_t t) { forced_lu_width_ = t; }
   // Bound of the waits between tiles (polls; <= 0 restores the default).
   // Captured graphs hold the old bound, so they are dropped.
   void set_wait_limit(int32_t polls) {
@@ -148,6 +151,7 @@ class Engine {
   void solve_core(const double* rhs, int32_t ldr, double* xp, const int32_t* nrhs, bool wide, cudaStream_t stream);
   void refine_core(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream);
   int32_t prec_ = 0;
+  int32_t forced_lu_width_ = 0;
   int32_t reuse_prec_ = 0;
   int32_t schedule_ = 0;
   int32_t reuse_schedule_ = 0;

@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import blockdaglu as bd
+import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -25,7 +26,7 @@ def test_tuner_picks_lu_small_widths(cuda_device, monkeypatch):
     widths = {e["bucket_m"]: e for e in rep["lu_small_threads"]}
     assert widths, rep
     for m, e in widths.items():
-        assert e["threads"] in (64, 128, 256) and e["threads"] >= m
+        assert (e["threads"] == 32 and m <= 64) or (e["threads"] in (64, 128, 256) and e["threads"] >= m)
         if "ms" in e:
             assert len(e["ms"]) == len(e["widths"]) and min(e["ms"]) > 0.0
             assert e["ms"][e["widths"].index(e["threads"])] == min(e["ms"])
@@ -62,3 +63,28 @@ def test_tuner_picks_refactor_schedule_per_pattern(cuda_device, monkeypatch):
     assert e["schedule"] in (0, 1) and e["ms_chain"] > 0.0 and e["ms_graph"] > 0.0
     assert e["schedule"] == (1 if e["ms_graph"] < e["ms_chain"] else 0)
     assert os.path.exists(rep["cache"])
+
+
+@pytest.mark.parametrize("width", [32, 64, 128, 256])
+def test_every_lu_width_bit_identical_to_oracle(cuda_device, monkeypatch, width):
+    """Each launch width of the shared-memory LU (32: one warp per unit, rows
+    in registers; 64 / 128 / 256 threads per unit) gives the reference
+    micro-kernel's factors and pivots bit for bit on every block of the
+    2,000-row block system (units of 10-90 rows; a bucket a width cannot take
+    runs the tuned width)."""
+    monkeypatch.delenv("BLOCKDAGLU_MODE", raising=False)
+    g = bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(0), 2000)
+    s = bd.Solver()
+    assert s.set_option("lu_small_threads", width)
+    assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze() and s.factor(), s.last_error_message()
+    d = s.decomposition()
+    ref = oracle.System(g.n, g.rows, g.cols, g.vals, d["P"], d["Q"], d["R"])
+    assert ref.factor()
+    R = d["R"]
+    for b in range(len(R) - 1):
+        lu, piv = s.block_lu(b)
+        lu_ref, piv_ref = ref.block_lu(b)
+        assert np.array_equal(piv, piv_ref) and np.array_equal(lu, lu_ref), (width, b, R[b + 1] - R[b])
+    x = g.b[:, 0].copy()
+    assert s.solve_in_place(x), s.last_error_message()
+    assert np.allclose(x, ref.solve(g.b[:, 0]), rtol=1e-9, atol=0.0)
