@@ -111,6 +111,7 @@ int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
   h->engine->set_lu_small_width(h->lu_small_threads);
+  h->engine->set_small_mode(h->small_mode);
   const int32_t sched = schedule_for(h);
   h->engine->set_refactor_schedule(sched);
   h->engine->set_wait_limit(h->wait_limit);
@@ -204,6 +205,7 @@ int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf*
     if (!h->engine) h->engine = std::make_unique<bdlu::Engine>();
     std::string err;
     if (!h->engine->upload(plan, h->dec, h->coo, err)) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+    h->engine->set_pattern_key(h->sig);
     // The engine keeps its own value buffer; load the analysed values.
     if (const int st = upload_values(h, h->coo.val.data(), false, nullptr)) return st;
   } catch (const std::bad_alloc&) {
@@ -266,6 +268,7 @@ int bdlu_device_restore(bdlu_solver* h) {
       h->engine.reset();
       return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
     }
+    h->engine->set_pattern_key(h->sig);
     if (const int st = upload_values(h, h->coo.val.data(), false, nullptr)) {
       h->engine.reset();
       return st;
@@ -480,6 +483,7 @@ int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nn
   const int tuned = schedule_tunable(h) ? Tuner::get().refactor_schedule(h->sig) : -1;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
   h->engine->set_lu_small_width(h->lu_small_threads);
+  h->engine->set_small_mode(h->small_mode);
   h->engine->set_refactor_schedule(tuned >= 0 ? tuned : h->refactor_schedule);
   h->engine->set_wait_limit(h->wait_limit);
   if (!h->engine->factor_async(h->engine->values_buffer(), s, err, h->reuse_pivots))
@@ -514,6 +518,7 @@ int bdlu_refactor_solve(bdlu_solver* h, const double* vals, int64_t nnz, double*
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
   h->engine->set_lu_small_width(h->lu_small_threads);
+  h->engine->set_small_mode(h->small_mode);
   const int32_t sched = schedule_for(h);
   h->engine->set_refactor_schedule(sched);
   h->engine->set_wait_limit(h->wait_limit);
@@ -634,6 +639,13 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
     if (value != 0.0 && value != 32.0 && value != 64.0 && value != 128.0 && value != 256.0)
       return BDLU_INVALID_DIMENSION;
     h->lu_small_threads = static_cast<int32_t>(value);
+    return BDLU_OK;
+  }
+  if (k == "small_launch") {
+    // Small units: -1 the autotuner's choice, 0 one launch per size bucket,
+    // 1 one persistent launch over a task queue.  Same factors either way.
+    if (value != -1.0 && value != 0.0 && value != 1.0) return BDLU_INVALID_DIMENSION;
+    h->small_mode = static_cast<int32_t>(value);
     return BDLU_OK;
   }
   if (k == "wait_limit") {

@@ -79,13 +79,11 @@ __device__ __forceinline__ void warp_pivot_signed(double v, int i, int none, dou
   bi = idx;
 }
 
+// One unit factored by the whole CTA (kT threads, kT >= m): A is the CTA's
+// m*m shared-memory slot.  A failed unit reports and returns (CTA-uniform).
 template <int kT>
-__global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __restrict__ vals,
-                                                  const int32_t* __restrict__ units) {
-  extern __shared__ double A[];
-  __shared__ double s_best[kT / 32], s_val[kT / 32];
-  __shared__ int s_bi[kT / 32];
-  const int u = units[blockIdx.x];
+__device__ __forceinline__ void lu_cta_unit(const DevPlan& dp, const double* __restrict__ vals, int u, double* A,
+                                            double* s_best, double* s_val, int* s_bi) {
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
   const int tid = threadIdx.x;
@@ -195,6 +193,15 @@ __global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __res
   for (int k = tid; k < m; k += kT) dp.lperm[s + k] = ord[k];
 }
 
+template <int kT>
+__global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __restrict__ vals,
+                                                  const int32_t* __restrict__ units) {
+  extern __shared__ double A[];
+  __shared__ double s_best[kT / 32], s_val[kT / 32];
+  __shared__ int s_bi[kT / 32];
+  lu_cta_unit<kT>(dp, vals, units[blockIdx.x], A, s_best, s_val, s_bi);
+}
+
 // ---------------------------------------------------------------------------
 // Column-warp LU: one warp per unit of up to 32*R rows (the C2 "column-warp"
 // path), several units per CTA, no CTA barriers.  Lane l holds rows l,
@@ -205,19 +212,16 @@ __global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __res
 // first strict maximum of |a| (ties to the smallest position), multipliers by
 // division, a - l*u as multiply then subtract; so the factors, pivots and row
 // order are bit-identical to k_lu_small's.
-template <int R, int W>
-__global__ void __launch_bounds__(32 * W) k_lu_warp(DevPlan dp, const double* __restrict__ vals,
-                                                    const int32_t* __restrict__ units, int32_t count) {
+// One unit of up to 32*R rows factored by one warp; S is the warp's
+// (32R)^2-double shared-memory staging slot.  A failed unit reports and
+// returns (warp-uniform).
+template <int R>
+__device__ __forceinline__ void lu_warp_unit(const DevPlan& dp, const double* __restrict__ vals, int u, double* S) {
   constexpr int M = 32 * R;
   constexpr int kNone = 1 << 20;  // position of rows outside the unit
-  extern __shared__ double wsm[];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int slot = blockIdx.x * W + wib;
-  if (slot >= count) return;  // warp-uniform
-  const int u = units[slot];
+  const int lane = threadIdx.x & 31;
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
-  double* S = wsm + static_cast<size_t>(wib) * M * M;  // staging, column-major, ld m
   for (int i = lane; i < m * m; i += 32) S[i] = 0.0;
   __syncwarp();
   for (int64_t e = dp.dent_ptr[u] + lane; e < dp.dent_ptr[u + 1]; e += 32) S[dp.dent_pos[e]] = vals[dp.dent_src[e]];
@@ -297,6 +301,48 @@ __global__ void __launch_bounds__(32 * W) k_lu_warp(DevPlan dp, const double* __
         if (j < m) out[static_cast<size_t>(j) * m + pos[r]] = a[r][j];
       dp.lperm[s + pos[r]] = row;
     }
+  }
+}
+
+template <int R, int W>
+__global__ void __launch_bounds__(32 * W) k_lu_warp(DevPlan dp, const double* __restrict__ vals,
+                                                    const int32_t* __restrict__ units, int32_t count) {
+  extern __shared__ double wsm[];
+  const int wib = threadIdx.x >> 5;
+  const int slot = blockIdx.x * W + wib;
+  if (slot >= count) return;  // warp-uniform
+  lu_warp_unit<R>(dp, vals, units[slot], wsm + static_cast<size_t>(wib) * (32 * R) * (32 * R));
+}
+
+// Every small unit of the pattern in one persistent launch: each CTA takes
+// tasks from a device queue (atomic ticket) until it is empty.  A task is one
+// unit for the whole CTA (more than 32 rows) or a pack of up to eight units of
+// at most 32 rows, one per warp (column-warp path).  Tasks come largest first
+// (host-built list: first unit, unit count; count > 0 marks a pack).  Shared
+// memory: the largest task's need.
+constexpr int kQueueThreads = 256;
+__global__ void __launch_bounds__(kQueueThreads) k_lu_queue(DevPlan dp, const double* __restrict__ vals,
+                                                            const int32_t* __restrict__ units,
+                                                            const int2* __restrict__ tasks, int32_t ntasks,
+                                                            int32_t* __restrict__ ticket) {
+  extern __shared__ double qsm[];
+  __shared__ double s_best[kQueueThreads / 32], s_val[kQueueThreads / 32];
+  __shared__ int s_bi[kQueueThreads / 32];
+  __shared__ int s_t;
+  const int warp = threadIdx.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) s_t = atomicAdd(ticket, 1);
+    __syncthreads();
+    const int t = s_t;
+    __syncthreads();
+    if (t >= ntasks) break;
+    const int2 task = tasks[t];
+    if (task.y == 0) {
+      lu_cta_unit<kQueueThreads>(dp, vals, units[task.x], qsm, s_best, s_val, s_bi);
+    } else if (warp < task.y) {
+      lu_warp_unit<1>(dp, vals, units[task.x + warp], qsm + static_cast<size_t>(warp) * 32 * 32);
+    }
+    __syncthreads();
   }
 }
 
@@ -654,6 +700,9 @@ void Engine::release() {
   d_rtask_ = nullptr;
   d_rwords_ = nullptr;
   d_vals_stage_ = nullptr;
+  d_qunits_ = d_qtasks_ = nullptr;
+  d_qticket_ = nullptr;
+  queue_tasks_ = 0;
   work_nrhs_ = 0;
   dp_ = DevPlan{};
 }
@@ -752,6 +801,8 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_lu_warp<2, kWarpLuW2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         kWarpLuW2 * 64 * 64 * static_cast<int>(sizeof(double)));
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_lu_queue, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
     });
     BDLU_CUDA(attr_err);
   }
@@ -781,6 +832,43 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   }
   small_list_ = small_list;
   large_list_ = large_list;
+  // Task queue of the one-launch small-unit LU: units largest first; units of
+  // more than 32 rows one task each, smaller ones in packs of eight.
+  queue_tasks_ = 0;
+  if (!plan.small_units.empty()) {
+    std::vector<int32_t> qunits(plan.small_units.rbegin(), plan.small_units.rend());
+    std::vector<int32_t> qtasks;
+    int64_t smem = 0;
+    size_t i = 0;
+    while (i < qunits.size()) {
+      const int32_t u = qunits[i];
+      const int32_t m = plan.ustart[static_cast<size_t>(u) + 1] - plan.ustart[static_cast<size_t>(u)];
+      if (m > 32) {
+        qtasks.push_back(static_cast<int32_t>(i));
+        qtasks.push_back(0);
+        smem = std::max<int64_t>(smem, static_cast<int64_t>(m) * m * 8);
+        ++i;
+      } else {
+        const size_t cnt = std::min<size_t>(8, qunits.size() - i);
+        qtasks.push_back(static_cast<int32_t>(i));
+        qtasks.push_back(static_cast<int32_t>(cnt));
+        smem = std::max<int64_t>(smem, 8 * 32 * 32 * 8);
+        i += cnt;
+      }
+    }
+    const int32_t* qu = nullptr;
+    const int32_t* qt = nullptr;
+    if (!upload_vec(allocs_, qunits, &qu, err)) return false;
+    if (!upload_vec(allocs_, qtasks, &qt, err)) return false;
+    if (!alloc_dev(allocs_, 1, &d_qticket_, err)) return false;
+    d_qunits_ = qu;
+    d_qtasks_ = qt;
+    queue_tasks_ = static_cast<int32_t>(qtasks.size() / 2);
+    queue_smem_ = static_cast<size_t>(smem);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_lu_queue, kQueueThreads, queue_smem_);
+    queue_grid_ = std::max(1, std::min(queue_tasks_, num_sms_ * std::max(1, per_sm)));
+  }
   lvl_scalar_ = lvl_scalar;
   lvl_dense_ = lvl_dense;
   return true;
@@ -859,6 +947,72 @@ cudaError_t Engine::tune_lu_small(const double* d_vals, cudaStream_t stream) {
   return e == cudaSuccess ? cudaGetLastError() : e;
 }
 
+// The shared-memory LU of every small unit as one launch per size bucket
+// (shared memory sized to the bucket), the buckets side by side on the
+// auxiliary streams (forked from and joined back into `stream`), largest
+// units first.
+cudaError_t Engine::launch_small_buckets(const double* d_vals, cudaStream_t stream) {
+  const Plan& p = plan_;
+  cudaError_t e = cudaEventRecord(fork_ev_[0], stream);
+  const size_t nbk = p.small_bucket_m.size();
+  for (size_t q = 0; q < nbk && e == cudaSuccess; ++q) {
+    const size_t bkt = nbk - 1 - q;
+    cudaStream_t sb = aux_[q % kAux];
+    if (q < static_cast<size_t>(kAux)) e = cudaStreamWaitEvent(sb, fork_ev_[0], 0);
+    const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
+    const int32_t mb = p.small_bucket_m[bkt];
+    launch_lu_small(lu_small_width(mb), q1 - q0, mb, sb, d_vals, small_list_ + q0);
+  }
+  for (int q = 0; q < kAux && q < static_cast<int>(nbk) && e == cudaSuccess; ++q) {
+    e = cudaEventRecord(aux_ev_[q], aux_[q]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, aux_ev_[q], 0);
+  }
+  return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
+// The same factors in one persistent launch over the task queue (k_lu_queue).
+cudaError_t Engine::launch_small_queue(const double* d_vals, cudaStream_t stream) {
+  cudaError_t e = cudaMemsetAsync(d_qticket_, 0, sizeof(int32_t), stream);
+  if (e != cudaSuccess) return e;
+  k_lu_queue<<<queue_grid_, kQueueThreads, queue_smem_, stream>>>(dp_, d_vals, d_qunits_,
+                                                                 reinterpret_cast<const int2*>(d_qtasks_),
+                                                                 queue_tasks_, d_qticket_);
+  return cudaGetLastError();
+}
+
+// 0: per-bucket launches, 1: one persistent launch; forced for this engine,
+// tuned for its pattern, else per-bucket.
+int Engine::small_mode() const {
+  if (queue_tasks_ <= 0) return 0;
+  if (forced_small_mode_ >= 0) return forced_small_mode_;
+  const int t = Tuner::get().enabled() ? Tuner::get().small_mode(pattern_key_) : -1;
+  return t == 1 ? 1 : 0;
+}
+
+// Times both ways of launching the small units on this pattern (after the
+// widths are tuned) once per pattern signature; both write the same factors.
+cudaError_t Engine::tune_small_mode(const double* d_vals, cudaStream_t stream) {
+  Tuner& tu = Tuner::get();
+  if (forced_small_mode_ >= 0 || queue_tasks_ <= 0 || tu.small_mode(pattern_key_) >= 0) return cudaSuccess;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  float ms[2] = {0.0f, 0.0f};
+  for (int mode = 0; mode < 2 && e == cudaSuccess; ++mode) {
+    for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
+      if (rep == 1) e = cudaEventRecord(e0, stream);
+      if (e == cudaSuccess) e = mode == 0 ? launch_small_buckets(d_vals, stream) : launch_small_queue(d_vals, stream);
+      if (rep == 1 && e == cudaSuccess) e = cudaEventRecord(e1, stream);
+    }
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms[mode], e0, e1);
+  }
+  if (e == cudaSuccess) tu.set_small_mode(pattern_key_, ms[1] < ms[0] ? 1 : 0, ms[0], ms[1]);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  return e;
+}
+
 bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string& err, bool reuse_pivots) {
   const Plan& p = plan_;
   const bool reuse = reuse_pivots && have_pivots_ && !p.large_units.empty();
@@ -876,22 +1030,17 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
     // Tuning waits for its timing events: never inside a caller's capture.
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     BDLU_CUDA(cudaStreamIsCapturing(stream, &cap));
-    if (cap == cudaStreamCaptureStatusNone) BDLU_CUDA(tune_lu_small(d_vals, stream));
+    if (cap == cudaStreamCaptureStatusNone) {
+      BDLU_CUDA(tune_lu_small(d_vals, stream));
+      BDLU_CUDA(tune_small_mode(d_vals, stream));
+    }
   }
   if (!p.small_bucket_m.empty()) {
-    BDLU_CUDA(cudaEventRecord(fork_ev_[0], stream));
-    const size_t nbk = p.small_bucket_m.size();
-    for (size_t q = 0; q < nbk; ++q) {
-      const size_t bkt = nbk - 1 - q;
-      cudaStream_t sb = aux_[q % kAux];
-      if (q < static_cast<size_t>(kAux)) BDLU_CUDA(cudaStreamWaitEvent(sb, fork_ev_[0], 0));
-      const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
-      const int32_t mb = p.small_bucket_m[bkt];
-      launch_lu_small(lu_small_width(mb), q1 - q0, mb, sb, d_vals, small_list_ + q0);
-    }
-    for (int q = 0; q < kAux && q < static_cast<int>(nbk); ++q) {
-      BDLU_CUDA(cudaEventRecord(aux_ev_[q], aux_[q]));
-      BDLU_CUDA(cudaStreamWaitEvent(stream, aux_ev_[q], 0));
+    if (small_mode() == 1) {
+      BDLU_CUDA(launch_small_queue(d_vals, stream));
+      launches_factor_ = 2;
+    } else {
+      BDLU_CUDA(launch_small_buckets(d_vals, stream));
     }
   }
   BDLU_CUDA(cudaEventRecord(pev_[1], stream));

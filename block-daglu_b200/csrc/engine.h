@@ -107,6 +107,11 @@ class Engine {
   // Launch width of the shared-memory LU forced for this engine (32: one
   // warp per unit; 64, 128, 256: threads per CTA; 0: the autotuner's).
   void set_lu_small_width(int32_t t) { forced_lu_width_ = t; }
+  // Small units as per-bucket launches (0) or one persistent launch over a
+  // task queue (1); -1: the autotuner's choice for the pattern.
+  void set_small_mode(int32_t m) { forced_small_mode_ = m; }
+  // Pattern signature under which the autotuner keeps this engine's choices.
+  void set_pattern_key(uint64_t k) { pattern_key_ = k; }
   // Bound of the waits between tiles (polls; <= 0 restores the default).
   // Captured graphs hold the old bound, so they are dropped.
   void set_wait_limit(int32_t polls) {
@@ -148,6 +153,18 @@ class Engine {
                        const int32_t* list);
   int lu_small_width(int32_t mb) const;
   cudaError_t tune_lu_small(const double* d_vals, cudaStream_t stream);
+  cudaError_t launch_small_buckets(const double* d_vals, cudaStream_t stream);
+  cudaError_t launch_small_queue(const double* d_vals, cudaStream_t stream);
+  int small_mode() const;
+  cudaError_t tune_small_mode(const double* d_vals, cudaStream_t stream);
+  int32_t forced_small_mode_ = -1;
+  uint64_t pattern_key_ = 0;
+  const int32_t* d_qunits_ = nullptr;  // small units, largest first
+  const int32_t* d_qtasks_ = nullptr;  // (first, count) per task
+  int32_t* d_qticket_ = nullptr;
+  int32_t queue_tasks_ = 0;
+  int queue_grid_ = 1;
+  size_t queue_smem_ = 0;
   void solve_core(const double* rhs, int32_t ldr, double* xp, const int32_t* nrhs, bool wide, cudaStream_t stream);
   void refine_core(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream);
   int32_t prec_ = 0;

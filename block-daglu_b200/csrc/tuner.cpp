@@ -34,6 +34,7 @@ struct ScheduleChoice {
 std::mutex g_mu;
 std::map<int32_t, SmallChoice> g_small;
 std::map<uint64_t, ScheduleChoice> g_sched;
+std::map<uint64_t, ScheduleChoice> g_mode;  // small-unit launch mode (0 buckets, 1 queue) and both times
 
 std::string sanitize(const std::string& s) {
   std::string out;
@@ -87,8 +88,21 @@ void Tuner::load() {
   for (size_t p = t.find("\"bucket_m\":"); p != std::string::npos; p = t.find("\"bucket_m\":", p + 1)) {
     int m = 0, th = 0;
     if (std::sscanf(t.c_str() + p, "\"bucket_m\": %d, \"threads\": %d", &m, &th) == 2 && m > 0 &&
-        (th == 64 || th == 128 || th == 256))
+        (th == 32 || th == 64 || th == 128 || th == 256))
       g_small[m].threads = th;
+  }
+  for (size_t p = t.find("\"mode_sig\":"); p != std::string::npos; p = t.find("\"mode_sig\":", p + 1)) {
+    unsigned long long sig = 0;
+    int mode = -1;
+    float a = 0.0f, b = 0.0f;
+    if (std::sscanf(t.c_str() + p, "\"mode_sig\": \"%llx\", \"mode\": %d, \"ms_buckets\": %f, \"ms_queue\": %f",
+                    &sig, &mode, &a, &b) >= 2 &&
+        (mode == 0 || mode == 1)) {
+      ScheduleChoice& c = g_mode[static_cast<uint64_t>(sig)];
+      c.schedule = mode;
+      c.ms_chain = a;
+      c.ms_graph = b;
+    }
   }
   for (size_t p = t.find("\"sig\":"); p != std::string::npos; p = t.find("\"sig\":", p + 1)) {
     unsigned long long sig = 0;
@@ -132,6 +146,15 @@ std::string Tuner::report() {
       << ", \"ms_chain\": " << kv.second.ms_chain << ", \"ms_graph\": " << kv.second.ms_graph << "}";
     first = false;
   }
+  o << "],\n \"small_mode\": [";
+  first = true;
+  for (const auto& kv : g_mode) {
+    char sig[32];
+    std::snprintf(sig, sizeof(sig), "%016" PRIx64, kv.first);
+    o << (first ? "\n  " : ",\n  ") << "{\"mode_sig\": \"" << sig << "\", \"mode\": " << kv.second.schedule
+      << ", \"ms_buckets\": " << kv.second.ms_chain << ", \"ms_queue\": " << kv.second.ms_graph << "}";
+    first = false;
+  }
   o << "]}\n";
   return o.str();
 }
@@ -161,6 +184,23 @@ void Tuner::set_lu_small_threads(int32_t bucket_m, int threads, const float* ms,
     c.threads = threads;
     c.widths.assign(widths, widths + count);
     c.ms.assign(ms, ms + count);
+  }
+  write_file(path_, report());
+}
+
+int Tuner::small_mode(uint64_t sig) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  const auto it = g_mode.find(sig);
+  return it == g_mode.end() ? -1 : it->second.schedule;
+}
+
+void Tuner::set_small_mode(uint64_t sig, int mode, float ms_buckets, float ms_queue) {
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    ScheduleChoice& c = g_mode[sig];
+    c.schedule = mode;
+    c.ms_chain = ms_buckets;
+    c.ms_graph = ms_queue;
   }
   write_file(path_, report());
 }

@@ -88,3 +88,32 @@ def test_every_lu_width_bit_identical_to_oracle(cuda_device, monkeypatch, width)
     x = g.b[:, 0].copy()
     assert s.solve_in_place(x), s.last_error_message()
     assert np.allclose(x, ref.solve(g.b[:, 0]), rtol=1e-9, atol=0.0)
+
+
+@pytest.mark.parametrize("family,n", [(bd.FAMILY_BLOCK, 2000), (bd.FAMILY_CIRCUIT, 20000)])
+def test_one_launch_queue_bit_identical_to_oracle(cuda_device, monkeypatch, family, n):
+    """All small units in one persistent launch over a task queue (whole-CTA
+    tasks for units above 32 rows, packs of eight warp tasks below) give the
+    same factors as the per-bucket launches and the reference micro-kernel."""
+    monkeypatch.delenv("BLOCKDAGLU_MODE", raising=False)
+    g = bd.Synth(family, bd.config_seed(0 if family == bd.FAMILY_BLOCK else 1, 52), n)
+    sols = []
+    for mode in (1, 0):
+        s = bd.Solver()
+        assert s.set_option("small_launch", mode)
+        assert s.set_matrix((g.rows, g.cols, g.vals), g.n) and s.analyze() and s.factor(), s.last_error_message()
+        sols.append(s)
+    d = sols[0].decomposition()
+    ref = oracle.System(g.n, g.rows, g.cols, g.vals, d["P"], d["Q"], d["R"])
+    assert ref.factor()
+    R = d["R"]
+    for b in range(len(R) - 1):
+        if R[b + 1] - R[b] > 169:
+            continue  # large units: not on this path
+        lu_q, piv_q = sols[0].block_lu(b)
+        lu_b, piv_b = sols[1].block_lu(b)
+        lu_ref, piv_ref = ref.block_lu(b)
+        assert np.array_equal(piv_q, piv_ref) and np.array_equal(lu_q, lu_ref), b
+        assert np.array_equal(piv_b, piv_ref) and np.array_equal(lu_b, lu_ref), b
+    x = g.b[:, 0].copy()
+    assert sols[0].solve_in_place(x), sols[0].last_error_message()
