@@ -336,9 +336,12 @@ int bdlu_matrix_signatures(const bdlu_solver* h, uint64_t* sigs);
  * No counterpart in the reference (it tunes by environment knobs,
  * blockdaglu/src/ubtf_block_solver.cpp:35-568).  The engine times its
  * launch-shape and schedule candidates on the GPU it runs on and keeps the
- * faster (every candidate computes bit-identical results): the CTA width of
- * the shared-memory LU per size bucket, and per pattern signature the
- * value-only refactor schedule of large units (step chain or tile task graph,
+ * faster (every candidate computes bit-identical results): the width of the
+ * shared-memory LU per size bucket (one warp per unit, or 64 / 128 / 256
+ * threads per unit), per pattern signature the small units as per-bucket
+ * launches or as one persistent launch over a task queue, and per pattern
+ * signature the value-only refactor schedule of large units (step chain or
+ * tile task graph,
  * decided over the pattern's first four refactors that wait for their
  * status).  Choices persist in $BDLU_TUNE_CACHE, else
  * $HOME/.cache/bdlu/tune-<gpu>.json; BDLU_AUTOTUNE=0 disables tuning.
