@@ -137,6 +137,23 @@ int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
 // True if no entry is NaN or infinite: branch-free over the whole array (no
 // early exit, so the loop vectorises).  One thread: helper threads lost to
 // busy OpenMP workers of the calling process in measurements.
+bool all_finite(const double* v, int64_t n);
+
+}  // namespace
+
+bool bdlu_copy_finite(double* dst, const double* src, int64_t n) {
+  uint64_t bad = 0;
+  for (int64_t k = 0; k < n; ++k) {
+    uint64_t x;
+    std::memcpy(&x, src + k, sizeof(x));
+    bad |= static_cast<uint64_t>(((x >> 52) & 0x7ff) == 0x7ff);
+    std::memcpy(dst + k, &x, sizeof(x));
+  }
+  return bad == 0;
+}
+
+namespace {
+
 bool all_finite(const double* v, int64_t n) {
   uint64_t bad = 0;
   for (int64_t k = 0; k < n; ++k) {
@@ -222,14 +239,14 @@ int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf*
 // buffers) and move to the value buffer only if every entry is finite.  No
 // host copy is kept (10 MB per million entries): coo.val is refreshed from
 // the device when something reads it.
-static int stage_host_values(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream) {
+static int stage_host_values(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream, bool checked) {
   std::string err;
   double* stg = h->engine->value_staging(err);
   if (!stg) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
   const size_t bytes = static_cast<size_t>(nnz) * sizeof(double);
   cudaError_t e = cudaMemcpyAsync(stg, vals, bytes, cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return fail(h, BDLU_BACKEND_UNAVAILABLE, std::string("value upload: ") + cudaGetErrorString(e));
-  if (!all_finite(vals, nnz)) {
+  if (!checked && !all_finite(vals, nnz)) {
     cudaStreamSynchronize(stream);  // the staging copy ends before the error returns
     return fail(h, BDLU_NON_FINITE_VALUE, "matrix contains NaN or infinity");
   }
@@ -248,9 +265,9 @@ static int refactor_checks(bdlu_solver* h, const double* vals, int64_t nnz) {
   return BDLU_OK;
 }
 
-int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream) {
+int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream, bool checked) {
   if (const int st = refactor_checks(h, vals, nnz)) return st;
-  if (const int st = stage_host_values(h, vals, nnz, stream)) return st;
+  if (const int st = stage_host_values(h, vals, nnz, stream, checked)) return st;
   return do_factor(h, stream, h->reuse_pivots);
 }
 
@@ -307,12 +324,13 @@ int bdlu_refactor_values_device_on(bdlu_solver* h, const double* d_vals, int64_t
   return do_factor(h, stream, h->reuse_pivots);
 }
 
-int bdlu_solve_checked_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream, bool device) {
+int bdlu_solve_checked_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream, bool device,
+                          bool checked) {
   if (!h) return BDLU_NOT_PREPARED;
   clear_error(h);
   if (!h->factored) return fail(h, BDLU_NOT_PREPARED, "factor must succeed before solve");
   if (!B || nrhs < 1 || ldb < h->n) return fail(h, BDLU_INVALID_RHS, "right-hand side size does not match matrix dimension");
-  if (!device)
+  if (!device && !checked)
     for (int32_t k = 0; k < nrhs; ++k)
       if (!all_finite(B + static_cast<size_t>(k) * ldb, h->n))
         return fail(h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
@@ -514,7 +532,7 @@ int bdlu_refactor_solve(bdlu_solver* h, const double* vals, int64_t nnz, double*
   // status after its first sweep and redoes a refactor whose reused pivot
   // order met a zero pivot (with pivoting), or reports a zero pivot.
   if (const int st = refactor_checks(h, vals, nnz)) return st;
-  if (const int st = stage_host_values(h, vals, nnz, nullptr)) return st;
+  if (const int st = stage_host_values(h, vals, nnz, nullptr, false)) return st;
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
   h->engine->set_lu_small_width(h->lu_small_threads);

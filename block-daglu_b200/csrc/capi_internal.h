@@ -79,15 +79,22 @@ int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf*
 // Host-buffer refactor and solve on a given stream (the C ABI's host-buffer
 // calls use the legacy default stream).  Same checks, fallbacks and
 // synchronisation as bdlu_refactor_values / bdlu_solve.
-int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream);
+// `checked`: the caller has already checked the values for NaN and infinity
+// (bdlu_copy_finite while staging them), so no second pass is made.
+int bdlu_refactor_values_on(bdlu_solver* h, const double* vals, int64_t nnz, cudaStream_t stream,
+                            bool checked = false);
 int bdlu_solve_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream);
+
+// Copies n doubles and reports whether all are finite, in one pass.
+bool bdlu_copy_finite(double* dst, const double* src, int64_t n);
 
 // The same two steps with the values and right-hand sides in device memory
 // (the serving loop's device-resident requests): no host finiteness check;
 // the solve still reads the residual and status and applies the fallbacks,
 // and returns with B overwritten on the device and `stream` synchronised.
 int bdlu_refactor_values_device_on(bdlu_solver* h, const double* d_vals, int64_t nnz, cudaStream_t stream);
-int bdlu_solve_checked_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream, bool device);
+int bdlu_solve_checked_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, cudaStream_t stream, bool device,
+                          bool checked = false);
 
 // Brings coo.val up to date from the engine's value buffer after refactors
 // that skipped the host copy (synchronises the device).  Returns a status

@@ -185,14 +185,21 @@ void worker(bdlu_server* s) {
       double* sv = vstage.get(static_cast<size_t>(p.nnz));
       double* sb = bstage.get(nb);
       if (st == BDLU_OK && (!sv || !sb)) st = -1;
+      // One pass per input: the copy into page-locked staging checks for
+      // NaN and infinity on the way; the checks fail the request where
+      // bdlu_refactor_solve's would (values before the refactor, right-hand
+      // sides after it).
+      bool finite_b = true;
       if (st == BDLU_OK) {
-        std::copy(r->vals, r->vals + p.nnz, sv);
-        for (int32_t k = 0; k < r->nrhs; ++k)
-          std::copy(r->B + static_cast<size_t>(k) * r->ldb, r->B + static_cast<size_t>(k) * r->ldb + p.n,
-                    sb + static_cast<size_t>(k) * p.n);
-        st = bdlu_refactor_values_on(p.h, sv, p.nnz, stream);
+        if (!bdlu_copy_finite(sv, r->vals, p.nnz))
+          st = bdlu_fail(p.h, BDLU_NON_FINITE_VALUE, "matrix contains NaN or infinity");
+        for (int32_t k = 0; k < r->nrhs && st == BDLU_OK; ++k)
+          finite_b &= bdlu_copy_finite(sb + static_cast<size_t>(k) * p.n, r->B + static_cast<size_t>(k) * r->ldb, p.n);
+        if (st == BDLU_OK) st = bdlu_refactor_values_on(p.h, sv, p.nnz, stream, true);
       }
-      if (st == BDLU_OK) st = bdlu_solve_on(p.h, sb, p.n, r->nrhs, stream);
+      if (st == BDLU_OK && !finite_b)
+        st = bdlu_fail(p.h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
+      if (st == BDLU_OK) st = bdlu_solve_checked_on(p.h, sb, p.n, r->nrhs, stream, false, true);
       if (st == BDLU_OK)
         for (int32_t k = 0; k < r->nrhs; ++k)
           std::copy(sb + static_cast<size_t>(k) * p.n, sb + static_cast<size_t>(k + 1) * p.n,
