@@ -161,3 +161,27 @@ def test_server_device_resident_requests_match_host_requests(cuda_device):
             if prec == 0:
                 assert np.allclose(X, xh, rtol=1e-12, atol=0.0)
         s.close()
+
+
+@pytest.mark.gpu
+def test_server_rejects_non_finite_inputs(cuda_device):
+    """NaN or infinity in a request's values or right-hand sides fails that
+    request with NonFiniteValue (the check runs while the inputs are staged);
+    the pattern keeps serving."""
+    g = bd.Synth(bd.FAMILY_CIRCUIT, bd.config_seed(4, 11), 6000)
+    s = bd.Server(8 << 30, 2)
+    k = s.add_pattern((g.rows, g.cols, g.vals), g.n)
+    v = g.vals.copy()
+    v[7] = np.nan
+    X = np.ones(g.n)
+    ok, _, _ = s.wait(s.submit(k, v, X))
+    assert not ok and s.last_error() == bd.SolverError.NonFiniteValue
+    X = np.ones(g.n)
+    X[3] = np.inf
+    ok, _, _ = s.wait(s.submit(k, g.vals, X))
+    assert not ok and s.last_error() == bd.SolverError.NonFiniteValue
+    B = g.b[:, 0].copy()
+    ok, resid, _ = s.wait(s.submit(k, g.vals, B))
+    assert ok and resid <= 1e-12
+    assert _relres(g, g.vals, B, g.b[:, 0]) <= 1e-12
+    s.close()
