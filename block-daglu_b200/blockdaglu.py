@@ -60,6 +60,7 @@ class ServerStats(ctypes.Structure):
         ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
         ("throughput", ctypes.c_double), ("resident_bytes", ctypes.c_int64), ("evictions", ctypes.c_int64),
         ("peak_concurrency", ctypes.c_int32), ("kernel_launches", ctypes.c_int64), ("factor_flops", ctypes.c_double),
+        ("mean_stage_ms", ctypes.c_double), ("mean_factor_ms", ctypes.c_double), ("mean_solve_ms", ctypes.c_double),
     ]
 
     def as_dict(self):

@@ -892,6 +892,17 @@ void Engine::launch_lu_small(int threads, int32_t units, int32_t mb, cudaStream_
   else k_lu_small<kThreads><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
 }
 
+// The autotuner keeps one width per size class (the bucket cuts of the plan
+// and the shared-memory limit), so buckets whose largest unit differs by a
+// row share a choice.  Widths are still checked against the bucket's own mb.
+static int32_t lu_bucket_class(int32_t mb) {
+  static const int32_t kClass[] = {8, 16, 24, 32, 48, 64, 80, 96, 128};
+  static const int32_t kMax = small_unit_max();
+  for (int32_t c : kClass)
+    if (mb <= c) return c;
+  return kMax;
+}
+
 // Admissible widths of a bucket of units up to mb rows: 32 (one warp per
 // unit, up to 64 rows), and CTA widths with one thread per row at least.
 static bool lu_width_ok(int t, int32_t mb) {
@@ -904,7 +915,7 @@ int Engine::lu_small_width(int32_t mb) const {
   // narrow CTAs for small units (more units per SM, cheaper per-column
   // barriers).
   if (forced_lu_width_ != 0 && lu_width_ok(forced_lu_width_, mb)) return forced_lu_width_;
-  const int t = Tuner::get().enabled() ? Tuner::get().lu_small_threads(mb) : 0;
+  const int t = Tuner::get().enabled() ? Tuner::get().lu_small_threads(lu_bucket_class(mb)) : 0;
   if (lu_width_ok(t, mb)) return t;
   return mb <= 32 ? 64 : (mb <= 64 ? 128 : kThreads);
 }
@@ -919,7 +930,7 @@ cudaError_t Engine::tune_lu_small(const double* d_vals, cudaStream_t stream) {
   cudaError_t e = cudaSuccess;
   for (size_t bkt = 0; bkt < p.small_bucket_m.size() && e == cudaSuccess; ++bkt) {
     const int32_t mb = p.small_bucket_m[bkt];
-    if (tu.lu_small_threads(mb) != 0) continue;
+    if (tu.lu_small_threads(lu_bucket_class(mb)) != 0) continue;
     if (!e0 && ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess)) break;
     const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
     int widths[4], count = 0;
@@ -940,7 +951,7 @@ cudaError_t Engine::tune_lu_small(const double* d_vals, cudaStream_t stream) {
         best = widths[c];
       }
     }
-    if (e == cudaSuccess) tu.set_lu_small_threads(mb, best, ms, widths, count);
+    if (e == cudaSuccess) tu.set_lu_small_threads(lu_bucket_class(mb), best, ms, widths, count);
   }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);

@@ -82,6 +82,7 @@ struct bdlu_server {
   int64_t completed = 0, failed = 0;
   int64_t kernel_launches = 0;
   double factor_flops = 0.0;
+  double stage_ms = 0.0, factor_ms = 0.0, solve_ms = 0.0;  // worker wall time per phase, summed
   std::string last_message;
   int last_error = BDLU_OK;
   double precision = 0.0;  // "precision" option of every pattern's handle
@@ -174,11 +175,15 @@ void worker(bdlu_server* s) {
     }
     Pattern& p = *pp;
     int st = BDLU_OK;
+    const double t_start = now_ms();
+    double t_staged = t_start, t_factored = t_start;
     const int64_t reserved = p.bytes;
     if (!bdlu_engine_ready(p.h)) st = bdlu_device_restore(p.h);
     if (r->device) {
       // Device-resident request: values and right-hand sides never leave HBM.
+      t_staged = now_ms();
       if (st == BDLU_OK) st = bdlu_refactor_values_device_on(p.h, r->vals, p.nnz, stream);
+      t_factored = now_ms();
       if (st == BDLU_OK) st = bdlu_solve_checked_on(p.h, r->B, r->ldb, r->nrhs, stream, true);
     } else {
       const size_t nb = static_cast<size_t>(p.n) * static_cast<size_t>(r->nrhs);
@@ -195,8 +200,10 @@ void worker(bdlu_server* s) {
           st = bdlu_fail(p.h, BDLU_NON_FINITE_VALUE, "matrix contains NaN or infinity");
         for (int32_t k = 0; k < r->nrhs && st == BDLU_OK; ++k)
           finite_b &= bdlu_copy_finite(sb + static_cast<size_t>(k) * p.n, r->B + static_cast<size_t>(k) * r->ldb, p.n);
+        t_staged = now_ms();
         if (st == BDLU_OK) st = bdlu_refactor_values_on(p.h, sv, p.nnz, stream, true);
       }
+      t_factored = now_ms();
       if (st == BDLU_OK && !finite_b)
         st = bdlu_fail(p.h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
       if (st == BDLU_OK) st = bdlu_solve_checked_on(p.h, sb, p.n, r->nrhs, stream, false, true);
@@ -230,6 +237,9 @@ void worker(bdlu_server* s) {
       r->done = true;
       --s->running;
       s->kernel_launches += static_cast<int64_t>(stats.factor_launches) + stats.solve_launches;
+      s->stage_ms += t_staged - t_start;
+      s->factor_ms += t_factored - t_staged;
+      s->solve_ms += now_ms() - t_factored;
       if (st == BDLU_OK) {
         s->factor_flops += stats.factor_flops;
         ++s->completed;
@@ -300,6 +310,11 @@ int32_t bdlu_server_add_pattern(bdlu_server* s, const int32_t* rows, const int32
   if (st == BDLU_OK) st = bdlu_set_option(p->h, "analysis_only", 1);
   if (st == BDLU_OK) st = bdlu_analyze(p->h);
   if (st == BDLU_OK) st = bdlu_set_option(p->h, "analysis_only", 0);
+  // The step chain for every served pattern: the tile task graph's
+  // persistent kernel waits on its own tiles, and with other requests'
+  // kernels on the GPU its CTAs lose the SMs they wait for (measured: tens of
+  // milliseconds to seconds per refactor while the chain takes a few).
+  if (st == BDLU_OK) st = bdlu_set_option(p->h, "refactor_schedule", 0);
   if (st == BDLU_OK) {
     std::lock_guard<std::mutex> lk(s->mu);
     st = bdlu_set_option(p->h, "precision", s->precision);
@@ -413,6 +428,10 @@ int bdlu_server_get_stats(bdlu_server* s, bdlu_server_stats* out) {
   out->peak_concurrency = s->peak_running;
   out->kernel_launches = s->kernel_launches;
   out->factor_flops = s->factor_flops;
+  const double done = static_cast<double>(std::max<int64_t>(1, s->completed + s->failed));
+  out->mean_stage_ms = s->stage_ms / done;
+  out->mean_factor_ms = s->factor_ms / done;
+  out->mean_solve_ms = s->solve_ms / done;
   return BDLU_OK;
 }
 
@@ -423,6 +442,7 @@ int bdlu_server_reset_stats(bdlu_server* s) {
   s->completed = s->failed = 0;
   s->kernel_launches = 0;
   s->factor_flops = 0.0;
+  s->stage_ms = s->factor_ms = s->solve_ms = 0.0;
   s->t_first = -1.0;
   s->t_last = 0.0;
   s->peak_running = s->running;

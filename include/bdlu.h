@@ -160,14 +160,26 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  *     replaced for this and later factorisations: TF32, then 3xTF32 (about
  *     FP32 accuracy), then FP64.  stats.precision and stats.refine_iters
  *     report the level and the refinement steps.  Device-pointer solves run
- *     "refine_iters" steps only.
+ *     "refine_iters" steps only.  2 is the mixed route starting at 3xTF32.
+ *     The tensor-core updates are tcgen05.mma (kind::tf32) with the
+ *     accumulator in tensor memory.
  *   "refactor_schedule": order of the FP64 value-only refactor of blocks
- *     above the shared-memory size.  0 (default): a chain of per-step
- *     launches (panel, then trailing update, one step of lookahead).  1: one
- *     persistent kernel works through the block's tile task graph (diagonal
- *     LU, strip solves, trailing updates; each task starts when its input
- *     tiles are ready).  Both give bit-identical factors.
- * Returns BDLU_OK, or BDLU_INVALID_DIMENSION for an unknown key. */
+ *     above the shared-memory size.  0: a chain of per-step launches (panel,
+ *     then trailing update, one step of lookahead).  1: one persistent kernel
+ *     works through the block's tile task graph (diagonal LU, strip solves,
+ *     trailing updates; each task starts when its input tiles are ready).
+ *     Both give bit-identical factors.  Unset, the autotuner picks per
+ *     pattern (see bdlu_tuner_report).
+ *   "lu_small_threads": launch width of the shared-memory LU: 0 (default)
+ *     the autotuner's, 32 one warp per unit (units up to 64 rows), 64 / 128 /
+ *     256 threads per unit (units up to that many rows).  Same factors.
+ *   "small_launch": -1 (default) the autotuner's, 0 one launch per size
+ *     bucket, 1 one persistent launch over a task queue.  Same factors.
+ *   "wait_limit": polls a bounded wait between tiles (large-unit solve
+ *     sweeps, tile task graph refactor) makes before it gives up with an
+ *     error status; 0 (default) about half a second.  Short limits make the
+ *     waits run out on purpose (tests of that error path).
+ * Returns BDLU_OK, or BDLU_INVALID_DIMENSION for an unknown key or value. */
 int bdlu_set_option(bdlu_solver* h, const char* key, double value);
 
 /* ---- Batches of independent systems ---------------------------------------
@@ -249,6 +261,9 @@ typedef struct bdlu_server_stats {
   int32_t peak_concurrency; /* most requests running at once */
   int64_t kernel_launches;  /* engine kernels launched by the completed requests (graph nodes counted) */
   double factor_flops;      /* dense-block LU flops of the completed requests (one factor each) */
+  double mean_stage_ms;     /* per request, worker wall time: device upload, input staging and checks */
+  double mean_factor_ms;    /*   value-only refactor, up to its status */
+  double mean_solve_ms;     /*   solve, residual, result copy-out */
 } bdlu_server_stats;
 bdlu_server* bdlu_server_create(int64_t memory_budget_bytes, int32_t slots);
 void bdlu_server_destroy(bdlu_server* s);

@@ -58,10 +58,10 @@ def _oracle_own_ordering(g, vals):
 
 
 def _large_system():
-    # 3,000 rows in 6 irreducible blocks of about 500 rows: every block is a
+    # 3,000 rows in 6 irreducible blocks of 274-741 rows: every block is a
     # large unit (above the 169-row shared-memory limit).
     g = bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(0, 31), 3000, 6)
-    assert g.block_sizes.min() > 300
+    assert g.block_sizes.min() > 169
     return g
 
 
