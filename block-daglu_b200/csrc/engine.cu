@@ -659,6 +659,10 @@ Engine::Engine() {
   for (auto& e : fork_ev_) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (auto& e : ev_) cudaEventCreate(&e);
   for (auto& e : pev_) cudaEventCreate(&e);
+  if (cudaMallocHost(reinterpret_cast<void**>(&readback_), kReadbackBytes) != cudaSuccess) {
+    readback_ = new char[kReadbackBytes];  // pageable: correct, only slower
+    readback_pinned_ = false;
+  }
   int dev = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev);
@@ -666,6 +670,8 @@ Engine::Engine() {
 
 Engine::~Engine() {
   release();
+  if (readback_pinned_) cudaFreeHost(readback_);
+  else delete[] readback_;
   if (cap_stream_) cudaStreamDestroy(cap_stream_);
   if (cap_stream2_) cudaStreamDestroy(cap_stream2_);
   for (auto& a : aux_)
@@ -1105,12 +1111,16 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
 
 int Engine::factor_status(cudaStream_t stream, std::string& err) {
   int32_t st[2] = {0, 0};
-  cudaError_t e = cudaMemcpyAsync(st, d_status_, sizeof(st), cudaMemcpyDeviceToHost, stream);
+  // Read back through the engine's page-locked words: a pageable
+  // destination would go through the driver's shared staging buffers, which
+  // serialises the status reads of concurrent requests.
+  cudaError_t e = cudaMemcpyAsync(readback_, d_status_, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) {
     err = std::string("factor status: ") + cudaGetErrorString(e);
     return -1;
   }
+  std::memcpy(st, readback_, sizeof(st));
   if (st[0] == kFailZeroPivot) {
     err = "block factorization failed: zero pivot in diagonal block " + std::to_string(st[1]);
     return 1;
@@ -1306,10 +1316,19 @@ bool Engine::last_residual(cudaStream_t stream, SolveResidual& out, std::string&
   out = SolveResidual{0, 0, 0, 0};
   if (last_nrhs_ <= 0) return true;
   int32_t st[2] = {0, 0};
-  BDLU_CUDA(cudaMemcpyAsync(st, d_status_, sizeof(st), cudaMemcpyDeviceToHost, stream));
-  std::vector<unsigned long long> h(static_cast<size_t>(4 * last_nrhs_));
-  BDLU_CUDA(cudaMemcpyAsync(h.data(), d_norms_, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+  // Status and norms through page-locked words (see factor_status); norms of
+  // more right-hand sides than they hold go through a host vector.
+  const size_t nn = static_cast<size_t>(4 * last_nrhs_);
+  std::vector<unsigned long long> h;
+  unsigned long long* hn = reinterpret_cast<unsigned long long*>(readback_ + 32);
+  if (nn > kReadbackNorms) {
+    h.resize(nn);
+    hn = h.data();
+  }
+  BDLU_CUDA(cudaMemcpyAsync(readback_, d_status_, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+  BDLU_CUDA(cudaMemcpyAsync(hn, d_norms_, nn * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
   BDLU_CUDA(cudaStreamSynchronize(stream));
+  std::memcpy(st, readback_, sizeof(st));
   if (st[0] == kFailSync) {
     err = "solve failed: a bounded wait between solve tiles ran out";
     return false;
@@ -1317,7 +1336,7 @@ bool Engine::last_residual(cudaStream_t stream, SolveResidual& out, std::string&
   double worst = -1.0;
   for (int32_t k = 0; k < last_nrhs_; ++k) {
     double v[4];
-    std::memcpy(v, &h[static_cast<size_t>(4 * k)], sizeof(v));
+    std::memcpy(v, hn + 4 * k, sizeof(v));
     const double denom = v[3] * v[2] + v[1];
     const double rel = denom > 0.0 ? v[0] / denom : v[0];
     if (rel > worst) {

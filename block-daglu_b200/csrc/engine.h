@@ -157,6 +157,12 @@ class Engine {
   cudaError_t launch_small_queue(const double* d_vals, cudaStream_t stream);
   int small_mode() const;
   cudaError_t tune_small_mode(const double* d_vals, cudaStream_t stream);
+  // Page-locked words for status and residual-norm read-backs: 8 int32
+  // status words, then kReadbackNorms norms.
+  static constexpr size_t kReadbackNorms = 4 * 64;
+  static constexpr size_t kReadbackBytes = 32 + kReadbackNorms * sizeof(unsigned long long);
+  char* readback_ = nullptr;
+  bool readback_pinned_ = true;
   int32_t forced_small_mode_ = -1;
   uint64_t pattern_key_ = 0;
   const int32_t* d_qunits_ = nullptr;  // small units, largest first
