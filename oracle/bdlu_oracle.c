@@ -283,6 +283,7 @@ const double* or_block_lu(const or_system* s, int32_t b, const int32_t** piv, in
 
 /* solve_ubtf, reverse schedule (ubtf_block_solver.cpp:2220-2414, 2548-2552). */
 int or_block_solve(const or_system* s, double* b) {
+  if (!s->lu) return 0; /* not factored (or_factor first) */
   const int32_t n = s->n;
   double* bperm = (double*)malloc(sizeof(double) * n);
   double* xperm = (double*)calloc(n, sizeof(double));

@@ -266,6 +266,7 @@ class System:
             self._lib.or_free(s)
 
     def factor(self):
+        self._factored = True
         return bool(self._lib.or_factor(self._s))
 
     def failed_block(self):
@@ -295,6 +296,8 @@ class System:
         return lu, pv
 
     def solve(self, b, refine_iters=0):
+        if not getattr(self, "_factored", False):
+            raise RuntimeError("oracle System.solve before factor")
         x = np.ascontiguousarray(b, np.float64).copy()
         taken = self._lib.or_solve_system(self._s, _p64(x), int(refine_iters))
         if taken < 0:
