@@ -111,6 +111,7 @@ int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
   h->engine->set_lu_small_width(h->lu_small_threads);
+  h->engine->set_blocking_sync(h->blocking_sync);
   h->engine->set_small_mode(h->small_mode);
   const int32_t sched = schedule_for(h);
   h->engine->set_refactor_schedule(sched);
@@ -413,7 +414,7 @@ int bdlu_solve_checked_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, 
   e = cudaMemcpy2DAsync(B, static_cast<size_t>(ldb) * sizeof(double), d_B, static_cast<size_t>(h->n) * sizeof(double),
                         static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs),
                         device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e == cudaSuccess) e = h->engine->wait(stream);
   if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("solution download: ") + cudaGetErrorString(e));
   h->last_refine = iters + steps;
   if (!std::isfinite(h->last_residual)) return fail(h, BDLU_SOLVE_FAILED, "block solve produced a non-finite solution");
@@ -501,6 +502,7 @@ int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nn
   const int tuned = schedule_tunable(h) ? Tuner::get().refactor_schedule(h->sig) : -1;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
   h->engine->set_lu_small_width(h->lu_small_threads);
+  h->engine->set_blocking_sync(h->blocking_sync);
   h->engine->set_small_mode(h->small_mode);
   h->engine->set_refactor_schedule(tuned >= 0 ? tuned : h->refactor_schedule);
   h->engine->set_wait_limit(h->wait_limit);
@@ -536,6 +538,7 @@ int bdlu_refactor_solve(bdlu_solver* h, const double* vals, int64_t nnz, double*
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
   h->engine->set_lu_small_width(h->lu_small_threads);
+  h->engine->set_blocking_sync(h->blocking_sync);
   h->engine->set_small_mode(h->small_mode);
   const int32_t sched = schedule_for(h);
   h->engine->set_refactor_schedule(sched);
@@ -657,6 +660,13 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
     if (value != 0.0 && value != 32.0 && value != 64.0 && value != 128.0 && value != 256.0)
       return BDLU_INVALID_DIMENSION;
     h->lu_small_threads = static_cast<int32_t>(value);
+    return BDLU_OK;
+  }
+  if (k == "blocking_sync") {
+    // 1: waits for the device sleep on blocking-sync events instead of
+    // spinning (for processes where many threads wait at once).
+    h->blocking_sync = value != 0.0;
+    if (h->engine) h->engine->set_blocking_sync(h->blocking_sync);
     return BDLU_OK;
   }
   if (k == "small_launch") {

@@ -47,6 +47,7 @@ struct bdlu_solver {
   int32_t wait_limit = 0;         // polls of a bounded wait between tiles (0: default; Engine::set_wait_limit)
   int32_t lu_small_threads = 0;   // forced shared-memory LU width (0: autotuned; Engine::set_lu_small_width)
   int32_t small_mode = -1;        // small units per bucket (0) or in one queue launch (1); -1 autotuned
+  bool blocking_sync = false;     // waits sleep on blocking-sync events (Engine::set_blocking_sync)
   // Error state (solver.h:122-123).
   int last_error = BDLU_OK;
   std::string last_message;

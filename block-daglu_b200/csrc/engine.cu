@@ -670,6 +670,7 @@ Engine::Engine() {
 
 Engine::~Engine() {
   release();
+  if (wait_ev_) cudaEventDestroy(wait_ev_);
   if (readback_pinned_) cudaFreeHost(readback_);
   else delete[] readback_;
   if (cap_stream_) cudaStreamDestroy(cap_stream_);
@@ -1109,13 +1110,28 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   return true;
 }
 
+cudaError_t Engine::wait(cudaStream_t stream) {
+  if (!blocking_sync_) return cudaStreamSynchronize(stream);
+  // Record an event created with cudaEventBlockingSync and wait on it: the
+  // calling thread sleeps instead of spinning on a core.
+  if (!wait_ev_) {
+    const cudaError_t e = cudaEventCreateWithFlags(&wait_ev_, cudaEventBlockingSync | cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+      wait_ev_ = nullptr;
+      return e;
+    }
+  }
+  const cudaError_t e = cudaEventRecord(wait_ev_, stream);
+  return e == cudaSuccess ? cudaEventSynchronize(wait_ev_) : e;
+}
+
 int Engine::factor_status(cudaStream_t stream, std::string& err) {
   int32_t st[2] = {0, 0};
   // Read back through the engine's page-locked words: a pageable
   // destination would go through the driver's shared staging buffers, which
   // serialises the status reads of concurrent requests.
   cudaError_t e = cudaMemcpyAsync(readback_, d_status_, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e == cudaSuccess) e = wait(stream);
   if (e != cudaSuccess) {
     err = std::string("factor status: ") + cudaGetErrorString(e);
     return -1;
@@ -1327,7 +1343,7 @@ bool Engine::last_residual(cudaStream_t stream, SolveResidual& out, std::string&
   }
   BDLU_CUDA(cudaMemcpyAsync(readback_, d_status_, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
   BDLU_CUDA(cudaMemcpyAsync(hn, d_norms_, nn * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
-  BDLU_CUDA(cudaStreamSynchronize(stream));
+  BDLU_CUDA(wait(stream));
   std::memcpy(st, readback_, sizeof(st));
   if (st[0] == kFailSync) {
     err = "solve failed: a bounded wait between solve tiles ran out";

@@ -120,6 +120,11 @@ class Engine {
     dp_.wait_limit = v;
     drop_graphs();
   }
+  // Waits for `stream`: spinning (cudaStreamSynchronize), or, with
+  // set_blocking_sync(true), sleeping on a blocking-sync event (many host
+  // threads waiting at once, as the serving loop's workers do).
+  cudaError_t wait(cudaStream_t stream);
+  void set_blocking_sync(bool b) { blocking_sync_ = b; }
   // Residual norms of the last solve (synchronises the stream), worst column.
   bool last_residual(cudaStream_t stream, SolveResidual& out, std::string& err);
 
@@ -162,6 +167,8 @@ class Engine {
   static constexpr size_t kReadbackNorms = 4 * 64;
   static constexpr size_t kReadbackBytes = 32 + kReadbackNorms * sizeof(unsigned long long);
   char* readback_ = nullptr;
+  bool blocking_sync_ = false;
+  cudaEvent_t wait_ev_ = nullptr;
   bool readback_pinned_ = true;
   int32_t forced_small_mode_ = -1;
   uint64_t pattern_key_ = 0;

@@ -86,6 +86,8 @@ struct bdlu_server {
   std::string last_message;
   int last_error = BDLU_OK;
   double precision = 0.0;  // "precision" option of every pattern's handle
+  int64_t max_nnz = 0;     // largest pattern: sizes the workers' page-locked staging once
+  int32_t max_n = 0;
 };
 
 namespace {
@@ -145,13 +147,17 @@ Request* pick(bdlu_server* s) {
 struct Staging {
   double* buf = nullptr;
   size_t cap = 0;  // doubles
-  double* get(size_t count) {
+  // `hint`: the size the largest pattern needs, allocated at once so the
+  // buffer is not regrown request after request (cudaMallocHost and
+  // cudaFreeHost are slow and cudaFreeHost synchronises the device).
+  double* get(size_t count, size_t hint) {
     if (count <= cap) return buf;
     if (buf) cudaFreeHost(buf);
     buf = nullptr;
     cap = 0;
-    if (cudaMallocHost(reinterpret_cast<void**>(&buf), count * sizeof(double)) != cudaSuccess) return nullptr;
-    cap = count;
+    const size_t want = std::max(count, hint);
+    if (cudaMallocHost(reinterpret_cast<void**>(&buf), want * sizeof(double)) != cudaSuccess) return nullptr;
+    cap = want;
     return buf;
   }
   ~Staging() {
@@ -166,12 +172,15 @@ void worker(bdlu_server* s) {
   while (true) {
     Request* r = nullptr;
     Pattern* pp = nullptr;
+    size_t hint_v = 0, hint_b = 0;
     {
       std::unique_lock<std::mutex> lk(s->mu);
       s->cv_work.wait(lk, [&] { return s->stop || (r = pick(s)) != nullptr; });
       if (!r) break;
       s->peak_running = std::max(s->peak_running, ++s->running);
       pp = s->patterns[static_cast<size_t>(r->pattern)].get();
+      hint_v = static_cast<size_t>(s->max_nnz);
+      hint_b = static_cast<size_t>(s->max_n) * 16;
     }
     Pattern& p = *pp;
     int st = BDLU_OK;
@@ -187,8 +196,8 @@ void worker(bdlu_server* s) {
       if (st == BDLU_OK) st = bdlu_solve_checked_on(p.h, r->B, r->ldb, r->nrhs, stream, true);
     } else {
       const size_t nb = static_cast<size_t>(p.n) * static_cast<size_t>(r->nrhs);
-      double* sv = vstage.get(static_cast<size_t>(p.nnz));
-      double* sb = bstage.get(nb);
+      double* sv = vstage.get(static_cast<size_t>(p.nnz), hint_v);
+      double* sb = bstage.get(nb, hint_b);
       if (st == BDLU_OK && (!sv || !sb)) st = -1;
       // One pass per input: the copy into page-locked staging checks for
       // NaN and infinity on the way; the checks fail the request where
@@ -315,6 +324,9 @@ int32_t bdlu_server_add_pattern(bdlu_server* s, const int32_t* rows, const int32
   // kernels on the GPU its CTAs lose the SMs they wait for (measured: tens of
   // milliseconds to seconds per refactor while the chain takes a few).
   if (st == BDLU_OK) st = bdlu_set_option(p->h, "refactor_schedule", 0);
+  // Many workers wait for the device at once: they sleep on blocking-sync
+  // events instead of each spinning a host core.
+  if (st == BDLU_OK) st = bdlu_set_option(p->h, "blocking_sync", 1);
   if (st == BDLU_OK) {
     std::lock_guard<std::mutex> lk(s->mu);
     st = bdlu_set_option(p->h, "precision", s->precision);
@@ -334,6 +346,8 @@ int32_t bdlu_server_add_pattern(bdlu_server* s, const int32_t* rows, const int32
     return -sfail(s, BDLU_ANALYSIS_FAILED, e.what());
   }
   std::lock_guard<std::mutex> lk(s->mu);
+  s->max_nnz = std::max(s->max_nnz, p->nnz);
+  s->max_n = std::max(s->max_n, p->n);
   s->patterns.push_back(std::move(p));
   return static_cast<int32_t>(s->patterns.size()) - 1;
 }
