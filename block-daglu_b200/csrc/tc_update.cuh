@@ -144,27 +144,54 @@ __device__ bool tile_update_tc(double* A, int m, int i0, int j0, int k0, int kk,
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int kWarps = kTcThreads / 32;
   // Stage: one warp per core matrix (8 rows x 4 K), lane = row%8 * 4 + k%4,
-  // so a warp writes 128 contiguous bytes.
+  // so a warp writes 128 contiguous bytes.  Each warp first issues the loads
+  // of kBatch core matrices (read-only path: the panels do not change during
+  // the launch), then converts and stores them, so the loads overlap.
   constexpr int kQG = K / 4;
-  for (int b = warp; b < (kTcM / 8) * kQG; b += kWarps) {
-    const int rg = b / kQG, qg = b - rg * kQG;
-    const int r = rg * 8 + (lane >> 2), q = qg * 4 + (lane & 3);
-    const double v = (i0 + r < m && q < kk) ? A[static_cast<size_t>(i0 + r) * m + k0 + q] : 0.0;
-    const float f = static_cast<float>(v);
-    const uint32_t h = tc_to_tf32(f);
-    const uint32_t off = (q >> 3) * kAChunk + rg * 256 + ((q >> 2) & 1) * 128 + lane * 4;
-    *reinterpret_cast<uint32_t*>(Ah + off) = h;
-    if (split3) *reinterpret_cast<uint32_t*>(Al + off) = tc_to_tf32(f - __uint_as_float(h));
+  constexpr int kBatch = 8;
+  constexpr int kBlocksA = (kTcM / 8) * kQG, kBlocksB = (TN / 8) * kQG;
+  static_assert(kBlocksA % (kWarps * kBatch) == 0 && kBlocksB % (kWarps * kBatch) == 0, "staging batches");
+  for (int b0 = warp; b0 < kBlocksA; b0 += kWarps * kBatch) {
+    double v[kBatch];
+#pragma unroll
+    for (int t = 0; t < kBatch; ++t) {
+      const int b = b0 + t * kWarps;
+      const int rg = b / kQG, qg = b - rg * kQG;
+      const int r = rg * 8 + (lane >> 2), q = qg * 4 + (lane & 3);
+      v[t] = (i0 + r < m && q < kk) ? __ldg(A + static_cast<size_t>(i0 + r) * m + k0 + q) : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < kBatch; ++t) {
+      const int b = b0 + t * kWarps;
+      const int rg = b / kQG, qg = b - rg * kQG;
+      const int q = qg * 4 + (lane & 3);
+      const float f = static_cast<float>(v[t]);
+      const uint32_t h = tc_to_tf32(f);
+      const uint32_t off = (q >> 3) * kAChunk + rg * 256 + ((q >> 2) & 1) * 128 + lane * 4;
+      *reinterpret_cast<uint32_t*>(Ah + off) = h;
+      if (split3) *reinterpret_cast<uint32_t*>(Al + off) = tc_to_tf32(f - __uint_as_float(h));
+    }
   }
-  for (int b = warp; b < (TN / 8) * kQG; b += kWarps) {
-    const int ng = b / kQG, qg = b - ng * kQG;
-    const int n = ng * 8 + (lane >> 2), q = qg * 4 + (lane & 3);
-    const double v = (q < kk && j0 + n < m) ? A[static_cast<size_t>(k0 + q) * m + j0 + n] : 0.0;
-    const float f = static_cast<float>(v);
-    const uint32_t h = tc_to_tf32(f);
-    const uint32_t off = (q >> 3) * kBChunk + ng * 256 + ((q >> 2) & 1) * 128 + lane * 4;
-    *reinterpret_cast<uint32_t*>(Bh + off) = h;
-    if (split3) *reinterpret_cast<uint32_t*>(Bl + off) = tc_to_tf32(f - __uint_as_float(h));
+  for (int b0 = warp; b0 < kBlocksB; b0 += kWarps * kBatch) {
+    double v[kBatch];
+#pragma unroll
+    for (int t = 0; t < kBatch; ++t) {
+      const int b = b0 + t * kWarps;
+      const int ng = b / kQG, qg = b - ng * kQG;
+      const int n = ng * 8 + (lane >> 2), q = qg * 4 + (lane & 3);
+      v[t] = (q < kk && j0 + n < m) ? __ldg(A + static_cast<size_t>(k0 + q) * m + j0 + n) : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < kBatch; ++t) {
+      const int b = b0 + t * kWarps;
+      const int ng = b / kQG, qg = b - ng * kQG;
+      const int q = qg * 4 + (lane & 3);
+      const float f = static_cast<float>(v[t]);
+      const uint32_t h = tc_to_tf32(f);
+      const uint32_t off = (q >> 3) * kBChunk + ng * 256 + ((q >> 2) & 1) * 128 + lane * 4;
+      *reinterpret_cast<uint32_t*>(Bh + off) = h;
+      if (split3) *reinterpret_cast<uint32_t*>(Bl + off) = tc_to_tf32(f - __uint_as_float(h));
+    }
   }
   // Generic-proxy writes become visible to the tensor core's async proxy.
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

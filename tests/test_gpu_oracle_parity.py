@@ -137,8 +137,11 @@ def test_mixed_route_matches_oracle():
     assert s.solve_in_place(X), s.last_error_message()
     assert s.stats()["residual_inf"] <= RESID_TOL
     ref = _oracle_own_ordering(g, g.vals)
+    # Refinement stops at the residual bound (1e-12), so the forward error is
+    # up to cond(A) * 1e-12 (the units here have condition numbers up to about
+    # 1e5), not the FP64 route's rounding level: relative 1e-6.
     for j in range(B.shape[1]):
-        assert close_vec(X[:, j], ref.solve(np.ascontiguousarray(B[:, j]))), j
+        assert close_vec(X[:, j], ref.solve(np.ascontiguousarray(B[:, j])), 1e-6), j
 
 
 def test_batch_systems_match_oracle():
