@@ -902,7 +902,7 @@ def run_precision(args, rank, world):
         B = np.asfortranarray(rng.uniform(-1.0, 1.0, (g.n, PREC_NRHS)))
         res = {"n": g.n, "nnz": int(g.nnz)}
         X64 = None
-        for mode in (0, 1):
+        for mode in (0, 1, 2):
             s = bd.Solver()
             s.set_option("precision", mode)
             s.set_option("refactor_pivoting", 1)   # every factorisation searches pivots
@@ -921,7 +921,7 @@ def run_precision(args, rank, world):
                 steps.append((time.perf_counter() - t0, tf))
             st = s.stats()
             ph = s.phase_times()
-            key = "fp64" if mode == 0 else "mixed"
+            key = {0: "fp64", 1: "mixed", 2: "mixed_3xtf32"}[mode]
             res[key] = {"seconds_per_step": statistics.mean(t for t, _ in steps),
                         "factor_seconds": statistics.mean(f for _, f in steps),
                         "residual_inf": st["residual_inf"], "refine_iters": st["refine_iters"],
@@ -931,18 +931,21 @@ def run_precision(args, rank, world):
             if mode == 0:
                 X64 = X.copy()
             else:
-                res["mixed"]["error_vs_fp64"] = float(np.max(np.abs(X - X64)) / np.max(np.abs(X64)))
+                res[key]["error_vs_fp64"] = float(np.max(np.abs(X - X64)) / np.max(np.abs(X64)))
             del s
         res["speedup_mixed_over_fp64"] = res["fp64"]["seconds_per_step"] / res["mixed"]["seconds_per_step"]
+        res["speedup_mixed_3xtf32_over_fp64"] = res["fp64"]["seconds_per_step"] / res["mixed_3xtf32"]["seconds_per_step"]
         out[label] = res
         del g
     a = out["a"]
-    value = 1.0 / a["mixed"]["seconds_per_step"]
+    best = min(("mixed", "mixed_3xtf32"), key=lambda k: a[k]["seconds_per_step"])
+    value = 1.0 / a[best]["seconds_per_step"]
     line = {"metric": PREC_METRIC, "value": value, "unit": PREC_METRIC, "n_gpus": 1, "steps": max(1, min(args.steps, 2)),
             "warmup": 1, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64 storage, tf32 tensor-core updates, f64 refinement", "data": "synthetic",
             "config": {"workload": PREC_WORKLOAD, "blocks": args.blocks, "nrhs": PREC_NRHS,
-                       "value_from": "instance a (kappa 1e4), mixed route, host buffers"},
+                       "value_from": "instance a (kappa 1e4), the faster mixed route (TF32 start or 3xTF32 start), "
+                                     "host buffers"},
             "instances": out, "roofline": None, "cpu_baseline": None, "gpu_launches": None}
     flops = a["mixed"]["factor_flops"]
     line["tensor_update_tflops"] = flops / a["mixed"]["factor_seconds"] / 1e12
