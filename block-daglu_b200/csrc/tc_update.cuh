@@ -245,14 +245,32 @@ __device__ bool tile_update_tc(double* A, int m, int i0, int j0, int k0, int kk,
   // The next tile's MMAs overwrite the accumulator only after this barrier.
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  // C -= accumulator, one warp per row at a time, lanes along the row.
-  for (int rr = warp; rr < kTcM; rr += kWarps) {
-    const int gi = i0 + rr;
-    if (gi >= m) break;
-    double* row = A + static_cast<size_t>(gi) * m + j0;
+  // C -= accumulator: warps along rows, lanes along a row (coalesced); each
+  // warp loads the C entries of kRows rows before it subtracts and stores,
+  // so those loads are in flight together.
+  constexpr int kCols = TN / 32, kRows = 4;
+  static_assert(kTcM % (kWarps * kRows) == 0, "epilogue row groups");
+  for (int rr0 = warp; rr0 < kTcM; rr0 += kWarps * kRows) {
+    double cv[kRows][kCols];
 #pragma unroll
-    for (int c = lane; c < TN; c += 32)
-      if (j0 + c < m) row[c] -= static_cast<double>(Cs[rr * kCS + c]);
+    for (int h = 0; h < kRows; ++h) {
+      const int gi = i0 + rr0 + h * kWarps;
+#pragma unroll
+      for (int t = 0; t < kCols; ++t) {
+        const int c = lane + 32 * t;
+        cv[h][t] = (gi < m && j0 + c < m) ? A[static_cast<size_t>(gi) * m + j0 + c] : 0.0;
+      }
+    }
+#pragma unroll
+    for (int h = 0; h < kRows; ++h) {
+      const int rr = rr0 + h * kWarps, gi = i0 + rr;
+#pragma unroll
+      for (int t = 0; t < kCols; ++t) {
+        const int c = lane + 32 * t;
+        if (gi < m && j0 + c < m)
+          A[static_cast<size_t>(gi) * m + j0 + c] = cv[h][t] - static_cast<double>(Cs[rr * kCS + c]);
+      }
+    }
   }
   __syncthreads();  // Cs is the next tile's staging area
   return true;
