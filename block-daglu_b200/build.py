@@ -30,7 +30,7 @@ def sources():
 
 
 def headers():
-    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     inc = os.path.join(ROOT, "include")
     for dp, _, fs in os.walk(inc):
         hs += [os.path.join(dp, f) for f in fs if f.endswith(".h")]
