@@ -1207,7 +1207,7 @@ __global__ void __launch_bounds__(kTcThreads) k_rgemm_tc(DevPlan dp, int32_t k0,
 }
 
 // First-factor update (k_gemm_rm's 128 x 128 tiles, K = kPanel).
-__global__ void __launch_bounds__(kTcThreads) k_gemm_rm_tc(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
+__global__ void __launch_bounds__(kTcThreads, 3) k_gemm_rm_tc(DevPlan dp, int32_t k0, int32_t ubase, int32_t nact,
                                                            int32_t split3) {
   extern __shared__ uint8_t tc_dyn_g[];
   __shared__ uint32_t s_tmem;

@@ -14,9 +14,14 @@
 //      FP32 accumulator in tensor memory; 3K/8 with split3: hi*hi + hi*lo +
 //      lo*hi) and commits them to an mbarrier;
 //   3. all threads wait on the mbarrier (bounded), read the accumulator
-//      (tcgen05.ld, warp w reads lanes 32(w%4).. of its sub-partition), pass
-//      it through shared memory and subtract it from C row by row
-//      (coalesced FP64 read-modify-write).
+//      (tcgen05.ld, warp w reads lanes 32(w%4).. of its sub-partition) and
+//      subtract it from C with coalesced FP64 read-modify-writes.  Square
+//      tiles (TN = 128) are computed transposed, D^T = U^T L^T, so a
+//      tensor-memory lane is a column of C: each thread updates its column
+//      straight from its registers, a warp touching 32 consecutive columns
+//      of one row at a time, and the first C rows are loaded before the
+//      wait.  Other tiles pass the accumulator through shared memory and
+//      update C row by row.
 // The accumulator's tensor-memory columns are allocated once per CTA
 // (tc_tmem_alloc) and freed before the CTA exits (tc_tmem_free).
 #pragma once
@@ -115,11 +120,12 @@ __device__ __forceinline__ bool tc_wait(uint64_t* s_bar, uint32_t parity) {
 }
 
 // Shared memory of one tile update: staged operands (hi, and lo with split3);
-// the accumulator pass-through reuses the same bytes.
+// the accumulator pass-through of non-square tiles reuses the same bytes.
 template <int K, int TN>
 __host__ __device__ constexpr size_t tc_smem_bytes() {
   constexpr size_t ops = 2 * (static_cast<size_t>(kTcM) * K * 4 + static_cast<size_t>(TN) * K * 4);
-  constexpr size_t acc = static_cast<size_t>(kTcM) * (TN + 1) * 4;
+  // (square tiles read the accumulator straight from tensor memory)
+  constexpr size_t acc = TN == kTcM ? 0 : static_cast<size_t>(kTcM) * (TN + 1) * 4;
   return (ops > acc ? ops : acc) + 1024;  // + alignment slack of the dynamic base
 }
 
@@ -143,6 +149,9 @@ __device__ bool tile_update_tc(double* A, int m, int i0, int j0, int k0, int kk,
   uint8_t* Bl = Al + kABytes;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int kWarps = kTcThreads / 32;
+  // Square tiles keep the accumulator transposed (lane = column of C), so
+  // each thread owns one column and a warp's C accesses are whole rows.
+  constexpr bool kColMajorAcc = TN == kTcM;
   // Stage: one warp per core matrix (8 rows x 4 K), lane = row%8 * 4 + k%4,
   // so a warp writes 128 contiguous bytes.  Each warp first issues the loads
   // of kBatch core matrices (read-only path: the panels do not change during
@@ -204,15 +213,69 @@ __device__ bool tile_update_tc(double* A, int m, int i0, int j0, int k0, int kk,
     for (int kc = 0; kc < nk; ++kc) {
       const uint64_t dah = tc_desc(ah + kc * kAChunk, 128, 256);
       const uint64_t dbh = tc_desc(bh + kc * kBChunk, 128, 256);
-      tc_mma_tf32(tmem, dah, dbh, idesc, kc > 0 ? 1u : 0u);
-      if (split3) {
-        tc_mma_tf32(tmem, dah, tc_desc(bl + kc * kBChunk, 128, 256), idesc, 1u);
-        tc_mma_tf32(tmem, tc_desc(al + kc * kAChunk, 128, 256), dbh, idesc, 1u);
+      const uint64_t dal = tc_desc(al + kc * kAChunk, 128, 256);
+      const uint64_t dbl = tc_desc(bl + kc * kBChunk, 128, 256);
+      if constexpr (kColMajorAcc) {
+        // D^T = U^T L^T: tensor-memory lane = column of C.
+        tc_mma_tf32(tmem, dbh, dah, idesc, kc > 0 ? 1u : 0u);
+        if (split3) {
+          tc_mma_tf32(tmem, dbh, dal, idesc, 1u);
+          tc_mma_tf32(tmem, dbl, dah, idesc, 1u);
+        }
+      } else {
+        tc_mma_tf32(tmem, dah, dbh, idesc, kc > 0 ? 1u : 0u);
+        if (split3) {
+          tc_mma_tf32(tmem, dah, dbl, idesc, 1u);
+          tc_mma_tf32(tmem, dal, dbh, idesc, 1u);
+        }
       }
     }
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                      tc_smem_addr(s_bar))
                  : "memory");
+  }
+  if constexpr (kColMajorAcc) {
+    // Thread (sub-partition s, lane l) owns column 32 s + l of the tile and
+    // rows [64 h, 64 h + 64) (h = warp / 4), in chunks of kCh rows.  The first
+    // chunk of C is loaded before the wait, so those loads overlap the MMAs.
+    constexpr int kCh = 16, kNch = kTcM / 2 / kCh;
+    const int sub = warp & 3, half = warp >> 2;
+    const int jj = sub * 32 + lane;
+    const bool colok = j0 + jj < m;
+    double* colp = A + j0 + jj;
+    const uint32_t tlane = tmem + (static_cast<uint32_t>(sub * 32) << 16);
+    double cv[kCh];
+    auto load_chunk = [&](int ch) {
+      const int rb = i0 + half * (kTcM / 2) + ch * kCh;
+#pragma unroll
+      for (int t = 0; t < kCh; ++t)
+        cv[t] = (colok && rb + t < m) ? colp[static_cast<size_t>(rb + t) * m] : 0.0;
+    };
+    load_chunk(0);
+    bool ok = tc_wait(s_bar, parity);
+    if (!ok) ok = tc_wait(s_bar, parity);
+    parity ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!__syncthreads_and(ok)) return false;
+#pragma unroll 1
+    for (int ch = 0; ch < kNch; ++ch) {
+      if (ch > 0) load_chunk(ch);
+      const int r0 = half * (kTcM / 2) + ch * kCh;
+      uint32_t v[kCh];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(tlane + static_cast<uint32_t>(r0)));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const int rb = i0 + r0;
+#pragma unroll
+      for (int t = 0; t < kCh; ++t)
+        if (colok && rb + t < m) colp[static_cast<size_t>(rb + t) * m] = cv[t] - static_cast<double>(__uint_as_float(v[t]));
+    }
+    // The next tile's MMAs overwrite the accumulator only after a barrier.
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    return true;
   }
   // Every thread waits; one that runs out waits once more (bounded) so no
   // tensor-core work is left reading shared memory, and the tile is skipped.
