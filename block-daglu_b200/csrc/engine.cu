@@ -28,6 +28,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <utility>
 
 namespace bdlu {
 
@@ -301,6 +302,108 @@ __device__ __forceinline__ void lu_warp_unit(const DevPlan& dp, const double* __
         if (j < m) out[static_cast<size_t>(j) * m + pos[r]] = a[r][j];
       dp.lperm[s + pos[r]] = row;
     }
+  }
+}
+
+// Row-per-thread LU: one CTA of M threads per unit of up to M rows (M = 64
+// or 96).  Thread t holds row t of the unit in registers (all M columns,
+// statically indexed: the column loop is unrolled); row swaps are logical as
+// in lu_warp_unit.  Per column: warp candidates (first strict maximum of |a|
+// over the rows not yet pivoted), combined by every thread from shared
+// memory; the pivot row's owner publishes its remaining entries; then each
+// row below forms its multiplier and updates itself.  Two barriers of M
+// threads per column, no shared-memory traffic in the update.  Arithmetic per
+// element is the micro-kernel's, so the factors, pivots and row order are
+// bit-identical to k_lu_small's.  The column loop is a fold over one
+// template instance per column (RowsLu::step<K>), so every index into the
+// register row is a constant and the row never leaves the registers.
+template <int M>
+struct RowsLu {
+  static_assert(M % 32 == 0 && M <= 96, "rows per unit");
+  static constexpr int kW = M / 32;
+  static constexpr int kNone = 1 << 20;
+  double* s_u;
+  double* s_best;
+  int* s_pos;
+  int32_t* piv;
+  int m, t, lane, warp, pos;
+  // Column K; false when the unit is done (K >= m) or failed.
+  template <int K>
+  __device__ __forceinline__ bool step(double (&a)[M], int& status) {
+    if (K >= m) return false;
+    const bool cand = pos >= K && pos != kNone;
+    double best = cand ? fabs(a[K]) : 0.0;
+    int bpos = cand ? pos : kNone;
+    warp_pivot_reduce(best, bpos, kNone);
+    if (lane == 0) {
+      s_best[warp] = best;
+      s_pos[warp] = bpos;
+    }
+    __syncthreads();
+    best = s_best[0];
+    bpos = s_pos[0];
+#pragma unroll
+    for (int w = 1; w < kW; ++w) pivot_combine(best, bpos, s_best[w], s_pos[w], kNone);
+    if (bpos == kNone || best == 0.0) {
+      status = 1;
+      return false;
+    }
+    const int p = bpos;
+    if (pos == p) {
+#pragma unroll
+      for (int j = K; j < M; ++j)
+        if (j < m) s_u[j] = a[j];
+    }
+    if (t == 0) piv[K] = p;
+    if (pos == K) pos = p;
+    else if (pos == p) pos = K;
+    __syncthreads();
+    if (pos > K && pos != kNone) {
+      const double l = __ddiv_rn(a[K], s_u[K]);
+      a[K] = l;
+#pragma unroll
+      for (int j = K + 1; j < M; ++j)
+        if (j < m) a[j] = __dsub_rn(a[j], __dmul_rn(l, s_u[j]));
+    }
+    return true;
+  }
+  template <int... Ks>
+  __device__ __forceinline__ void run(double (&a)[M], int& status, std::integer_sequence<int, Ks...>) {
+    (void)(step<Ks>(a, status) && ...);
+  }
+};
+
+template <int M>
+__global__ void __launch_bounds__(M) k_lu_rows(DevPlan dp, const double* __restrict__ vals,
+                                               const int32_t* __restrict__ units) {
+  extern __shared__ double S[];
+  __shared__ double s_u[M];
+  __shared__ double s_best[M / 32];
+  __shared__ int s_pos[M / 32];
+  const int u = units[blockIdx.x];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int t = threadIdx.x;
+  for (int i = t; i < m * m; i += M) S[i] = 0.0;
+  __syncthreads();
+  for (int64_t e = dp.dent_ptr[u] + t; e < dp.dent_ptr[u + 1]; e += M) S[dp.dent_pos[e]] = vals[dp.dent_src[e]];
+  __syncthreads();
+  double a[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) a[j] = (t < m && j < m) ? S[j * m + t] : 0.0;
+  RowsLu<M> lu{s_u, s_best, s_pos, dp.piv + s, m, t, t & 31, t >> 5, t < m ? t : RowsLu<M>::kNone};
+  int status = 0;
+  lu.run(a, status, std::make_integer_sequence<int, M>{});
+  if (status) {
+    if (t == 0) report_failure(dp.status, u);
+    return;
+  }
+  if (t < m) {
+    double* out = dp.lu + dp.lu_off[u];
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+      if (j < m) out[static_cast<size_t>(j) * m + lu.pos] = a[j];
+    dp.lperm[s + lu.pos] = t;
   }
 }
 
@@ -810,6 +913,10 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
                                         kWarpLuW2 * 64 * 64 * static_cast<int>(sizeof(double)));
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_lu_queue, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_lu_rows<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 64 * 8);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_lu_rows<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 96 * 8);
     });
     BDLU_CUDA(attr_err);
   }
@@ -894,6 +1001,14 @@ void Engine::launch_lu_small(int threads, int32_t units, int32_t mb, cudaStream_
                               st>>>(dp_, d_vals, list, units);
     return;
   }
+  if (threads == kLuRowsWidth && mb <= 64) {
+    k_lu_rows<64><<<units, 64, smem, st>>>(dp_, d_vals, list);
+    return;
+  }
+  if (threads == kLuRowsWidth && mb <= 96) {
+    k_lu_rows<96><<<units, 96, smem, st>>>(dp_, d_vals, list);
+    return;
+  }
   if (threads == 64) k_lu_small<64><<<units, 64, smem, st>>>(dp_, d_vals, list);
   else if (threads == 128) k_lu_small<128><<<units, 128, smem, st>>>(dp_, d_vals, list);
   else k_lu_small<kThreads><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
@@ -911,9 +1026,11 @@ static int32_t lu_bucket_class(int32_t mb) {
 }
 
 // Admissible widths of a bucket of units up to mb rows: 32 (one warp per
-// unit, up to 64 rows), and CTA widths with one thread per row at least.
+// unit, up to 64 rows), kLuRowsWidth (one thread per row, rows in registers,
+// up to 96 rows), and CTA widths with one thread per row at least.
 static bool lu_width_ok(int t, int32_t mb) {
   if (t == 32) return mb <= 64;
+  if (t == kLuRowsWidth) return mb <= 96;
   return (t == 64 || t == 128 || t == kThreads) && t >= mb;
 }
 
@@ -940,10 +1057,10 @@ cudaError_t Engine::tune_lu_small(const double* d_vals, cudaStream_t stream) {
     if (tu.lu_small_threads(lu_bucket_class(mb)) != 0) continue;
     if (!e0 && ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess)) break;
     const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
-    int widths[4], count = 0;
-    for (int t : {32, 64, 128, kThreads})
+    int widths[5], count = 0;
+    for (int t : {32, kLuRowsWidth, 64, 128, kThreads})
       if (lu_width_ok(t, mb)) widths[count++] = t;
-    float ms[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float ms[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     int best = widths[count - 1];
     float best_ms = 1e30f;
     for (int c = 0; c < count && e == cudaSuccess; ++c) {

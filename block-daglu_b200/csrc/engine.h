@@ -12,6 +12,11 @@
 
 namespace bdlu {
 
+// Width code of the row-per-thread small-unit LU (one CTA of 64 or 96
+// threads per unit, each thread one row in registers).
+constexpr int kLuRowsWidth = 1;
+
+
 // Device-side view of a plan (all pointers device memory owned by Engine).
 struct DevPlan {
   int32_t n;
@@ -105,7 +110,8 @@ class Engine {
   // persistent kernel over the tile task graph (when the plan has one).
   void set_refactor_schedule(int32_t s) { schedule_ = s; }
   // Launch width of the shared-memory LU forced for this engine (32: one
-  // warp per unit; 64, 128, 256: threads per CTA; 0: the autotuner's).
+  // warp per unit; kLuRowsWidth: one thread per row, rows in registers;
+  // 64, 128, 256: threads per CTA; 0: the autotuner's).
   void set_lu_small_width(int32_t t) { forced_lu_width_ = t; }
   // Small units as per-bucket launches (0) or one persistent launch over a
   // task queue (1); -1: the autotuner's choice for the pattern.

@@ -88,7 +88,7 @@ void Tuner::load() {
   for (size_t p = t.find("\"bucket_m\":"); p != std::string::npos; p = t.find("\"bucket_m\":", p + 1)) {
     int m = 0, th = 0;
     if (std::sscanf(t.c_str() + p, "\"bucket_m\": %d, \"threads\": %d", &m, &th) == 2 && m > 0 &&
-        (th == 32 || th == 64 || th == 128 || th == 256))
+        (th == 1 || th == 32 || th == 64 || th == 128 || th == 256))
       g_small[m].threads = th;
   }
   for (size_t p = t.find("\"mode_sig\":"); p != std::string::npos; p = t.find("\"mode_sig\":", p + 1)) {

@@ -27,7 +27,8 @@ class Tuner {
  public:
   static Tuner& get();
   bool enabled() const { return enabled_; }
-  // CTA width chosen for buckets of units up to `bucket_m` rows; 0 if none yet.
+  // Launch width chosen for buckets of units up to `bucket_m` rows (1: one
+  // thread per row, 32: one warp per unit, else threads per CTA); 0 if none.
   int lu_small_threads(int32_t bucket_m);
   void set_lu_small_threads(int32_t bucket_m, int threads, const float* ms, const int* widths, int count);
   // Small-unit launch mode for pattern `sig`: 0 per-bucket launches, 1 one
