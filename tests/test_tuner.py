@@ -26,7 +26,10 @@ def test_tuner_picks_lu_small_widths(cuda_device, monkeypatch):
     widths = {e["bucket_m"]: e for e in rep["lu_small_threads"]}
     assert widths, rep
     for m, e in widths.items():
-        assert (e["threads"] == 32 and m <= 64) or (e["threads"] in (64, 128, 256) and e["threads"] >= m)
+        # 1: one thread per row (units up to 96 rows); 32: one warp per unit
+        # (up to 64 rows); else threads per CTA, at least one per row.
+        assert (e["threads"] == 1 and m <= 96) or (e["threads"] == 32 and m <= 64) or \
+            (e["threads"] in (64, 128, 256) and e["threads"] >= m)
         if "ms" in e:
             assert len(e["ms"]) == len(e["widths"]) and min(e["ms"]) > 0.0
             assert e["ms"][e["widths"].index(e["threads"])] == min(e["ms"])
