@@ -35,6 +35,9 @@ namespace bdlu {
 namespace {
 
 constexpr int kThreads = 256;
+// Rows of the largest small unit any kernel here takes (the shared-memory
+// limit, small_unit_max(), is 169 on a 227 KB part), rounded up to a warp.
+constexpr int kLuRowsMax = 192;
 constexpr int32_t kWorkRhs = 16;
 // ---------------------------------------------------------------------------
 // Value gather for coupling entries and scalar units.
@@ -80,9 +83,10 @@ __device__ __forceinline__ void warp_pivot_signed(double v, int i, int none, dou
   bi = idx;
 }
 
-// One unit factored by the whole CTA (kT threads, kT >= m): A is the CTA's
-// m*m shared-memory slot.  A failed unit reports and returns (CTA-uniform).
-template <int kT>
+// One unit factored by the whole CTA (kT threads, kT >= m, m <= 32 kR): A is
+// the CTA's m*m shared-memory slot.  A failed unit reports and returns
+// (CTA-uniform).
+template <int kT, int kR>
 __device__ __forceinline__ void lu_cta_unit(const DevPlan& dp, const double* __restrict__ vals, int u, double* A,
                                             double* s_best, double* s_val, int* s_bi) {
   const int s = dp.ustart[u];
@@ -147,19 +151,44 @@ __device__ __forceinline__ void lu_cta_unit(const DevPlan& dp, const double* __r
     __syncthreads();
     if (tid == 0) colk[k] = pv;
     // Update: warp per column (column k+1 is warp 0's, which also yields the
-    // next pivot candidates), lane per row.
+    // next pivot candidates), lane per row (rows k+1+lane+32r, r < kR).  A
+    // warp takes kCC of its columns at a time and loads all their entries
+    // before it computes, so the shared-memory loads overlap.
     double cb = 0.0, cv = 0.0;
     int ci = m;
-    for (int j = k + 1 + warp; j < m; j += kT / 32) {
-      double* c = A + static_cast<size_t>(j) * m;
-      const double ukj = c[k];
-      for (int i = k + 1 + lane; i < m; i += 32) {
-        const double v = __dsub_rn(c[i], __dmul_rn(colk[i], ukj));
-        c[i] = v;
-        if (j == k + 1 && (ci == m || fabs(v) > cb)) {
-          cb = fabs(v);
-          cv = v;
-          ci = i;
+    {
+      constexpr int kWarps = kT / 32, kCC = 4;
+      const int i0 = k + 1 + lane;
+      double l[kR];
+#pragma unroll
+      for (int r = 0; r < kR; ++r) l[r] = (i0 + 32 * r < m) ? colk[i0 + 32 * r] : 0.0;
+      for (int j0 = k + 1 + warp; j0 < m; j0 += kWarps * kCC) {
+        double ukj[kCC], x[kCC][kR];
+#pragma unroll
+        for (int c = 0; c < kCC; ++c) {
+          const int j = j0 + c * kWarps;
+          const double* col = A + static_cast<size_t>(j) * m;
+          ukj[c] = (j < m) ? col[k] : 0.0;
+#pragma unroll
+          for (int r = 0; r < kR; ++r) x[c][r] = (j < m && i0 + 32 * r < m) ? col[i0 + 32 * r] : 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c < kCC; ++c) {
+          const int j = j0 + c * kWarps;
+          double* col = A + static_cast<size_t>(j) * m;
+#pragma unroll
+          for (int r = 0; r < kR; ++r) {
+            const int i = i0 + 32 * r;
+            if (j < m && i < m) {
+              const double v = __dsub_rn(x[c][r], __dmul_rn(l[r], ukj[c]));
+              col[i] = v;
+              if (j == k + 1 && (ci == m || fabs(v) > cb)) {
+                cb = fabs(v);
+                cv = v;
+                ci = i;
+              }
+            }
+          }
         }
       }
     }
@@ -194,13 +223,13 @@ __device__ __forceinline__ void lu_cta_unit(const DevPlan& dp, const double* __r
   for (int k = tid; k < m; k += kT) dp.lperm[s + k] = ord[k];
 }
 
-template <int kT>
+template <int kT, int kR>
 __global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __restrict__ vals,
                                                   const int32_t* __restrict__ units) {
   extern __shared__ double A[];
   __shared__ double s_best[kT / 32], s_val[kT / 32];
   __shared__ int s_bi[kT / 32];
-  lu_cta_unit<kT>(dp, vals, units[blockIdx.x], A, s_best, s_val, s_bi);
+  lu_cta_unit<kT, kR>(dp, vals, units[blockIdx.x], A, s_best, s_val, s_bi);
 }
 
 // ---------------------------------------------------------------------------
@@ -441,7 +470,7 @@ __global__ void __launch_bounds__(kQueueThreads) k_lu_queue(DevPlan dp, const do
     if (t >= ntasks) break;
     const int2 task = tasks[t];
     if (task.y == 0) {
-      lu_cta_unit<kQueueThreads>(dp, vals, units[task.x], qsm, s_best, s_val, s_bi);
+      lu_cta_unit<kQueueThreads, kLuRowsMax / 32>(dp, vals, units[task.x], qsm, s_best, s_val, s_bi);
     } else if (warp < task.y) {
       lu_warp_unit<1>(dp, vals, units[task.x + warp], qsm + static_cast<size_t>(warp) * 32 * 32);
     }
@@ -746,7 +775,7 @@ int32_t small_unit_max() {
   const int64_t budget = optin - 2048;
   int32_t m = 1;
   while (static_cast<int64_t>(m + 1) * (m + 1) * 8 <= budget) ++m;
-  return m;
+  return std::min<int32_t>(m, kLuRowsMax);  // the kernels' row registers cover kLuRowsMax
 }
 
 Engine::Engine() {
@@ -901,11 +930,18 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
       const int dyn = optin - 2048;
-      attr_err = cudaFuncSetAttribute(k_lu_small<kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      attr_err = cudaFuncSetAttribute(k_lu_small<kThreads, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_lu_small<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        attr_err = cudaFuncSetAttribute(k_lu_small<kThreads, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_lu_small<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        attr_err = cudaFuncSetAttribute(k_lu_small<kThreads, kLuRowsMax / 32>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_lu_small<128, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_lu_small<128, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_lu_small<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_solve_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
@@ -1009,9 +1045,13 @@ void Engine::launch_lu_small(int threads, int32_t units, int32_t mb, cudaStream_
     k_lu_rows<96><<<units, 96, smem, st>>>(dp_, d_vals, list);
     return;
   }
-  if (threads == 64) k_lu_small<64><<<units, 64, smem, st>>>(dp_, d_vals, list);
-  else if (threads == 128) k_lu_small<128><<<units, 128, smem, st>>>(dp_, d_vals, list);
-  else k_lu_small<kThreads><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
+  // Rows per lane of the update: the bucket's largest unit, rounded up.
+  if (threads == 64) k_lu_small<64, 2><<<units, 64, smem, st>>>(dp_, d_vals, list);
+  else if (threads == 128 && mb <= 96) k_lu_small<128, 3><<<units, 128, smem, st>>>(dp_, d_vals, list);
+  else if (threads == 128) k_lu_small<128, 4><<<units, 128, smem, st>>>(dp_, d_vals, list);
+  else if (mb <= 96) k_lu_small<kThreads, 3><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
+  else if (mb <= 128) k_lu_small<kThreads, 4><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
+  else k_lu_small<kThreads, kLuRowsMax / 32><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
 }
 
 // The autotuner keeps one width per size class (the bucket cuts of the plan
