@@ -523,10 +523,13 @@ __global__ void k_solve_scalar(DevPlan dp, const int32_t* __restrict__ rows, int
 // registers and each finished unknown broadcast by a shuffle, and writes x.
 // The backward sweep multiplies by the reciprocal of the pivot, which keeps
 // the division off the dependent chain.
-constexpr int kSlots = 6;  // rows per lane: units up to 192 rows
-static_assert(32 * kSlots >= 170, "register slots must cover the shared-memory LU limit");
+// kS rows per lane, chosen per launch from the level's largest unit: units
+// up to 32 kS rows; at most kSlots (192 rows).
+constexpr int kSlots = 6;
+static_assert(32 * kSlots >= kLuRowsMax, "register slots must cover the small-unit limit");
 
-__global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int32_t* __restrict__ units,
+template <int kS>
+__global__ void __launch_bounds__(kThreads, 4) k_solve_dense(DevPlan dp, const int32_t* __restrict__ units,
                                                            const double* __restrict__ rhs, int32_t ldr,
                                                            double* __restrict__ xp,
                                                            const int32_t* __restrict__ nrhs_p) {
@@ -539,16 +542,16 @@ __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int3
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int kWarps = kThreads / 32;
   const int nmine = (nrhs - warp + kWarps - 1) / kWarps;  // right-hand sides of this warp
-  double a[kSlots];
-  int rows[kSlots];
+  double a[kS];
+  int rows[kS];
 #pragma unroll
-  for (int k = 0; k < kSlots; ++k) {
+  for (int k = 0; k < kS; ++k) {
     const int i = lane + 32 * k;
     rows[k] = (i < m) ? s + dp.lperm[s + i] : -1;
   }
   auto form = [&](int c) {
 #pragma unroll
-    for (int k = 0; k < kSlots; ++k) {
+    for (int k = 0; k < kS; ++k) {
       a[k] = 0.0;
       const int r = rows[k];
       if (r >= 0) {
@@ -606,7 +609,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int3
   }
   // Reciprocals of the pivots, formed in parallel: the backward sweep
   // multiplies, with no division on its dependent chain.
-  __shared__ double rdiag[32 * kSlots];
+  __shared__ double rdiag[32 * kS];
   for (int i = tid; i < m; i += kThreads) rdiag[i] = 1.0 / T[i * m + i];
   __syncthreads();
   for (int t = 0; t < nmine; ++t) {
@@ -614,14 +617,14 @@ __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int3
     if (t > 0) form(c);
     // L: unit lower triangle, columns j = 0 .. m-2.
 #pragma unroll
-    for (int kk = 0; kk < kSlots; ++kk) {
+    for (int kk = 0; kk < kS; ++kk) {
       const int jend = min(32, m - 1 - 32 * kk);
       for (int jj = 0; jj < jend; ++jj) {
         const int j = 32 * kk + jj;
         const double xr = __shfl_sync(0xffffffffu, a[kk], jj);
         const double* col = T + j * m;
 #pragma unroll
-        for (int k = kk; k < kSlots; ++k) {
+        for (int k = kk; k < kS; ++k) {
           const int i = lane + 32 * k;
           if (i > j && i < m) a[k] = fma(-col[i], xr, a[k]);
         }
@@ -629,7 +632,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int3
     }
     // U with its diagonal, columns j = m-1 .. 0.
 #pragma unroll
-    for (int kk = kSlots - 1; kk >= 0; --kk) {
+    for (int kk = kS - 1; kk >= 0; --kk) {
       const int jtop = min(31, m - 1 - 32 * kk);
       for (int jj = jtop; jj >= 0; --jj) {
         const int j = 32 * kk + jj;
@@ -645,7 +648,7 @@ __global__ void __launch_bounds__(kThreads) k_solve_dense(DevPlan dp, const int3
     }
     double* xo = xp + static_cast<size_t>(c) * n + s;
 #pragma unroll
-    for (int k = 0; k < kSlots; ++k) {
+    for (int k = 0; k < kS; ++k) {
       const int i = lane + 32 * k;
       if (i < m) xo[i] = a[k];
     }
@@ -943,7 +946,15 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_lu_small<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_solve_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        attr_err = cudaFuncSetAttribute(k_solve_dense<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_solve_dense<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_solve_dense<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_solve_dense<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      if (attr_err == cudaSuccess)
+        attr_err = cudaFuncSetAttribute(k_solve_dense<kSlots>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_lu_warp<2, kWarpLuW2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         kWarpLuW2 * 64 * 64 * static_cast<int>(sizeof(double)));
@@ -1388,8 +1399,16 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_
     if (has_d) {
       ++launches_solve_;
       const size_t mm = static_cast<size_t>(p.lvl_dense_maxm[static_cast<size_t>(l)]);
-      k_solve_dense<<<d1 - d0, kThreads, mm * mm * sizeof(double) + 16, st_d>>>(dp_, lvl_dense_ + d0, rhs, ldr, xp,
-                                                                                nrhs);
+      const size_t smem = mm * mm * sizeof(double) + 16;
+      const int32_t nu = d1 - d0;
+      const int32_t* lst = lvl_dense_ + d0;
+      switch ((mm + 31) / 32) {
+        case 1: k_solve_dense<1><<<nu, kThreads, smem, st_d>>>(dp_, lst, rhs, ldr, xp, nrhs); break;
+        case 2: k_solve_dense<2><<<nu, kThreads, smem, st_d>>>(dp_, lst, rhs, ldr, xp, nrhs); break;
+        case 3: k_solve_dense<3><<<nu, kThreads, smem, st_d>>>(dp_, lst, rhs, ldr, xp, nrhs); break;
+        case 4: k_solve_dense<4><<<nu, kThreads, smem, st_d>>>(dp_, lst, rhs, ldr, xp, nrhs); break;
+        default: k_solve_dense<kSlots><<<nu, kThreads, smem, st_d>>>(dp_, lst, rhs, ldr, xp, nrhs); break;
+      }
     }
     large_solve_level(dp_, p, l, lvl_large_, lvl_large_tile0_, d_sync_, rhs, ldr, xp, nrhs, wide, st_g,
                       &launches_solve_);
