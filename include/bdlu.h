@@ -310,9 +310,10 @@ int bdlu_server_set_option(bdlu_server* s, const char* key, double value);
  * BDLU_FACTORIZATION_FAILED (a zero or NaN pivot); the X block of every
  * matrix that failed is left unwritten (with X the same buffer as B it still
  * holds B) and the other matrices are solved.  Uses the calling
- * thread's current device; the call waits for `stream` before returning.
- * The first call on a device resolves the scratch's address and sets a kernel
- * attribute, so make it before any stream capture begins.  Every call on a
+ * thread's current device; the call waits for `stream` before returning
+ * (it reads the per-matrix status back), so it can never be called while a
+ * stream capture is active on that stream or in relaxed-capture mode on
+ * the thread.  Every call on a
  * device shares the one scratch, so calls whose work overlaps on the GPU (other
  * streams, other host threads) race and must be serialised by the caller.
  * msg (may be NULL) receives an error message of at most msg_len bytes. */
