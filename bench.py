@@ -797,6 +797,28 @@ def run_serve(args, rank, world):
     open_spec, w1 = open_loop(args.rate, 17)
     open_fit, w2 = open_loop(0.7 * e2e / world, 23)
     worst = max(worst, w1, w2)
+    # The same closed loop (host buffers) on the mixed route from 3xTF32
+    # (server option "precision" 2: tensor-core trailing updates of the large
+    # units, FP64 refinement to the same residual bound), after one 1-rhs and
+    # one 16-rhs warm-up request per pattern at that precision.
+    mixed = None
+    if args.precision == 0:
+        assert srv.set_option("precision", 2), srv.last_error_message()
+        for k, v, B in warm[len(patterns):]:
+            srv.submit(ids[k], v, np.asfortranarray(np.ones(B.shape)))
+        srv.drain()
+        mouts = [B.copy(order="F") for _, _, B in closed]
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        rids = [srv.submit(ids[k], v, X) for (k, v, _), X in zip(closed, mouts)]
+        mres = [srv.wait(r) for r in rids]
+        msecs = max_over_ranks(time.perf_counter() - t0, dist, dev)
+        mst = srv.stats()
+        assert all(r[0] for r in mres), srv.last_error_message()
+        worst = max(worst, max(r[1] for r in mres))
+        mixed = {"precision": 2, "requests": len(closed), "seconds": msecs,
+                 "throughput": world * len(closed) / msecs, "p50_ms": mst["p50_ms"], "p99_ms": mst["p99_ms"],
+                 "host_buffers": True, "worst_residual": max(r[1] for r in mres)}
     srv.close()
     # Plain FP64 GPU path: one request at a time, one Solver per pattern.
     sample = closed[: min(len(closed), 192)]
@@ -863,6 +885,7 @@ def run_serve(args, rank, world):
                                 "peak_concurrency": hstats["peak_concurrency"]},
         "served_open_loop": open_spec,
         "served_open_loop_sustainable": open_fit,
+        "served_mixed_3xtf32": mixed,
         "plain_fp64_path": {"requests": len(sample), "throughput": plain, "host_buffers": True},
         "ratio_served_over_plain": e2e / plain,
         "ratio_served_device_resident_over_plain": value / plain,
