@@ -335,33 +335,48 @@ __device__ __forceinline__ void lu_warp_unit(const DevPlan& dp, const double* __
 }
 
 // Row-per-thread LU: one CTA of M threads per unit of up to M rows (M = 64
-// or 96).  Thread t holds row t of the unit in registers (all M columns,
-// statically indexed: the column loop is unrolled); row swaps are logical as
-// in lu_warp_unit.  Per column: warp candidates (first strict maximum of |a|
-// over the rows not yet pivoted), combined by every thread from shared
-// memory; the pivot row's owner publishes its remaining entries; then each
-// row below forms its multiplier and updates itself.  Two barriers of M
-// threads per column, no shared-memory traffic in the update.  Arithmetic per
+// or 96).  Thread t holds row t of the unit in registers; row swaps are
+// logical as in lu_warp_unit (a row's position is final once it has been the
+// pivot row).  The column loop runs at run time over a compact body: the
+// update walks the row in chunks of kRC columns with constant register
+// indices and skips, by a warp-uniform branch, every chunk left of the
+// current column; multipliers go to the shared staging buffer (column-major,
+// as the factor is written out), so no register is indexed by the column.
+// Per column: warp candidates (first strict maximum of |a| over the rows not
+// yet pivoted), combined by every thread from shared memory; the pivot row's
+// owner publishes its remaining entries; each row below forms its multiplier
+// and updates itself.  Two barriers of M threads per column.  Arithmetic per
 // element is the micro-kernel's, so the factors, pivots and row order are
-// bit-identical to k_lu_small's.  The column loop is a fold over one
-// template instance per column (RowsLu::step<K>), so every index into the
-// register row is a constant and the row never leaves the registers.
+// bit-identical to k_lu_small's.
+constexpr int kRC = 8;  // columns per register chunk of k_lu_rows
 template <int M>
-struct RowsLu {
-  static_assert(M % 32 == 0 && M <= 96, "rows per unit");
-  static constexpr int kW = M / 32;
-  static constexpr int kNone = 1 << 20;
-  double* s_u;
-  double* s_best;
-  int* s_pos;
-  int32_t* piv;
-  int m, t, lane, warp, pos;
-  // Column K; false when the unit is done (K >= m) or failed.
-  template <int K>
-  __device__ __forceinline__ bool step(double (&a)[M], int& status) {
-    if (K >= m) return false;
-    const bool cand = pos >= K && pos != kNone;
-    double best = cand ? fabs(a[K]) : 0.0;
+__global__ void __launch_bounds__(M) k_lu_rows(DevPlan dp, const double* __restrict__ vals,
+                                               const int32_t* __restrict__ units) {
+  static_assert(M % 32 == 0 && M % kRC == 0 && M <= 96, "rows per unit");
+  constexpr int kW = M / 32, kChunks = M / kRC;
+  constexpr int kNone = 1 << 20;
+  extern __shared__ double S[];  // m x m: the unit's entries, then the multipliers
+  __shared__ __align__(16) double s_u[M];  // the pivot row of the current column
+  __shared__ double s_best[kW];
+  __shared__ int s_pos[kW];
+  const int u = units[blockIdx.x];
+  const int s = dp.ustart[u];
+  const int m = dp.ustart[u + 1] - s;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int i = t; i < m * m; i += M) S[i] = 0.0;
+  __syncthreads();
+  for (int64_t e = dp.dent_ptr[u] + t; e < dp.dent_ptr[u + 1]; e += M) S[dp.dent_pos[e]] = vals[dp.dent_src[e]];
+  __syncthreads();
+  double a[M];
+#pragma unroll
+  for (int j = 0; j < M; ++j) a[j] = (t < m && j < m) ? S[j * m + t] : 0.0;
+  __syncthreads();  // S now takes the multipliers
+  int pos = t < m ? t : kNone;
+  double ak = a[0];  // this row's entry in the current column
+  int32_t* piv = dp.piv + s;
+  for (int k = 0; k < m; ++k) {
+    const bool cand = pos >= k && pos != kNone;
+    double best = cand ? fabs(ak) : 0.0;
     int bpos = cand ? pos : kNone;
     warp_pivot_reduce(best, bpos, kNone);
     if (lane == 0) {
@@ -373,66 +388,64 @@ struct RowsLu {
     bpos = s_pos[0];
 #pragma unroll
     for (int w = 1; w < kW; ++w) pivot_combine(best, bpos, s_best[w], s_pos[w], kNone);
-    if (bpos == kNone || best == 0.0) {
-      status = 1;
-      return false;
+    if (bpos == kNone || best == 0.0) {  // CTA-uniform
+      if (t == 0) report_failure(dp.status, u);
+      return;
     }
     const int p = bpos;
     if (pos == p) {
+      s_u[k] = ak;
 #pragma unroll
-      for (int j = K; j < M; ++j)
-        if (j < m) s_u[j] = a[j];
+      for (int c = 0; c < kChunks; ++c) {
+        if (kRC * c + kRC - 1 <= k) continue;  // uniform
+#pragma unroll
+        for (int e = 0; e < kRC; ++e) {
+          const int j = kRC * c + e;
+          if (j > k && j < m) s_u[j] = a[j];
+        }
+      }
     }
-    if (t == 0) piv[K] = p;
-    if (pos == K) pos = p;
-    else if (pos == p) pos = K;
+    if (t == 0) piv[k] = p;
+    if (pos == k) pos = p;
+    else if (pos == p) pos = k;
     __syncthreads();
-    if (pos > K && pos != kNone) {
-      const double l = __ddiv_rn(a[K], s_u[K]);
-      a[K] = l;
+    double nk = 0.0;
+    if (pos > k && pos != kNone) {
+      const double l = __ddiv_rn(ak, s_u[k]);
+      S[k * m + t] = l;
 #pragma unroll
-      for (int j = K + 1; j < M; ++j)
-        if (j < m) a[j] = __dsub_rn(a[j], __dmul_rn(l, s_u[j]));
+      for (int c = 0; c < kChunks; ++c) {
+        if (kRC * c + kRC - 1 <= k || kRC * c >= m) continue;  // uniform
+        if (kRC * c > k && kRC * c + kRC <= m) {
+#pragma unroll
+          for (int e = 0; e < kRC; ++e) {
+            const int j = kRC * c + e;
+            a[j] = __dsub_rn(a[j], __dmul_rn(l, s_u[j]));
+            if (j == k + 1) nk = a[j];
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < kRC; ++e) {
+            const int j = kRC * c + e;
+            if (j > k && j < m) {
+              a[j] = __dsub_rn(a[j], __dmul_rn(l, s_u[j]));
+              if (j == k + 1) nk = a[j];
+            }
+          }
+        }
+      }
     }
-    return true;
+    ak = nk;
   }
-  template <int... Ks>
-  __device__ __forceinline__ void run(double (&a)[M], int& status, std::integer_sequence<int, Ks...>) {
-    (void)(step<Ks>(a, status) && ...);
-  }
-};
-
-template <int M>
-__global__ void __launch_bounds__(M) k_lu_rows(DevPlan dp, const double* __restrict__ vals,
-                                               const int32_t* __restrict__ units) {
-  extern __shared__ double S[];
-  __shared__ double s_u[M];
-  __shared__ double s_best[M / 32];
-  __shared__ int s_pos[M / 32];
-  const int u = units[blockIdx.x];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const int t = threadIdx.x;
-  for (int i = t; i < m * m; i += M) S[i] = 0.0;
-  __syncthreads();
-  for (int64_t e = dp.dent_ptr[u] + t; e < dp.dent_ptr[u + 1]; e += M) S[dp.dent_pos[e]] = vals[dp.dent_src[e]];
-  __syncthreads();
-  double a[M];
-#pragma unroll
-  for (int j = 0; j < M; ++j) a[j] = (t < m && j < m) ? S[j * m + t] : 0.0;
-  RowsLu<M> lu{s_u, s_best, s_pos, dp.piv + s, m, t, t & 31, t >> 5, t < m ? t : RowsLu<M>::kNone};
-  int status = 0;
-  lu.run(a, status, std::make_integer_sequence<int, M>{});
-  if (status) {
-    if (t == 0) report_failure(dp.status, u);
-    return;
-  }
+  // Row t sits at position `pos`, the step at which it was the pivot row:
+  // its multipliers (columns before pos) are in S, its row of U in registers.
   if (t < m) {
     double* out = dp.lu + dp.lu_off[u];
+    for (int j = 0; j < pos; ++j) out[static_cast<size_t>(j) * m + pos] = S[j * m + t];
 #pragma unroll
     for (int j = 0; j < M; ++j)
-      if (j < m) out[static_cast<size_t>(j) * m + lu.pos] = a[j];
-    dp.lperm[s + lu.pos] = t;
+      if (j >= pos && j < m) out[static_cast<size_t>(j) * m + pos] = a[j];
+    dp.lperm[s + pos] = t;
   }
 }
 
