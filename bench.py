@@ -542,7 +542,7 @@ def run_batch(args, rank, world):
         "e2e": {"value": e2e, "unit": BATCH_METRIC, "h2d_bytes_per_step": 8 * nnz + 8 * N * BATCH_NRHS,
                 "d2h_bytes_per_step": 8 * N * BATCH_NRHS},
         "phases_ms": ph, "residual_inf_max": worst, "roofline": roofline, "cpu_baseline": cpu,
-        "clocks": clocks.summary(), "gpu_launches": int(sum(launches)),
+        "clocks": clocks.summary(), "gpu_launches": int(sum(launches)), "tuner": bd.tuner_report(),
     }
     print(json.dumps(line), flush=True)
     if dist:
