@@ -417,10 +417,19 @@ __global__ void __launch_bounds__(M) k_lu_rows(DevPlan dp, const double* __restr
       for (int c = 0; c < kChunks; ++c) {
         if (kRC * c + kRC - 1 <= k || kRC * c >= m) continue;  // uniform
         if (kRC * c > k && kRC * c + kRC <= m) {
+          // The chunk of the pivot row first (16-byte loads), then the
+          // arithmetic: the loads overlap instead of each update waiting.
+          double uc[kRC];
+#pragma unroll
+          for (int e = 0; e < kRC; e += 2) {
+            const double2 v = *reinterpret_cast<const double2*>(s_u + kRC * c + e);
+            uc[e] = v.x;
+            uc[e + 1] = v.y;
+          }
 #pragma unroll
           for (int e = 0; e < kRC; ++e) {
             const int j = kRC * c + e;
-            a[j] = __dsub_rn(a[j], __dmul_rn(l, s_u[j]));
+            a[j] = __dsub_rn(a[j], __dmul_rn(l, uc[e]));
             if (j == k + 1) nk = a[j];
           }
         } else {
