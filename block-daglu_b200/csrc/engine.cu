@@ -83,10 +83,9 @@ __device__ __forceinline__ void warp_pivot_signed(double v, int i, int none, dou
   bi = idx;
 }
 
-// One unit factored by the whole CTA (kT threads, kT >= m, m <= 32 kR): A is
-// the CTA's m*m shared-memory slot.  A failed unit reports and returns
-// (CTA-uniform).
-template <int kT, int kR>
+// One unit factored by the whole CTA (kT threads, kT >= m): A is the CTA's
+// m*m shared-memory slot.  A failed unit reports and returns (CTA-uniform).
+template <int kT>
 __device__ __forceinline__ void lu_cta_unit(const DevPlan& dp, const double* __restrict__ vals, int u, double* A,
                                             double* s_best, double* s_val, int* s_bi) {
   const int s = dp.ustart[u];
@@ -150,45 +149,33 @@ __device__ __forceinline__ void lu_cta_unit(const DevPlan& dp, const double* __r
     for (int i = k + 1 + tid; i < m; i += kT) colk[i] = __ddiv_rn(i == p ? akk : colk[i], pv);
     __syncthreads();
     if (tid == 0) colk[k] = pv;
-    // Update: warp per column (column k+1 is warp 0's, which also yields the
-    // next pivot candidates), lane per row (rows k+1+lane+32r, r < kR).  A
-    // warp takes kCC of its columns at a time and loads all their entries
-    // before it computes, so the shared-memory loads overlap.
+    // Update of the active (m-k-1) x (m-k-1) block, spread evenly over the
+    // CTA: element e = tid + kT q is row k+1 + e % nr of column k+1 + e / nr
+    // (column-major, so a warp's loads and stores are consecutive), the row
+    // and column advanced incrementally.  Every issued update is a real one.
+    // Column k+1's entries (e < nr) also yield the next pivot candidates.
     double cb = 0.0, cv = 0.0;
     int ci = m;
-    {
-      constexpr int kWarps = kT / 32, kCC = 4;
-      const int i0 = k + 1 + lane;
-      double l[kR];
-#pragma unroll
-      for (int r = 0; r < kR; ++r) l[r] = (i0 + 32 * r < m) ? colk[i0 + 32 * r] : 0.0;
-      for (int j0 = k + 1 + warp; j0 < m; j0 += kWarps * kCC) {
-        double ukj[kCC], x[kCC][kR];
-#pragma unroll
-        for (int c = 0; c < kCC; ++c) {
-          const int j = j0 + c * kWarps;
-          const double* col = A + static_cast<size_t>(j) * m;
-          ukj[c] = (j < m) ? col[k] : 0.0;
-#pragma unroll
-          for (int r = 0; r < kR; ++r) x[c][r] = (j < m && i0 + 32 * r < m) ? col[i0 + 32 * r] : 0.0;
+    const int nr = m - k - 1;
+    if (nr > 0) {
+      const int ne = nr * nr;
+      const int sr = kT % nr, sc = kT / nr;
+      int ii = tid % nr, jj = tid / nr;
+      for (int e = tid; e < ne; e += kT) {
+        const int i = k + 1 + ii;
+        double* c = A + static_cast<size_t>(k + 1 + jj) * m;
+        const double v = __dsub_rn(c[i], __dmul_rn(colk[i], c[k]));
+        c[i] = v;
+        if (jj == 0 && (ci == m || fabs(v) > cb)) {
+          cb = fabs(v);
+          cv = v;
+          ci = i;
         }
-#pragma unroll
-        for (int c = 0; c < kCC; ++c) {
-          const int j = j0 + c * kWarps;
-          double* col = A + static_cast<size_t>(j) * m;
-#pragma unroll
-          for (int r = 0; r < kR; ++r) {
-            const int i = i0 + 32 * r;
-            if (j < m && i < m) {
-              const double v = __dsub_rn(x[c][r], __dmul_rn(l[r], ukj[c]));
-              col[i] = v;
-              if (j == k + 1 && (ci == m || fabs(v) > cb)) {
-                cb = fabs(v);
-                cv = v;
-                ci = i;
-              }
-            }
-          }
+        ii += sr;
+        jj += sc;
+        if (ii >= nr) {
+          ii -= nr;
+          ++jj;
         }
       }
     }
@@ -223,13 +210,13 @@ __device__ __forceinline__ void lu_cta_unit(const DevPlan& dp, const double* __r
   for (int k = tid; k < m; k += kT) dp.lperm[s + k] = ord[k];
 }
 
-template <int kT, int kR>
+template <int kT>
 __global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __restrict__ vals,
                                                   const int32_t* __restrict__ units) {
   extern __shared__ double A[];
   __shared__ double s_best[kT / 32], s_val[kT / 32];
   __shared__ int s_bi[kT / 32];
-  lu_cta_unit<kT, kR>(dp, vals, units[blockIdx.x], A, s_best, s_val, s_bi);
+  lu_cta_unit<kT>(dp, vals, units[blockIdx.x], A, s_best, s_val, s_bi);
 }
 
 // ---------------------------------------------------------------------------
@@ -492,7 +479,7 @@ __global__ void __launch_bounds__(kQueueThreads) k_lu_queue(DevPlan dp, const do
     if (t >= ntasks) break;
     const int2 task = tasks[t];
     if (task.y == 0) {
-      lu_cta_unit<kQueueThreads, kLuRowsMax / 32>(dp, vals, units[task.x], qsm, s_best, s_val, s_bi);
+      lu_cta_unit<kQueueThreads>(dp, vals, units[task.x], qsm, s_best, s_val, s_bi);
     } else if (warp < task.y) {
       lu_warp_unit<1>(dp, vals, units[task.x + warp], qsm + static_cast<size_t>(warp) * 32 * 32);
     }
@@ -955,18 +942,11 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
       const int dyn = optin - 2048;
-      attr_err = cudaFuncSetAttribute(k_lu_small<kThreads, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+      attr_err = cudaFuncSetAttribute(k_lu_small<kThreads>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_lu_small<kThreads, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        attr_err = cudaFuncSetAttribute(k_lu_small<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_lu_small<kThreads, kLuRowsMax / 32>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-      if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_lu_small<128, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-      if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_lu_small<128, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
-      if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_lu_small<64, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        attr_err = cudaFuncSetAttribute(k_lu_small<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_solve_dense<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
@@ -1078,13 +1058,9 @@ void Engine::launch_lu_small(int threads, int32_t units, int32_t mb, cudaStream_
     k_lu_rows<96><<<units, 96, smem, st>>>(dp_, d_vals, list);
     return;
   }
-  // Rows per lane of the update: the bucket's largest unit, rounded up.
-  if (threads == 64) k_lu_small<64, 2><<<units, 64, smem, st>>>(dp_, d_vals, list);
-  else if (threads == 128 && mb <= 96) k_lu_small<128, 3><<<units, 128, smem, st>>>(dp_, d_vals, list);
-  else if (threads == 128) k_lu_small<128, 4><<<units, 128, smem, st>>>(dp_, d_vals, list);
-  else if (mb <= 96) k_lu_small<kThreads, 3><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
-  else if (mb <= 128) k_lu_small<kThreads, 4><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
-  else k_lu_small<kThreads, kLuRowsMax / 32><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
+  if (threads == 64) k_lu_small<64><<<units, 64, smem, st>>>(dp_, d_vals, list);
+  else if (threads == 128) k_lu_small<128><<<units, 128, smem, st>>>(dp_, d_vals, list);
+  else k_lu_small<kThreads><<<units, kThreads, smem, st>>>(dp_, d_vals, list);
 }
 
 // The autotuner keeps one width per size class (the bucket cuts of the plan
