@@ -164,6 +164,39 @@ def test_server_device_resident_requests_match_host_requests(cuda_device):
 
 
 @pytest.mark.gpu
+def test_server_mixed_route_on_large_units(cuda_device):
+    """The server's mixed route from 3xTF32 (option "precision" 2) on a
+    pattern whose units are all above the shared-memory limit (tensor-core
+    trailing updates): every request meets the residual bound, the residual
+    it reports is the one of the returned solution, and the solution agrees
+    with a plain FP64 Solver's (the refinement bound, 1e-12 relative residual,
+    leaves a forward error up to cond * 1e-12: relative 1e-6 here)."""
+    g = bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(0, 31), 3000, 6)
+    rng = np.random.default_rng(12)
+    reqs = [(0, g.perturbed(20_000 + r), np.asfortranarray(rng.uniform(-1.0, 1.0, (g.n, 1 + r % 3))))
+            for r in range(6)]
+    s = bd.Server(64 << 30, 2)
+    assert s.set_option("precision", 2)
+    assert s.add_pattern((g.rows, g.cols, g.vals), g.n) == 0, s.last_error_message()
+    outs = [B.copy(order="F") for _, _, B in reqs]
+    rids = [s.submit(k, v, X) for (k, v, _), X in zip(reqs, outs)]
+    res = [s.wait(r) for r in rids]
+    s.close()
+    ref = bd.Solver()
+    assert ref.set_matrix((g.rows, g.cols, g.vals), g.n) and ref.analyze() and ref.factor(), ref.last_error_message()
+    assert ref.stats()["max_unit"] > 169
+    for (k, v, B), X, (ok, resid, _) in zip(reqs, outs, res):
+        assert ok
+        host = max(_relres(g, v, X[:, j], B[:, j]) for j in range(B.shape[1]))
+        assert host <= 1e-12 and 0.0 < resid <= 1e-12, (host, resid)
+        assert resid == pytest.approx(host, rel=0.5), (host, resid)
+        assert ref.refactor_values(v), ref.last_error_message()
+        Xr = B.copy(order="F")
+        assert ref.solve_in_place(Xr), ref.last_error_message()
+        assert np.allclose(X, Xr, rtol=1e-6, atol=1e-6 * np.max(np.abs(Xr)))
+
+
+@pytest.mark.gpu
 def test_server_rejects_non_finite_inputs(cuda_device):
     """NaN or infinity in a request's values or right-hand sides fails that
     request with NonFiniteValue (the check runs while the inputs are staged);
