@@ -1007,9 +1007,9 @@ def measure_circuit(args, world, dist, dev):
         assert s.refactor_values_device(d_vals[k].data_ptr(), nnz, sh), s.last_error_message()
         assert s.solve_device(d_x.data_ptr(), g.n, 1, sh), s.last_error_message()
 
-    # Untimed: four host-buffer refactor + solve calls (the autotuner's trials
+    # Untimed: six host-buffer refactor + solve calls (the autotuner's trials
     # of the large-unit refactor schedule), then the device-path warm-up.
-    for k in range(4):
+    for k in range(6):
         v, b = inputs[k % total]
         x = b.copy()
         assert s.refactor_values(v) and s.solve_in_place(x), s.last_error_message()

@@ -83,7 +83,7 @@ bool schedule_tunable(const bdlu_solver* h) {
 }
 
 // Schedule of the next value-only refactor: the caller's, the tuned one, or
-// the next trial (chain, graph, chain, graph).
+// the next trial (chain, graph, chain, graph, chain, graph).
 int32_t schedule_for(bdlu_solver* h) {
   if (!schedule_tunable(h)) return h->refactor_schedule;
   const int t = Tuner::get().refactor_schedule(h->sig);
@@ -92,13 +92,17 @@ int32_t schedule_for(bdlu_solver* h) {
 }
 
 // After a refactor that reused the pivot order completed: a trial's device
-// time; after the fourth trial the faster schedule is kept for the pattern.
+// time.  The first trial of each schedule captures its graph and is not
+// counted; each schedule's time is the faster of its next two, and after the
+// sixth trial the faster schedule is kept for the pattern.
+constexpr int kScheduleTrials = 6;
 void record_schedule(bdlu_solver* h, int32_t used) {
   if (!schedule_tunable(h) || !h->engine->last_factor_reused()) return;
   Tuner& tu = Tuner::get();
   if (tu.refactor_schedule(h->sig) >= 0 || (h->sched_trials & 1) != used) return;
-  h->sched_ms[used] = h->engine->last_factor_ms();
-  if (++h->sched_trials == 4) {
+  const float ms = h->engine->last_factor_ms();
+  if (h->sched_trials >= 2) h->sched_ms[used] = h->sched_trials < 4 ? ms : std::min(h->sched_ms[used], ms);
+  if (++h->sched_trials == kScheduleTrials) {
     const int best = h->sched_ms[1] < h->sched_ms[0] ? 1 : 0;
     tu.set_refactor_schedule(h->sig, best, h->sched_ms[0], h->sched_ms[1]);
   }

@@ -42,7 +42,8 @@ def test_tuner_picks_lu_small_widths(cuda_device, monkeypatch):
 
 def test_tuner_picks_refactor_schedule_per_pattern(cuda_device, monkeypatch):
     # One 2,000-row large unit: its value-only refactors run the step chain
-    # and the tile task graph in turn (4 trials), then the faster stays.
+    # and the tile task graph in turn (6 trials: a capture trial and two
+    # timed trials each), then the faster stays.
     monkeypatch.setenv("BLOCKDAGLU_MODE", "klu")
     g = bd.Synth(bd.FAMILY_BLOCK, bd.config_seed(0, 51), 2000, 40)
     s = bd.Solver()
