@@ -103,7 +103,9 @@ void record_schedule(bdlu_solver* h, int32_t used) {
   const float ms = h->engine->last_factor_ms();
   if (h->sched_trials >= 2) h->sched_ms[used] = h->sched_trials < 4 ? ms : std::min(h->sched_ms[used], ms);
   if (++h->sched_trials == kScheduleTrials) {
-    const int best = h->sched_ms[1] < h->sched_ms[0] ? 1 : 0;
+    // The chain is the default: the graph must win by more than 2 %, so
+    // trial noise between two close schedules does not flip the choice.
+    const int best = h->sched_ms[1] < 0.98f * h->sched_ms[0] ? 1 : 0;
     tu.set_refactor_schedule(h->sig, best, h->sched_ms[0], h->sched_ms[1]);
   }
 }

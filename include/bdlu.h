@@ -361,7 +361,8 @@ int bdlu_matrix_signatures(const bdlu_solver* h, uint64_t* sigs);
  * tile task graph,
  * decided over the pattern's first six refactors that wait for their
  * status: the faster of two steady trials each, after one capture trial
- * each).  Choices persist in $BDLU_TUNE_CACHE, else
+ * each; the tile task graph replaces the chain only if it is more than 2 %
+ * faster).  Choices persist in $BDLU_TUNE_CACHE, else
  * $HOME/.cache/bdlu/tune-<gpu>.json; BDLU_AUTOTUNE=0 disables tuning.
  * bdlu_tuner_report writes the choices as JSON (NUL-terminated, at most len
  * bytes) and returns the bytes needed including the NUL. */

@@ -65,7 +65,7 @@ def test_tuner_picks_refactor_schedule_per_pattern(cuda_device, monkeypatch):
     assert len(entry) == 1, rep
     e = entry[0]
     assert e["schedule"] in (0, 1) and e["ms_chain"] > 0.0 and e["ms_graph"] > 0.0
-    assert e["schedule"] == (1 if e["ms_graph"] < e["ms_chain"] else 0)
+    assert e["schedule"] == (1 if e["ms_graph"] < 0.98 * e["ms_chain"] else 0)
     assert os.path.exists(rep["cache"])
 
 
