@@ -275,6 +275,74 @@ int or_factor(or_system* s) {
   return 1;
 }
 
+/* or_gp_lu / or_gp_gate (gp_oracle.c). */
+typedef struct or_gp_stats { int32_t ok, row_swaps, tiny_pivots, zero_pivots; double min_abs_diag; } or_gp_stats;
+int or_gp_lu(int32_t m, const int32_t* col_ptr, const int32_t* row_ind, const double* val, int32_t scale,
+             double diag_prefer_tol, double pivot_tol, double perturb, double drop_tol, double* lu, int32_t* piv,
+             double* row_scale, or_gp_stats* st);
+int or_gp_gate(const or_gp_stats* st, int32_t m, int32_t require_no_swaps, int32_t swap_max_n, int32_t swap_max,
+               int32_t require_no_tiny, double min_abs_diag);
+
+/* Factors every block as factor_one_block does with the sparse-LU route on
+ * (USERALGO_SPARSE_LU_KERNEL=gp, ubtf_block_solver.cpp:1439-1498 and
+ * :1749-1773) under the default gate: blocks of at most dense_max rows by the
+ * dense micro-kernel; blocks of up to gp_max_n rows by or_gp_lu (no scaling,
+ * no dropping), kept when the gate accepts it (no row swaps, no tiny pivots,
+ * smallest |pivot| >= min_abs_diag); every other block by the dense
+ * partial-pivoting micro-kernel, the stand-in for the reference's KLU.
+ * Accepted factors are stored like dense ones (row-major LU, LAPACK-style
+ * pivots), so the block solve is or_dense_solve: a row-oriented sweep in
+ * ascending column order, the order of gp_lu_solve_inplace_strided
+ * (gp_lu.cpp:242-306).  reason[b] = -1 (not tried) or the gate's reason.
+ * Returns 1, or 0 with failed_block set. */
+int or_factor_gp(or_system* s, int32_t dense_max, int32_t gp_max_n, double diag_tol, double pivot_tol,
+                 double perturb, double min_abs_diag, int32_t* reason) {
+  int32_t b;
+  int64_t total = 0;
+  s->lu_off = (int64_t*)malloc(sizeof(int64_t) * (s->nblocks + 1));
+  for (b = 0; b < s->nblocks; ++b) {
+    const int64_t m = s->R[b + 1] - s->R[b];
+    s->lu_off[b] = total;
+    total += m * m;
+  }
+  s->lu_off[s->nblocks] = total;
+  s->lu = (double*)calloc((size_t)(total + 1), sizeof(double));
+  s->piv = (int32_t*)calloc((size_t)s->n + 1, sizeof(int32_t));
+  for (b = 0; b < s->nblocks; ++b) {
+    const int32_t m = s->R[b + 1] - s->R[b];
+    double* a = s->lu + s->lu_off[b];
+    int64_t q;
+    reason[b] = -1;
+    if (m > dense_max && m <= gp_max_n) {
+      /* Block CSC (coo_to_csc_i32) and the sparse LU with its gate. */
+      int32_t* cp = (int32_t*)calloc((size_t)m + 1, sizeof(int32_t));
+      const int64_t cnt = s->diag_ptr[b + 1] - s->diag_ptr[b];
+      int32_t* ri = (int32_t*)malloc(sizeof(int32_t) * (size_t)(cnt + 1));
+      double* rv = (double*)malloc(sizeof(double) * (size_t)(cnt + 1));
+      double* rs = (double*)malloc(sizeof(double) * (size_t)m);
+      int32_t* nx = (int32_t*)malloc(sizeof(int32_t) * (size_t)m);
+      or_gp_stats st;
+      int32_t c;
+      for (q = s->diag_ptr[b]; q < s->diag_ptr[b + 1]; ++q) cp[s->diag_c[q] + 1]++;
+      for (c = 0; c < m; ++c) cp[c + 1] += cp[c];
+      memcpy(nx, cp, sizeof(int32_t) * (size_t)m);
+      for (q = s->diag_ptr[b]; q < s->diag_ptr[b + 1]; ++q) {
+        const int32_t k = nx[s->diag_c[q]]++;
+        ri[k] = s->diag_r[q];
+        rv[k] = s->diag_v[q];
+      }
+      or_gp_lu(m, cp, ri, rv, 0, diag_tol, pivot_tol, perturb, 0.0, a, s->piv + s->R[b], rs, &st);
+      reason[b] = or_gp_gate(&st, m, 1, 256, 0, 1, min_abs_diag);
+      free(cp); free(ri); free(rv); free(rs); free(nx);
+      if (reason[b] == 0) continue;
+      memset(a, 0, sizeof(double) * (size_t)m * (size_t)m);
+    }
+    for (q = s->diag_ptr[b]; q < s->diag_ptr[b + 1]; ++q) a[(size_t)s->diag_r[q] * m + s->diag_c[q]] += s->diag_v[q];
+    if (!or_dense_lu(a, s->piv + s->R[b], m)) { s->failed_block = b; return 0; }
+  }
+  return 1;
+}
+
 const double* or_block_lu(const or_system* s, int32_t b, const int32_t** piv, int32_t* m) {
   *m = s->R[b + 1] - s->R[b];
   *piv = s->piv + s->R[b];

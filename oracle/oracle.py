@@ -30,7 +30,7 @@ def load():
     global _lib
     if _lib is not None:
         return _lib
-    srcs = ("bdlu_oracle.c", "btf_oracle.c", "synth_oracle.c")
+    srcs = ("bdlu_oracle.c", "btf_oracle.c", "synth_oracle.c", "gp_oracle.c")
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(os.path.join(HERE, f)) for f in srcs):
         build()
     lib = ctypes.CDLL(LIB)
@@ -59,6 +59,13 @@ def load():
         "or_synth_nnz": (ctypes.c_int64, [vp]),
         "or_synth_copy": (None, [vp, _i32p, _i32p, _f64p, _f64p, _f64p]),
         "or_synth_perturb": (None, [vp, ctypes.c_uint64, _f64p]),
+        "or_gp_lu": (ctypes.c_int, [ctypes.c_int32, _i32p, _i32p, _f64p, ctypes.c_int32, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, _f64p, _i32p, _f64p,
+                                    ctypes.c_void_p]),
+        "or_gp_gate": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.c_int32, ctypes.c_double]),
+        "or_factor_gp": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                        ctypes.c_double, ctypes.c_double, _i32p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -92,6 +99,45 @@ def dense_lu(a):
     piv = np.zeros(m, np.int32)
     ok = lib.or_dense_lu(_p64(lu), _p32(piv), m)
     return bool(ok), lu, piv
+
+
+class _GpStats(ctypes.Structure):
+    _fields_ = [("ok", ctypes.c_int32), ("row_swaps", ctypes.c_int32), ("tiny_pivots", ctypes.c_int32),
+                ("zero_pivots", ctypes.c_int32), ("min_abs_diag", ctypes.c_double)]
+
+
+# GpLuOptions defaults (blockdaglu/src/gp_lu.h:43-49) and the gate's defaults
+# (blockdaglu/src/ubtf_block_solver.cpp:118-157).
+GP_DEFAULTS = dict(scale=0, diag_prefer_tol=1e-3, pivot_tol=1e-12, perturb=1e-12, drop_tol=0.0)
+GP_GATE_DEFAULTS = dict(require_no_swaps=1, swap_max_n=256, swap_max=0, require_no_tiny=1, min_abs_diag=1e-12)
+
+
+def gp_lu(m, col_ptr, row_ind, val, **opts):
+    """Restated gp_lu_factor on an m x m CSC (gp_oracle.c).  Returns (ok, lu,
+    piv, row_scale, stats): lu row-major with L multipliers below the
+    diagonal, piv LAPACK style, stats a dict of the diagnostics."""
+    lib = load()
+    o = dict(GP_DEFAULTS, **opts)
+    cp = np.ascontiguousarray(col_ptr, np.int32)
+    ri = np.ascontiguousarray(row_ind, np.int32)
+    v = np.ascontiguousarray(val, np.float64)
+    lu = np.zeros((m, m))
+    piv = np.zeros(m, np.int32)
+    rs = np.ones(m)
+    st = _GpStats()
+    ok = lib.or_gp_lu(int(m), _p32(cp), _p32(ri), _p64(v), int(o["scale"]), float(o["diag_prefer_tol"]),
+                      float(o["pivot_tol"]), float(o["perturb"]), float(o["drop_tol"]), _p64(lu), _p32(piv), _p64(rs),
+                      ctypes.byref(st))
+    stats = {f: getattr(st, f) for f, _ in _GpStats._fields_}
+    stats["_c"] = st
+    return bool(ok), lu, piv, rs, stats
+
+
+def gp_gate(stats, m, **opts):
+    """Restated gp_gate_eval: 0 accepted, else the reject reason (1-4)."""
+    o = dict(GP_GATE_DEFAULTS, **opts)
+    return int(load().or_gp_gate(ctypes.byref(stats["_c"]), int(m), int(o["require_no_swaps"]), int(o["swap_max_n"]),
+                                 int(o["swap_max"]), int(o["require_no_tiny"]), float(o["min_abs_diag"])))
 
 
 def metrics(rows, cols, vals, x, b, x_true=None, n=None):
@@ -268,6 +314,17 @@ class System:
     def factor(self):
         self._factored = True
         return bool(self._lib.or_factor(self._s))
+
+    def factor_gp(self, dense_max=64, gp_max_n=4096, diag_tol=1e-3, pivot_tol=1e-12, perturb=1e-12,
+                  min_abs_diag=1e-12):
+        """Factor with the reference's sparse-LU route on (or_factor_gp):
+        returns (ok, reason) with reason[b] = -1 (block not tried), 0 (kept)
+        or the gate's reject reason."""
+        self._factored = True
+        reason = np.full(self.nblocks, -1, np.int32)
+        ok = self._lib.or_factor_gp(self._s, int(dense_max), int(gp_max_n), float(diag_tol), float(pivot_tol),
+                                    float(perturb), float(min_abs_diag), _p32(reason))
+        return bool(ok), reason
 
     def failed_block(self):
         return self._lib.or_failed_block(self._s)

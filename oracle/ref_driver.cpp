@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "blockdaglu/solver.h"
+#include "gp_lu.h"
 #include "ubtf_block_solver.h"
 
 using blockdaglu::CooMatrix;
@@ -158,6 +159,85 @@ int ref_block_solve(void* p, double* b, int32_t n, int32_t threads) {
   if (!solve_ubtf(run->dec, run->fac, x, static_cast<size_t>(threads > 0 ? threads : 1))) return 1;
   std::memcpy(b, x.data(), sizeof(double) * static_cast<size_t>(n));
   return 0;
+}
+
+// gp_lu_factor (gp_lu.cpp:84-240) on an m x m CSC with the given options.
+// lu: row-major m*m (L multipliers strictly below the diagonal from L_rows,
+// U on and above from U_rows and Udiag), perm: GpLuFactor::perm, row_scale
+// (1.0 when scaling is off); stats: ok, row swaps, tiny pivots, zero pivots.
+int ref_gp_lu(int32_t m, const int32_t* col_ptr, const int32_t* row_ind, const double* val, int32_t scale,
+              double diag_tol, double pivot_tol, double perturb, double drop_tol, double* lu, int32_t* perm,
+              double* row_scale, int32_t* stats) {
+  CscMatrixI32 a;
+  a.n = m;
+  a.nnz = col_ptr[m];
+  a.col_ptr.assign(col_ptr, col_ptr + m + 1);
+  a.row_ind.assign(row_ind, row_ind + col_ptr[m]);
+  a.values.assign(val, val + col_ptr[m]);
+  GpLuOptions opt;
+  opt.scale = scale;
+  opt.diag_prefer_tol = diag_tol;
+  opt.pivot_tol = pivot_tol;
+  opt.perturb = perturb;
+  opt.drop_tol = drop_tol;
+  GpLuFactor f;
+  const bool ok = gp_lu_factor(a, f, opt);
+  stats[0] = ok ? 1 : 0;
+  stats[1] = f.row_swap_count;
+  stats[2] = f.tiny_pivot_count;
+  stats[3] = f.zero_pivot_count;
+  if (!ok) return 0;
+  std::memset(lu, 0, sizeof(double) * static_cast<size_t>(m) * m);
+  for (int32_t i = 0; i < m; ++i) {
+    for (const auto& e : f.L_rows[static_cast<size_t>(i)]) lu[static_cast<size_t>(i) * m + e.first] = e.second;
+    for (const auto& e : f.U_rows[static_cast<size_t>(i)])
+      if (e.first > i) lu[static_cast<size_t>(i) * m + e.first] = e.second;
+    lu[static_cast<size_t>(i) * m + i] = f.Udiag[static_cast<size_t>(i)];
+    perm[i] = f.perm[static_cast<size_t>(i)];
+    row_scale[i] = f.row_scale.empty() ? 1.0 : f.row_scale[static_cast<size_t>(i)];
+  }
+  return 1;
+}
+
+// gp_lu_solve_inplace_strided (gp_lu.cpp:242-306) after gp_lu_factor with the
+// default options: b (m) is replaced by x.  Returns 1 on success.
+int ref_gp_solve(int32_t m, const int32_t* col_ptr, const int32_t* row_ind, const double* val, double* b) {
+  CscMatrixI32 a;
+  a.n = m;
+  a.nnz = col_ptr[m];
+  a.col_ptr.assign(col_ptr, col_ptr + m + 1);
+  a.row_ind.assign(row_ind, row_ind + col_ptr[m]);
+  a.values.assign(val, val + col_ptr[m]);
+  GpLuFactor f;
+  if (!gp_lu_factor(a, f, GpLuOptions{})) return 0;
+  return gp_lu_solve_inplace_strided(f, b, m, 1) ? 1 : 0;
+}
+
+// Route of block b after ref_factor: 0 dense micro-kernel, 1 sparse LU (GP)
+// accepted, 2 KLU stand-in; *reason = BlockFactor::gp_reject_reason.
+int32_t ref_block_route(void* p, int32_t b, int32_t* reason) {
+  const auto& bf = static_cast<RefRun*>(p)->fac.blocks[static_cast<size_t>(b)];
+  if (reason) *reason = bf.gp_reject_reason;
+  if (!bf.dense_lu.empty()) return 0;
+  return bf.gp ? 1 : 2;
+}
+
+// Factors of a block the sparse-LU route kept, as in ref_gp_lu.  Returns m,
+// or 0 when the block has none.
+int32_t ref_block_gp(void* p, int32_t b, double* lu, int32_t* perm) {
+  const auto& bf = static_cast<RefRun*>(p)->fac.blocks[static_cast<size_t>(b)];
+  if (!bf.gp) return 0;
+  const GpLuFactor& f = *bf.gp;
+  const int32_t m = f.n;
+  std::memset(lu, 0, sizeof(double) * static_cast<size_t>(m) * m);
+  for (int32_t i = 0; i < m; ++i) {
+    for (const auto& e : f.L_rows[static_cast<size_t>(i)]) lu[static_cast<size_t>(i) * m + e.first] = e.second;
+    for (const auto& e : f.U_rows[static_cast<size_t>(i)])
+      if (e.first > i) lu[static_cast<size_t>(i) * m + e.first] = e.second;
+    lu[static_cast<size_t>(i) * m + i] = f.Udiag[static_cast<size_t>(i)];
+    perm[i] = f.perm[static_cast<size_t>(i)];
+  }
+  return m;
 }
 
 }  // extern "C"
