@@ -110,9 +110,14 @@ void record_schedule(bdlu_solver* h, int32_t used) {
   }
 }
 
+int replan_without(bdlu_solver* h, const std::vector<int32_t>& units, const std::vector<int32_t>& reasons,
+                   cudaStream_t stream);
+
 // Factor from the engine's value buffer.  reuse: large blocks keep the pivot
 // order of the last full factorisation (value-only refactor); a zero pivot
-// met that way falls back to a factorisation with pivoting.
+// met that way falls back to a factorisation with pivoting.  A sparse-LU unit
+// that fails its pivot test (the reference's gate would reject it) moves to
+// the dense route: the plan is rebuilt without it and the factor rerun.
 int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   std::string err;
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
@@ -122,6 +127,8 @@ int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   const int32_t sched = schedule_for(h);
   h->engine->set_refactor_schedule(sched);
   h->engine->set_wait_limit(h->wait_limit);
+  h->engine->set_sparse_tests(h->gp.diag_tol, h->gp.pivot_tol, h->gp.min_abs_diag);
+  int replans = 0;
   for (int attempt = 0; attempt < 2; ++attempt) {
     const bool r = reuse && attempt == 0;
     if (!h->engine->factor_async(h->engine->values_buffer(), stream, err, r))
@@ -132,6 +139,17 @@ int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
       h->exported = false;
       if (r) record_schedule(h, sched);
       return BDLU_OK;
+    }
+    if (st == 3 && replans < 2) {
+      std::vector<int32_t> units, reasons;
+      if (!h->engine->sparse_rejections(units, reasons, err)) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+      if (const int e = replan_without(h, units, reasons, stream)) {
+        h->factored = false;
+        return e;
+      }
+      ++replans;
+      --attempt;
+      continue;
     }
     if (st == 2 && r) continue;
     h->factored = false;
@@ -177,6 +195,29 @@ int upload_values(bdlu_solver* h, const double* vals, bool device, cudaStream_t 
                                         device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream);
   if (e != cudaSuccess) return fail(h, BDLU_BACKEND_UNAVAILABLE, std::string("value upload: ") + cudaGetErrorString(e));
   return BDLU_OK;
+}
+
+// Units whose sparse LU failed its pivot test join the dense route for this
+// handle (the reference rejects such a block at its gate and factors it with
+// KLU): the plan is rebuilt without them, with the current values.
+int replan_without(bdlu_solver* h, const std::vector<int32_t>& units, const std::vector<int32_t>& reasons,
+                   cudaStream_t stream) {
+  const bdlu::Plan& old = h->engine->plan();
+  for (size_t i = 0; i < units.size(); ++i) {
+    const int32_t s0 = old.ustart[static_cast<size_t>(units[i])];
+    h->gp.rejected.push_back(s0);
+    h->gp_rejected_reason.emplace_back(s0, reasons[i]);
+  }
+  if (const int st = bdlu_sync_host_values(h)) return st;
+  try {
+    const bdlu::Plan plan = bdlu::build_plan(h->coo, h->dec, bdlu::small_unit_max(), &h->gp);
+    std::string err;
+    if (!h->engine->upload(plan, h->dec, h->coo, err)) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
+  } catch (const std::exception& e) {
+    return fail(h, BDLU_ANALYSIS_FAILED, e.what());
+  }
+  h->engine->set_pattern_key(h->sig);
+  return upload_values(h, h->coo.val.data(), false, stream);
 }
 
 }  // namespace
@@ -225,7 +266,12 @@ int bdlu_analyze_validated(bdlu_solver* h, int mode, const bdlu::PrecomputedBtf*
     if (ce != cudaSuccess || dev_count <= 0)
       return fail(h, BDLU_BACKEND_UNAVAILABLE,
                   std::string("no CUDA device available: ") + (ce != cudaSuccess ? cudaGetErrorString(ce) : "0 devices"));
-    const bdlu::Plan plan = bdlu::build_plan(h->coo, h->dec, bdlu::small_unit_max());
+    h->gp = bdlu::gp_config_from_env();
+    if (h->sparse_lu_opt >= 0) h->gp.mode = h->sparse_lu_opt;
+    if (h->sparse_fill_max > 0.0) h->gp.fill_max = h->sparse_fill_max;
+    if (h->sparse_max_n > 0) h->gp.max_n = h->sparse_max_n;
+    h->gp_rejected_reason.clear();
+    const bdlu::Plan plan = bdlu::build_plan(h->coo, h->dec, bdlu::small_unit_max(), &h->gp);
     if (!h->engine) h->engine = std::make_unique<bdlu::Engine>();
     std::string err;
     if (!h->engine->upload(plan, h->dec, h->coo, err)) return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
@@ -285,7 +331,7 @@ int bdlu_device_restore(bdlu_solver* h) {
   if (h->engine) return BDLU_OK;
   if (h->host_vals_stale) return fail(h, BDLU_BACKEND_UNAVAILABLE, "values were not saved before the device release");
   try {
-    const bdlu::Plan plan = bdlu::build_plan(h->coo, h->dec, bdlu::small_unit_max());
+    const bdlu::Plan plan = bdlu::build_plan(h->coo, h->dec, bdlu::small_unit_max(), &h->gp);
     h->engine = std::make_unique<bdlu::Engine>();
     std::string err;
     if (!h->engine->upload(plan, h->dec, h->coo, err)) {
@@ -693,6 +739,25 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
     if (h->engine) h->engine->set_wait_limit(h->wait_limit);
     return BDLU_OK;
   }
+  if (k == "sparse_lu") {
+    // Sparse-LU route for diagonal blocks, from the next analyze: 0 off,
+    // 1 the reference's route (USERALGO_SPARSE_LU_KERNEL=gp: every block of
+    // USERALGO_DENSE_BLOCK_MAX < m <= USERALGO_GP_MAX_N rows), 2 only blocks
+    // whose no-pivot fill is at most "sparse_fill_max" of m^2.
+    if (value != 0.0 && value != 1.0 && value != 2.0) return BDLU_INVALID_DIMENSION;
+    h->sparse_lu_opt = static_cast<int32_t>(value);
+    return BDLU_OK;
+  }
+  if (k == "sparse_fill_max") {
+    if (!(value > 0.0 && value <= 1.0)) return BDLU_INVALID_DIMENSION;
+    h->sparse_fill_max = value;
+    return BDLU_OK;
+  }
+  if (k == "sparse_max_n") {
+    if (!(value >= 1.0 && value <= 2147483647.0)) return BDLU_INVALID_DIMENSION;
+    h->sparse_max_n = static_cast<int32_t>(value);
+    return BDLU_OK;
+  }
   if (k == "analysis_only") {
     h->analysis_only = value != 0.0;
     return BDLU_OK;
@@ -707,6 +772,25 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
     return BDLU_OK;
   }
   return BDLU_INVALID_DIMENSION;
+}
+
+int32_t bdlu_get_unit_routes(const bdlu_solver* h, int32_t* start, int32_t* route, int32_t* reason, int32_t cap) {
+  if (!h || !h->decomposed || !h->engine) return -BDLU_NOT_PREPARED;
+  const bdlu::Plan& p = h->engine->plan();
+  for (int32_t u = 0; u < p.nunits && u < cap; ++u) {
+    const int32_t s0 = p.ustart[static_cast<size_t>(u)];
+    if (start) start[u] = s0;
+    if (route) route[u] = p.ukind[static_cast<size_t>(u)];
+    if (reason) {
+      int32_t r = p.ukind[static_cast<size_t>(u)] == bdlu::kUnitSparse ? 0 : -1;
+      for (const auto& e : h->gp_rejected_reason)
+        if (e.first == s0) r = e.second;
+      if (std::find(p.gp_symbolic_rejected.begin(), p.gp_symbolic_rejected.end(), u) != p.gp_symbolic_rejected.end())
+        r = 5;
+      reason[u] = r;
+    }
+  }
+  return p.nunits;
 }
 
 int32_t bdlu_btf_order(int32_t n, const int32_t* Ap, const int32_t* Ai, int32_t* P, int32_t* Q, int32_t* R,

@@ -11,6 +11,7 @@
 #include "analysis.h"
 #include "bdlu.h"
 #include "engine.h"
+#include "gp.h"
 
 struct bdlu_solver {
   // Stage flags (solver.h:86-90).
@@ -48,6 +49,15 @@ struct bdlu_solver {
   int32_t lu_small_threads = 0;   // forced shared-memory LU width (0: autotuned; Engine::set_lu_small_width)
   int32_t small_mode = -1;        // small units per bucket (0) or in one queue launch (1); -1 autotuned
   bool blocking_sync = false;     // waits sleep on blocking-sync events (Engine::set_blocking_sync)
+  // Sparse-LU route (gp.h): configuration of the current analysis (the
+  // environment's, overridden by the options below; -1 = not set) and, by
+  // first permuted row, the reasons of units a factor's pivot test sent to
+  // the dense route.
+  bdlu::GpConfig gp;
+  int32_t sparse_lu_opt = -1;
+  double sparse_fill_max = -1.0;
+  int32_t sparse_max_n = -1;
+  std::vector<std::pair<int32_t, int32_t>> gp_rejected_reason;
   // Error state (solver.h:122-123).
   int last_error = BDLU_OK;
   std::string last_message;

@@ -11,6 +11,7 @@ constexpr int kFailZeroPivot = 1;
 constexpr int kFailReusedPivot = 2;  // a reused pivot order met a zero pivot
 constexpr int kFailSync = 3;         // a bounded wait of the solve ran out
 constexpr int kFailRefactorSync = 4; // a bounded wait of the tile-graph refactor ran out
+constexpr int kFailSparseReject = 6; // a sparse-LU unit failed the pivot test (gp.h): factor it dense
 
 __device__ __forceinline__ void report_failure(int32_t* status, int32_t unit) {
   if (atomicCAS(status, 0, kFailZeroPivot) == 0) status[1] = unit;

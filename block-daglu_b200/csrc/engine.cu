@@ -19,6 +19,7 @@
 #include "engine.h"
 
 #include "device_util.cuh"
+#include "gp_dev.h"
 #include "tc_update.cuh"
 #include "tuner.h"
 #include "large.h"
@@ -803,6 +804,8 @@ Engine::Engine() {
   for (auto& e : fork_ev_) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   for (auto& e : ev_) cudaEventCreate(&e);
   for (auto& e : pev_) cudaEventCreate(&e);
+  cudaStreamCreateWithFlags(&gp_stream_, cudaStreamNonBlocking);
+  for (auto& e : gp_ev_) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   if (cudaMallocHost(reinterpret_cast<void**>(&readback_), kReadbackBytes) != cudaSuccess) {
     readback_ = new char[kReadbackBytes];  // pageable: correct, only slower
     readback_pinned_ = false;
@@ -828,6 +831,9 @@ Engine::~Engine() {
   for (auto& e : ev_)
     if (e) cudaEventDestroy(e);
   for (auto& e : pev_)
+    if (e) cudaEventDestroy(e);
+  if (gp_stream_) cudaStreamDestroy(gp_stream_);
+  for (auto& e : gp_ev_)
     if (e) cudaEventDestroy(e);
 }
 
@@ -856,6 +862,12 @@ void Engine::release() {
   queue_tasks_ = 0;
   work_nrhs_ = 0;
   dp_ = DevPlan{};
+  const GpDev keep = gp_;
+  gp_ = GpDev{};
+  gp_.diag_tol = keep.diag_tol;
+  gp_.pivot_tol = keep.pivot_tol;
+  gp_.min_abs_diag = keep.min_abs_diag;
+  lvl_sparse_ = nullptr;
 }
 
 #define BDLU_CUDA(call)                                                      \
@@ -1034,6 +1046,37 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
   }
   lvl_scalar_ = lvl_scalar;
   lvl_dense_ = lvl_dense;
+  if (!plan.sparse_units.empty()) {
+    BDLU_CUDA(gp_setup());
+    GpDev& g = gp_;
+    if (!upload_vec(allocs_, plan.sparse_units, &g.units, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_col0, &g.col0, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_cptr, &g.cptr, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_row, &g.row, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_dpos, &g.dpos, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_aptr, &g.aptr, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_arow, &g.arow, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_asrc, &g.asrc, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_clvl0, &g.clvl0, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_clvlb, &g.clvlb, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_corder, &g.corder, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_lrp, &g.lrp, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_lci, &g.lci, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_lpos, &g.lpos, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_urp, &g.urp, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_uci, &g.uci, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_upos, &g.upos, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_flvl0, &g.flvl0, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_flvlb, &g.flvlb, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_frow, &g.frow, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_blvl0, &g.blvl0, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_blvlb, &g.blvlb, err)) return false;
+    if (!upload_vec(allocs_, plan.gp_brow, &g.brow, err)) return false;
+    if (!alloc_dev(allocs_, static_cast<size_t>(std::max<int64_t>(plan.gp_nnz, 1)), &g.val, err)) return false;
+    if (!alloc_dev(allocs_, plan.sparse_units.size(), &g.gstat, err)) return false;
+    g.maxm = plan.gp_maxm;
+    if (!upload_vec(allocs_, plan.lvl_sparse, &lvl_sparse_, err)) return false;
+  }
   return true;
 }
 
@@ -1207,6 +1250,15 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
   launches_factor_ = 1 + static_cast<int32_t>(p.small_bucket_m.size());
   k_gather<<<grid_for(std::max<int64_t>(ncpl, p.n), kThreads, num_sms_ * 8), kThreads, 0, stream>>>(dp_, d_vals, ncpl);
   BDLU_CUDA(cudaEventRecord(pev_[0], stream));
+  // Sparse units on their own stream beside the dense ones, joined below.
+  const int32_t nsparse = static_cast<int32_t>(p.sparse_units.size());
+  if (nsparse > 0) {
+    BDLU_CUDA(cudaEventRecord(gp_ev_[0], stream));
+    BDLU_CUDA(cudaStreamWaitEvent(gp_stream_, gp_ev_[0], 0));
+    BDLU_CUDA(cudaMemsetAsync(gp_.gstat, 0, static_cast<size_t>(nsparse) * sizeof(int32_t), gp_stream_));
+    BDLU_CUDA(gp_factor_launch(gp_, nsparse, d_vals, d_status_, gp_stream_));
+    BDLU_CUDA(cudaEventRecord(gp_ev_[1], gp_stream_));
+  }
   // One launch per size bucket, shared memory sized to the bucket; the
   // buckets run side by side on the auxiliary streams (forked from and
   // joined back into `stream`), largest units first.
@@ -1270,6 +1322,10 @@ bool Engine::factor_async(const double* d_vals, cudaStream_t stream, std::string
     ++launches_factor_;
     BDLU_CUDA(large_factor(dp_, p, large_list_, stream, &launches_factor_, prec_));
   }
+  if (nsparse > 0) {
+    BDLU_CUDA(cudaStreamWaitEvent(stream, gp_ev_[1], 0));
+    ++launches_factor_;  // the sparse factor
+  }
   BDLU_CUDA(cudaGetLastError());
   BDLU_CUDA(cudaEventRecord(ev_[1], stream));
   factor_timed_ = true;
@@ -1311,6 +1367,10 @@ int Engine::factor_status(cudaStream_t stream, std::string& err) {
     err = "reused pivot order met a zero pivot in diagonal block " + std::to_string(st[1]);
     return 2;
   }
+  if (st[0] == kFailSparseReject) {
+    err = "sparse LU of diagonal block " + std::to_string(st[1]) + " failed its pivot test";
+    return 3;
+  }
   if (st[0] == kFailTensorSync) {
     err = "tensor-core update: a bounded wait for the tensor cores ran out";
     return -1;
@@ -1323,6 +1383,22 @@ int Engine::factor_status(cudaStream_t stream, std::string& err) {
   }
   if (!last_reuse_) have_pivots_ = true;
   return 0;
+}
+
+bool Engine::sparse_rejections(std::vector<int32_t>& units, std::vector<int32_t>& reasons, std::string& err) {
+  units.clear();
+  reasons.clear();
+  const size_t ns = plan_.sparse_units.size();
+  if (ns == 0) return true;
+  std::vector<int32_t> st(ns);
+  BDLU_CUDA(cudaDeviceSynchronize());
+  BDLU_CUDA(cudaMemcpy(st.data(), gp_.gstat, ns * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  for (size_t g = 0; g < ns; ++g)
+    if (st[g] != 0) {
+      units.push_back(plan_.sparse_units[g]);
+      reasons.push_back(st[g]);
+    }
+  return true;
 }
 
 bool Engine::ensure_work(int32_t nrhs, std::string& err) {
@@ -1378,15 +1454,23 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_
     const int32_t s0 = p.lvl_scalar_ptr[static_cast<size_t>(l)], s1 = p.lvl_scalar_ptr[static_cast<size_t>(l) + 1];
     const int32_t d0 = p.lvl_dense_ptr[static_cast<size_t>(l)], d1 = p.lvl_dense_ptr[static_cast<size_t>(l) + 1];
     const int32_t g0 = p.lvl_large_ptr[static_cast<size_t>(l)], g1 = p.lvl_large_ptr[static_cast<size_t>(l) + 1];
-    const bool has_s = s1 > s0, has_d = d1 > d0, has_g = g1 > g0;
-    const int kinds = static_cast<int>(has_s) + static_cast<int>(has_d) + static_cast<int>(has_g);
-    cudaStream_t st_s = stream, st_d = stream, st_g = stream;
+    const int32_t q0 = p.lvl_sparse_ptr.empty() ? 0 : p.lvl_sparse_ptr[static_cast<size_t>(l)];
+    const int32_t q1 = p.lvl_sparse_ptr.empty() ? 0 : p.lvl_sparse_ptr[static_cast<size_t>(l) + 1];
+    const bool has_s = s1 > s0, has_d = d1 > d0, has_g = g1 > g0, has_p = q1 > q0;
+    const int kinds = static_cast<int>(has_s) + static_cast<int>(has_d) + static_cast<int>(has_g) +
+                      static_cast<int>(has_p);
+    cudaStream_t st_s = stream, st_d = stream, st_g = stream, st_p = stream;
     if (kinds > 1) {
       cudaEventRecord(fork_ev_[0], stream);
       int used = 0;
       if (has_d && (has_s)) st_d = aux_[used++];
       if (has_g && (has_s || has_d)) st_g = aux_[used++];
+      if (has_p && (has_s || has_d || has_g)) st_p = aux_[used++];
       for (int q = 0; q < used; ++q) cudaStreamWaitEvent(aux_[q], fork_ev_[0], 0);
+    }
+    if (has_p) {
+      ++launches_solve_;
+      gp_solve_launch(dp_, gp_, lvl_sparse_ + q0, q1 - q0, rhs, ldr, xp, nrhs, st_p);
     }
     if (has_s) {
       ++launches_solve_;
@@ -1412,7 +1496,7 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_
                       &launches_solve_);
     if (kinds > 1) {
       int q = 0;
-      for (cudaStream_t sx : {st_d, st_g}) {
+      for (cudaStream_t sx : {st_d, st_g, st_p}) {
         if (sx == stream) continue;
         cudaEventRecord(aux_ev_[q], sx);
         cudaStreamWaitEvent(stream, aux_ev_[q], 0);
@@ -1579,6 +1663,20 @@ bool Engine::download_unit(int32_t u, std::vector<double>& lu, std::vector<int32
   }
   lu.resize(static_cast<size_t>(m) * m);
   piv.resize(static_cast<size_t>(m));
+  if (plan_.ukind[static_cast<size_t>(u)] == kUnitSparse) {
+    // Expand the column-compressed factor; no row was swapped.
+    const int32_t g = plan_.gp_index[static_cast<size_t>(u)];
+    const int32_t c0 = plan_.gp_col0[static_cast<size_t>(g)];
+    const int32_t e0 = plan_.gp_cptr[static_cast<size_t>(c0)], e1 = plan_.gp_cptr[static_cast<size_t>(c0 + m)];
+    std::vector<double> v(static_cast<size_t>(e1 - e0));
+    BDLU_CUDA(cudaMemcpy(v.data(), gp_.val + e0, v.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    std::fill(lu.begin(), lu.end(), 0.0);
+    for (int32_t j = 0; j < m; ++j)
+      for (int32_t q = plan_.gp_cptr[static_cast<size_t>(c0 + j)]; q < plan_.gp_cptr[static_cast<size_t>(c0 + j) + 1]; ++q)
+        lu[static_cast<size_t>(j) * m + plan_.gp_row[static_cast<size_t>(q)]] = v[static_cast<size_t>(q - e0)];
+    for (int32_t k = 0; k < m; ++k) piv[static_cast<size_t>(k)] = k;
+    return true;
+  }
   BDLU_CUDA(cudaMemcpy(lu.data(), dp_.lu + plan_.lu_off[static_cast<size_t>(u)], lu.size() * sizeof(double),
                        cudaMemcpyDeviceToHost));
   if (plan_.ukind[static_cast<size_t>(u)] == kUnitLarge) {

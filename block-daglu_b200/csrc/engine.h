@@ -8,6 +8,7 @@
 #include <utility>
 #include <vector>
 
+#include "gp.h"
 #include "plan.h"
 
 namespace bdlu {
@@ -86,9 +87,13 @@ class Engine {
   // ignored until one full factorisation has succeeded.
   bool factor_async(const double* d_vals, cudaStream_t stream, std::string& err, bool reuse_pivots = false);
   // Waits for the factor.  Returns 0 (ok), 1 (zero pivot: the matrix is
-  // singular) or 2 (a reused pivot order met a zero pivot: factor again with
-  // pivoting); -1 on a CUDA error.
+  // singular), 2 (a reused pivot order met a zero pivot: factor again with
+  // pivoting) or 3 (a sparse-LU unit failed its pivot test: re-plan it as a
+  // dense unit, see sparse_rejections); -1 on a CUDA error.
   int factor_status(cudaStream_t stream, std::string& err);
+  // After factor_status returned 3: the sparse units whose pivot test failed
+  // (unit ids) and the reasons (gp_dev.h).
+  bool sparse_rejections(std::vector<int32_t>& units, std::vector<int32_t>& reasons, std::string& err);
   bool last_factor_reused() const { return last_reuse_; }
 
   // Enqueues X = A^{-1} B for nrhs columns (column-major, ld ldb, in place),
@@ -116,6 +121,13 @@ class Engine {
   // Small units as per-bucket launches (0) or one persistent launch over a
   // task queue (1); -1: the autotuner's choice for the pattern.
   void set_small_mode(int32_t m) { forced_small_mode_ = m; }
+  // Pivot test of the sparse-LU units (gp.h): diagonal preference, tiny
+  // pivot and smallest pivot thresholds.
+  void set_sparse_tests(double diag_tol, double pivot_tol, double min_abs_diag) {
+    gp_.diag_tol = diag_tol;
+    gp_.pivot_tol = pivot_tol;
+    gp_.min_abs_diag = min_abs_diag;
+  }
   // Pattern signature under which the autotuner keeps this engine's choices.
   void set_pattern_key(uint64_t k) { pattern_key_ = k; }
   // Bound of the waits between tiles (polls; <= 0 restores the default).
@@ -151,7 +163,8 @@ class Engine {
   static constexpr int kPhases = 5;
   void phase_ms(float out[kPhases]);
 
-  // Copies a dense unit's LU (column-major m*m) and pivots to the host.
+  // Copies a unit's LU (column-major m*m; a sparse unit's factor expanded,
+  // with identity pivots) and pivots to the host.
   bool download_unit(int32_t u, std::vector<double>& lu, std::vector<int32_t>& piv, double& scalar,
                      std::string& err);
 
@@ -196,6 +209,12 @@ class Engine {
 
   Plan plan_;
   DevPlan dp_{};
+  // Sparse-LU units (gp_dev.h): device tables, their solve lists by level,
+  // and the stream their factor runs on beside the dense units.
+  GpDev gp_{};
+  const int32_t* lvl_sparse_ = nullptr;
+  cudaStream_t gp_stream_ = nullptr;
+  cudaEvent_t gp_ev_[2] = {nullptr, nullptr};
   std::vector<std::pair<void*, size_t>> allocs_;  // device allocations and their bytes
   double* d_vals_ = nullptr;
   double* d_vals_stage_ = nullptr;

@@ -5,6 +5,9 @@
 #include <array>
 #include <climits>
 #include <cmath>
+#include <map>
+
+#include "gp.h"
 
 namespace bdlu {
 
@@ -93,7 +96,7 @@ int64_t build_rtasks(const std::vector<int32_t>& units, const std::vector<int32_
   return static_cast<int64_t>(tasks.size() / 4);
 }
 
-Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max) {
+Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max, const GpConfig* gp) {
   Plan p;
   const int32_t n = d.n;
   p.n = n;
@@ -111,6 +114,56 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
     for (int32_t r = s; r < e; ++r) p.unit_of[static_cast<size_t>(r)] = u;
     p.ukind[static_cast<size_t>(u)] = (m == 1) ? kUnitScalar : (m <= small_max ? kUnitSmall : kUnitLarge);
     p.max_unit = std::max(p.max_unit, m);
+  }
+  const double drop = [&] {
+    const AnalysisOptions o = analysis_options_from_env();
+    return o.drop_abs_lt < 0.0 ? (n >= 50000 ? 1e-20 : 0.0) : o.drop_abs_lt;
+  }();
+  // Sparse-LU route (gp.h): the units it tries get their no-pivot symbolic
+  // factorisation; a unit whose pattern qualifies becomes a sparse unit.
+  std::map<int32_t, GpSymbolic> gp_sym;
+  p.gp_index.assign(static_cast<size_t>(nu), -1);
+  if (gp && gp->mode > 0 && !gp->unsupported) {
+    std::vector<int32_t> cand(static_cast<size_t>(nu), 0);
+    bool any = false;
+    for (int32_t u = 0; u < nu; ++u) {
+      const int32_t s0 = p.ustart[static_cast<size_t>(u)];
+      const int32_t m = p.ustart[static_cast<size_t>(u) + 1] - s0;
+      if (m <= 1 || m <= gp->dense_max || (!gp->force && m > gp->max_n) || m > kGpMaxRows) continue;
+      if (std::find(gp->rejected.begin(), gp->rejected.end(), s0) != gp->rejected.end()) continue;
+      cand[static_cast<size_t>(u)] = 1;
+      any = true;
+    }
+    if (any) {
+      std::map<int32_t, std::array<std::vector<int32_t>, 3>> ent;  // unit -> local rows, cols, sources
+      const size_t nz = static_cast<size_t>(a.nnz());
+      for (size_t k = 0; k < nz; ++k) {
+        if (drop > 0.0 && std::abs(a.val[k]) < drop) continue;
+        const int32_t rp = d.invP[static_cast<size_t>(a.row[k])], cp = d.invQ[static_cast<size_t>(a.col[k])];
+        const int32_t ur = p.unit_of[static_cast<size_t>(rp)];
+        if (ur != p.unit_of[static_cast<size_t>(cp)] || !cand[static_cast<size_t>(ur)]) continue;
+        auto& e = ent[ur];
+        const int32_t s0 = p.ustart[static_cast<size_t>(ur)];
+        e[0].push_back(rp - s0);
+        e[1].push_back(cp - s0);
+        e[2].push_back(static_cast<int32_t>(k));
+      }
+      int64_t total = 0;
+      for (int32_t u = 0; u < nu; ++u) {
+        if (!cand[static_cast<size_t>(u)]) continue;
+        const int64_t m = p.ustart[static_cast<size_t>(u) + 1] - p.ustart[static_cast<size_t>(u)];
+        const int64_t limit = gp->mode == 2 ? static_cast<int64_t>(gp->fill_max * static_cast<double>(m * m)) : -1;
+        GpSymbolic sym;
+        auto& e = ent[u];
+        if (gp_symbolic(static_cast<int32_t>(m), e[0], e[1], e[2], limit, sym) && total + sym.nnz < INT32_MAX) {
+          total += sym.nnz;
+          p.ukind[static_cast<size_t>(u)] = kUnitSparse;
+          gp_sym.emplace(u, std::move(sym));
+        } else {
+          p.gp_symbolic_rejected.push_back(u);
+        }
+      }
+    }
   }
   // Arena: small units first, then large units contiguously (so one memset
   // clears all large slots).  Slots are padded to 32 doubles.
@@ -152,10 +205,6 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
   }
 
   // Split entries into unit-diagonal entries and coupling, canonical order.
-  const double drop = [&] {
-    const AnalysisOptions o = analysis_options_from_env();
-    return o.drop_abs_lt < 0.0 ? (n >= 50000 ? 1e-20 : 0.0) : o.drop_abs_lt;
-  }();
   p.sdiag_src.assign(static_cast<size_t>(n), -1);
   for (int32_t u = 0; u < nu; ++u)
     if (p.ukind[static_cast<size_t>(u)] == kUnitScalar) p.sdiag_src[static_cast<size_t>(p.ustart[static_cast<size_t>(u)])] = -2;
@@ -224,8 +273,24 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
     const int32_t k = p.ukind[static_cast<size_t>(u)];
     if (k == kUnitScalar) p.lvl_scalar_ptr[static_cast<size_t>(l) + 1]++;
     else if (k == kUnitSmall) p.lvl_dense_ptr[static_cast<size_t>(l) + 1]++;
-    else p.lvl_large_ptr[static_cast<size_t>(l) + 1]++;
+    else if (k == kUnitLarge) p.lvl_large_ptr[static_cast<size_t>(l) + 1]++;
   }
+  // Sparse units by level (g indices, in unit order).
+  p.lvl_sparse_ptr.assign(static_cast<size_t>(nl) + 1, 0);
+  for (const auto& kv : gp_sym) {
+    p.gp_index[static_cast<size_t>(kv.first)] = static_cast<int32_t>(p.sparse_units.size());
+    gp_append_unit(p, kv.first, kv.second);
+    p.lvl_sparse_ptr[static_cast<size_t>(p.ulevel[static_cast<size_t>(kv.first)]) + 1]++;
+  }
+  for (int32_t l = 0; l < nl; ++l) p.lvl_sparse_ptr[static_cast<size_t>(l) + 1] += p.lvl_sparse_ptr[static_cast<size_t>(l)];
+  p.lvl_sparse.resize(p.sparse_units.size());
+  {
+    std::vector<int32_t> gn(p.lvl_sparse_ptr.begin(), p.lvl_sparse_ptr.end() - 1);
+    for (size_t g = 0; g < p.sparse_units.size(); ++g)
+      p.lvl_sparse[static_cast<size_t>(gn[static_cast<size_t>(p.ulevel[static_cast<size_t>(p.sparse_units[g])])]++)] =
+          static_cast<int32_t>(g);
+  }
+  p.factor_flops += p.gp_flops;
   for (int32_t l = 0; l < nl; ++l) {
     p.lvl_scalar_ptr[static_cast<size_t>(l) + 1] += p.lvl_scalar_ptr[static_cast<size_t>(l)];
     p.lvl_dense_ptr[static_cast<size_t>(l) + 1] += p.lvl_dense_ptr[static_cast<size_t>(l)];
@@ -245,7 +310,7 @@ Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max
         p.lvl_scalar[static_cast<size_t>(sn[static_cast<size_t>(l)]++)] = p.ustart[static_cast<size_t>(u)];
       else if (k == kUnitSmall)
         p.lvl_dense[static_cast<size_t>(dn[static_cast<size_t>(l)]++)] = u;
-      else
+      else if (k == kUnitLarge)
         p.lvl_large[static_cast<size_t>(ln[static_cast<size_t>(l)]++)] = u;
     }
   }

@@ -24,6 +24,7 @@ enum UnitKind : int32_t {
   kUnitScalar = 0,  // 1x1 raw block: the LU is the diagonal entry
   kUnitSmall = 1,   // dense LU in one CTA's shared memory
   kUnitLarge = 2,   // dense blocked LU across CTAs
+  kUnitSparse = 3,  // sparse LU without pivoting over a fixed fill pattern (gp.h)
 };
 
 struct Plan {
@@ -93,6 +94,36 @@ struct Plan {
   std::vector<int32_t> rtask;
   int32_t rtasks = 0;
   int32_t rt_words = 0;
+  // Sparse-LU units (gp.h), indexed g = 0 .. sparse_units.size() - 1.  Their
+  // columns are numbered globally: unit g's local column j is gp_col0[g] + j.
+  //   gp_cptr / gp_row: entries of L + U per column (local rows ascending),
+  //     gp_dpos: index of each column's diagonal entry; values in gp_val
+  //     order (device): U above the diagonal, the pivot, L multipliers below.
+  //   gp_aptr / gp_arow / gp_asrc: A's entries per column (local row,
+  //     canonical source).
+  //   Column levels: unit g's levels t = gp_clvl0[g] .. gp_clvl0[g + 1] - 1
+  //     hold local columns gp_corder[gp_clvlb[t] .. gp_clvlb[t + 1] - 1];
+  //     a column depends only on columns of earlier levels.
+  //   Solve: strict L and strict U by rows (local column, value position),
+  //     rows per global row index gp_col0[g] + i, columns ascending; row
+  //     levels of the forward (L) and backward (U) sweeps in the same form.
+  std::vector<int32_t> sparse_units;
+  std::vector<int32_t> gp_col0;
+  std::vector<int32_t> gp_cptr, gp_row, gp_dpos;
+  std::vector<int32_t> gp_aptr, gp_arow, gp_asrc;
+  std::vector<int32_t> gp_clvl0, gp_clvlb, gp_corder;
+  std::vector<int32_t> gp_lrp, gp_lci, gp_lpos;
+  std::vector<int32_t> gp_urp, gp_uci, gp_upos;
+  std::vector<int32_t> gp_flvl0, gp_flvlb, gp_frow;
+  std::vector<int32_t> gp_blvl0, gp_blvlb, gp_brow;
+  std::vector<int32_t> lvl_sparse_ptr, lvl_sparse;  // g by unit level
+  std::vector<int32_t> gp_index;                    // per unit: g, or -1
+  int64_t gp_nnz = 0;
+  int32_t gp_maxm = 0;
+  double gp_flops = 0.0;
+  // Units the sparse route tried and kept dense: the symbolic rejected them
+  // (no structural diagonal) or their fill exceeded the route's limit.
+  std::vector<int32_t> gp_symbolic_rejected;  // unit ids
   // Canonical CSR (original coordinates) for the residual.
   std::vector<int32_t> csr_ptr;
   double factor_flops = 0.0;
@@ -133,6 +164,8 @@ constexpr int64_t kRTaskMax = int64_t{1} << 24;  // task-graph refactor: largest
 int64_t build_rtasks(const std::vector<int32_t>& units, const std::vector<int32_t>& sizes, int64_t max_tasks,
                      std::vector<int32_t>& tasks, int32_t& words);
 
-Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max);
+struct GpConfig;
+// gp: the sparse-LU route's configuration (nullptr: off).
+Plan build_plan(const CanonicalCoo& a, const Decomposition& d, int32_t small_max, const GpConfig* gp = nullptr);
 
 }  // namespace bdlu

@@ -149,6 +149,19 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  *     (KLU's klu_refactor reuses the pivot order the same way); a zero pivot,
  *     or a host-buffer solve whose residual exceeds 1e-12, triggers a
  *     factorisation with partial pivoting.  1 pivots on every refactor.
+ *   "sparse_lu": sparse LU of diagonal blocks (the reference's opt-in
+ *     Gilbert-Peierls route, gp_lu.cpp:84-306), from the next analyze.  0 off
+ *     (default unless USERALGO_SPARSE_LU_KERNEL=gp), 1 the reference's route:
+ *     every block of USERALGO_DENSE_BLOCK_MAX (64) < m <= USERALGO_GP_MAX_N
+ *     (4096) rows is factored without pivoting over its fill pattern and kept
+ *     if the reference's gate would accept it (no row swap under the
+ *     diagonal preference USERALGO_GP_DIAG_TOL, no pivot below
+ *     USERALGO_GP_PIVOT_TOL or USERALGO_GP_MIN_ABS_DIAG); accepted factors
+ *     are bit-identical to the reference's.  A rejected block is factored
+ *     dense, for this factor and later ones of the handle.  2 the same for
+ *     blocks whose fill is at most "sparse_fill_max" (default 0.1) of m^2.
+ *     Environment settings that relax the gate, scale rows or drop entries
+ *     turn the route off.  "sparse_max_n" overrides USERALGO_GP_MAX_N.
  *   "analysis_only": 1 makes analyze stop after the host analysis (no device
  *     upload); factor then reports BDLU_BACKEND_UNAVAILABLE.  For structure
  *     inspection on machines without a GPU.
@@ -342,6 +355,20 @@ int bdlu_get_decomposition(const bdlu_solver* h, int32_t* P, int32_t* Q, int32_t
  * micro-kernel, ubtf_block_solver.cpp:1450-1498): m*m values row-major and m
  * LAPACK-style pivots.  Returns m, or -(status). */
 int32_t bdlu_get_block_lu(bdlu_solver* h, int32_t b, double* lu_rowmajor, int32_t* piv);
+
+/* Factor route of every unit (raw BTF block, the device's factor and solve
+ * unit) after analyze: start[u] its first permuted row, route[u] 0 scalar,
+ * 1 dense LU in shared memory, 2 dense blocked LU, 3 sparse LU;
+ * reason[u] -1 when the sparse-LU route did not try the unit, 0 when it
+ * factors it, 1-4 when a factor's pivot test rejected it (the reference's
+ * gp_gate_eval reasons, ubtf_block_solver.cpp:197-235: 1 zero pivot, 2 a row
+ * swap, 3 a tiny pivot, 4 smallest pivot below USERALGO_GP_MIN_ABS_DIAG) and
+ * it was factored dense since, 5 when its pattern kept it dense (no
+ * structural diagonal after fill, or fill above "sparse_fill_max").  Writes
+ * min(cap, nunits) entries of each non-NULL array; returns nunits, or
+ * -(status).  The reference's counterpart is its per-block diagnostics
+ * (BlockFactor::gp_tried / gp_reject_reason, ubtf_block_solver.h:74-84). */
+int32_t bdlu_get_unit_routes(const bdlu_solver* h, int32_t* start, int32_t* route, int32_t* reason, int32_t cap);
 
 /* Pattern and value signatures of the canonical matrix after analyze
  * (compute_matrix_sig, compute_matrix_sig2, compute_matrix_value_sig,
