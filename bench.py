@@ -8,7 +8,7 @@ One analyze + first factor (untimed), then steps of one value-only refactor
 (values x (1 + U(-0.1, 0.1)), fresh per step) followed by one 1-RHS solve.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
-                    [--workload circuit-200k|batch-256|serve-64|precision-200]
+                    [--workload circuit-200k|batch-256|serve-64|precision-200|sparse-units]
 
 Workload "precision-200" (precision): 200 irreducible blocks of U{2000..8000}
 rows with ~20 entries per row plus Pareto-sized small blocks (about 10 % of
@@ -33,6 +33,15 @@ block generator's kind with n log-uniform in [1,000, 50,000] and n/50 blocks,
 8 right-hand sides U(-1, 1); each step refactors all 256 systems (values
 x (1 + U(-0.1, 0.1))) and solves the 8 right-hand sides of each, through one
 batch (bdlu_batch_*); the metric is systems factored and solved per second.
+
+Workload "sparse-units" (fill sweep of the sparse-LU route): per class of
+extra entries per row (0.1 .. 4), 300 sparse irreducible blocks of U{200..600}
+rows (a cyclic chain, the diagonal and the extra entries, magnitudes
+U(0.5, 2) with random sign), coupled above the blocks, randomly permuted;
+steps of one value-only refactor (values x (1 + U(-0.01, 0.01))) and one
+1-rhs solve on the dense route and on the sparse-LU route (option
+"sparse_lu" = 2, no fill limit), device-timed; reports the fill of the
+sparse factors and the speed-up per class.
 
 Prints one JSON line on rank 0.  `value` is device-timed (inputs resident in
 HBM, CUDA events per step on the launching stream, L2 flushed between steps
@@ -72,6 +81,9 @@ REF_SERVE_MAX_BLOCK = 4000
 PREC_WORKLOAD = "precision-200"
 PREC_METRIC = "factor+16-rhs solves/s"
 PREC_BLOCKS, PREC_CONFIG, PREC_NRHS = 200, 3, 16
+SPARSE_WORKLOAD = "sparse-units"
+SPARSE_EXTRAS = (0.1, 0.25, 0.5, 1.0, 2.0, 4.0)
+SPARSE_BLOCKS, SPARSE_MIN_ROWS, SPARSE_MAX_ROWS, SPARSE_SEED = 300, 200, 600, 20261277
 
 
 def parse():
@@ -82,9 +94,11 @@ def parse():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD,
-                    choices=[SERVE_WORKLOAD, CIRCUIT_WORKLOAD, BATCH_WORKLOAD, PREC_WORKLOAD])
+                    choices=[SERVE_WORKLOAD, CIRCUIT_WORKLOAD, BATCH_WORKLOAD, PREC_WORKLOAD, SPARSE_WORKLOAD])
     ap.add_argument("--blocks", type=int, default=PREC_BLOCKS, help="precision-200: number of large blocks")
     ap.add_argument("--rate", type=float, default=2000.0, help="serve-64: Poisson arrival rate (requests/s)")
+    ap.add_argument("--sparse-extra", type=float, nargs="*", default=None,
+                    help="sparse-units: the classes to run (extra entries per row), default all")
     ap.add_argument("--duration", type=float, default=2.0, help="serve-64: seconds of open-loop arrivals")
     ap.add_argument("--slots", type=int, default=16, help="serve-64: concurrent request slots")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1, 2],
@@ -1162,6 +1176,111 @@ def run_circuit(args, rank, world):
         dist.destroy_process_group()
 
 
+def sparse_units_system(seed, blocks, extra, lo=SPARSE_MIN_ROWS, hi=SPARSE_MAX_ROWS):
+    """Upper block triangular system of `blocks` sparse irreducible blocks of
+    U{lo..hi} rows: a cyclic chain, the diagonal and extra*m random entries
+    per block, magnitudes U(0.5, 2) with random sign; every third row couples
+    to a later block (N(0, 0.1)); random row and column permutations.
+    Returns the canonical COO (rows sorted, duplicates summed)."""
+    import scipy.sparse as sp
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(lo, hi + 1, blocks)
+    starts = np.concatenate([[0], np.cumsum(sizes)])
+    n = int(starts[-1])
+    rows, cols = [], []
+    for b, m in enumerate(sizes):
+        o = int(starts[b])
+        i = np.arange(m)
+        k = int(extra * m)
+        rows += [o + i, o + i, o + rng.integers(0, m, k)]
+        cols += [o + i, o + (i + 1) % m, o + rng.integers(0, m, k)]
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    v = rng.uniform(0.5, 2.0, len(r)) * rng.choice([-1.0, 1.0], len(r))
+    cr, cc = [], []
+    for b, m in enumerate(sizes[:-1]):
+        i = np.arange(int(starts[b]), int(starts[b + 1]), 3)
+        cr.append(i)
+        cc.append(rng.integers(int(starts[b + 1]), n, len(i)))
+    cr, cc = np.concatenate(cr), np.concatenate(cc)
+    r = np.concatenate([r, cr])
+    c = np.concatenate([c, cc])
+    v = np.concatenate([v, 0.1 * rng.standard_normal(len(cr))])
+    p, q = rng.permutation(n), rng.permutation(n)
+    A = sp.csr_matrix((v, (np.argsort(p)[r], np.argsort(q)[c])), shape=(n, n))
+    A.sum_duplicates()
+    A.eliminate_zeros()
+    A = A.tocoo()
+    order = np.lexsort((A.col, A.row))
+    return n, A.row[order].astype(np.int32), A.col[order].astype(np.int32), A.data[order].astype(np.float64)
+
+
+def run_sparse_units(args, rank, world):
+    """sparse-units: refactor + solve of systems of sparse blocks on the
+    sparse-LU route against the dense route, per fill class."""
+    import blockdaglu as bd
+    if args.impl == "reference" or (world > 1 and rank != 0):
+        if rank == 0:
+            print(json.dumps({"impl": "reference", "metric": METRIC, "unavailable":
+                              "sparse-units is the engine's fill-threshold sweep; the reference's sparse route is "
+                              "timed in its cpu_baseline"}), flush=True)
+        return
+    classes = []
+    steps, warm = max(1, args.steps), max(1, args.warmup)
+    for ci, extra in enumerate(SPARSE_EXTRAS):
+        if args.sparse_extra and extra not in args.sparse_extra:
+            continue
+        n, r, c, v = sparse_units_system(SPARSE_SEED + ci, SPARSE_BLOCKS, extra)
+        rng = np.random.default_rng(ci)
+        vals = [v * (1.0 + rng.uniform(-0.01, 0.01, len(v))) for _ in range(steps + warm)]
+        b = rng.uniform(-1.0, 1.0, n)
+        res = {"extra_per_row": extra, "n": n, "nnz": int(len(v))}
+        for label, mode in (("dense", 0), ("sparse", 2)):
+            s = bd.Solver()
+            s.set_option("sparse_lu", mode)
+            s.set_option("sparse_fill_max", 1.0)
+            assert s.set_matrix((r, c, v), n) and s.analyze() and s.factor(), s.last_error_message()
+            fac, sol = [], []
+            for k in range(steps + warm):
+                x = b.copy()
+                assert s.refactor_values(vals[k]), s.last_error_message()
+                st = s.stats()
+                assert s.solve_in_place(x), s.last_error_message()
+                st2 = s.stats()
+                if k >= warm:
+                    fac.append(st["last_factor_ms"])
+                    sol.append(st2["last_solve_ms"])
+                assert st2["residual_inf"] <= 1e-12, st2["residual_inf"]
+            start, route, reason, lu_nnz = s.unit_routes(with_nnz=True)
+            m = np.diff(np.append(start, n))
+            sel = route == 3
+            res[label] = {"factor_ms": statistics.median(fac), "solve_ms": statistics.median(sol),
+                          "factor_flops": s.stats()["factor_flops"]}
+            if mode:
+                big = m > 64
+                res[label].update({"sparse_units": int(sel.sum()), "candidate_units": int(big.sum()),
+                                   "rejected_by_pivot_test": int(((reason >= 1) & (reason <= 4)).sum()),
+                                   "mean_fill": float(np.mean(lu_nnz[sel] / (m[sel].astype(float) ** 2)))
+                                   if sel.any() else None})
+            del s
+        res["sparse_over_dense"] = ((res["dense"]["factor_ms"] + res["dense"]["solve_ms"]) /
+                                    (res["sparse"]["factor_ms"] + res["sparse"]["solve_ms"]))
+        classes.append(res)
+        print(json.dumps({"class": res}), file=sys.stderr, flush=True)
+    wins = [cl["sparse"]["mean_fill"] for cl in classes if cl["sparse_over_dense"] > 1.0 and cl["sparse"]["mean_fill"]]
+    first = classes[0]
+    ms = first["sparse"]["factor_ms"] + first["sparse"]["solve_ms"]
+    line = {"metric": METRIC, "value": 1000.0 / ms, "unit": METRIC, "n_gpus": 1, "steps": steps, "warmup": warm,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": SPARSE_WORKLOAD, "blocks": SPARSE_BLOCKS,
+                       "block_rows": [SPARSE_MIN_ROWS, SPARSE_MAX_ROWS],
+                       "value_from": "lowest-fill class on the sparse-LU route, device-timed factor + 1-rhs solve"},
+            "classes": classes, "largest_fill_where_sparse_wins": max(wins) if wins else None,
+            "roofline": None, "cpu_baseline": None, "gpu_launches": None}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -1172,6 +1291,8 @@ def main():
         run_serve(args, rank, world)
     elif args.workload == PREC_WORKLOAD:
         run_precision(args, rank, world)
+    elif args.workload == SPARSE_WORKLOAD:
+        run_sparse_units(args, rank, world)
     elif args.impl == "reference":
         run_reference(args, rank, world)
     else:

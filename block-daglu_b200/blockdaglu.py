@@ -104,7 +104,8 @@ def load_library(path=LIB_PATH):
         "bdlu_get_decomposition": (ctypes.c_int, [vp, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _i32p]),
         "bdlu_get_block_lu": (ctypes.c_int32, [vp, ctypes.c_int32, _f64p, _i32p]),
         "bdlu_matrix_signatures": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_uint64)]),
-        "bdlu_get_unit_routes": (ctypes.c_int32, [vp, _i32p, _i32p, _i32p, ctypes.c_int32]),
+        "bdlu_get_unit_routes": (ctypes.c_int32, [vp, _i32p, _i32p, _i32p, ctypes.POINTER(ctypes.c_int64),
+                                                  ctypes.c_int32]),
         "bdlu_tuner_report": (ctypes.c_int64, [ctypes.c_char_p, ctypes.c_int64]),
         "bdlu_batch_create": (vp, []),
         "bdlu_batch_destroy": (None, [vp]),
@@ -302,15 +303,17 @@ class Solver:
             return None
         return tuple(int(v) for v in out)
 
-    def unit_routes(self):
-        """Per unit (raw BTF block): (start rows, routes, reasons) as
-        bdlu_get_unit_routes gives them (route 3 = sparse LU)."""
-        nu = self._lib.bdlu_get_unit_routes(self._h, None, None, None, 0)
+    def unit_routes(self, with_nnz=False):
+        """Per unit (raw BTF block): (start rows, routes, reasons[, factor
+        entries]) as bdlu_get_unit_routes gives them (route 3 = sparse LU)."""
+        nu = self._lib.bdlu_get_unit_routes(self._h, None, None, None, None, 0)
         if nu < 0:
             raise RuntimeError(self.last_error_message() or "unit routes unavailable")
         start, route, reason = (np.zeros(nu, np.int32) for _ in range(3))
-        self._lib.bdlu_get_unit_routes(self._h, _p32(start), _p32(route), _p32(reason), nu)
-        return start, route, reason
+        nnz = np.zeros(nu, np.int64)
+        self._lib.bdlu_get_unit_routes(self._h, _p32(start), _p32(route), _p32(reason),
+                                       nnz.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), nu)
+        return (start, route, reason, nnz) if with_nnz else (start, route, reason)
 
     def block_lu(self, b):
         """Dense LU (row-major m*m) and pivots of merged block b, as the reference's micro-kernel stores them."""

@@ -774,7 +774,8 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
   return BDLU_INVALID_DIMENSION;
 }
 
-int32_t bdlu_get_unit_routes(const bdlu_solver* h, int32_t* start, int32_t* route, int32_t* reason, int32_t cap) {
+int32_t bdlu_get_unit_routes(const bdlu_solver* h, int32_t* start, int32_t* route, int32_t* reason, int64_t* lu_nnz,
+                             int32_t cap) {
   if (!h || !h->decomposed || !h->engine) return -BDLU_NOT_PREPARED;
   const bdlu::Plan& p = h->engine->plan();
   for (int32_t u = 0; u < p.nunits && u < cap; ++u) {
@@ -788,6 +789,13 @@ int32_t bdlu_get_unit_routes(const bdlu_solver* h, int32_t* start, int32_t* rout
       if (std::find(p.gp_symbolic_rejected.begin(), p.gp_symbolic_rejected.end(), u) != p.gp_symbolic_rejected.end())
         r = 5;
       reason[u] = r;
+    }
+    if (lu_nnz) {
+      const int64_t m = p.ustart[static_cast<size_t>(u) + 1] - s0;
+      const int32_t g = p.gp_index.empty() ? -1 : p.gp_index[static_cast<size_t>(u)];
+      lu_nnz[u] = g >= 0 ? static_cast<int64_t>(p.gp_cptr[static_cast<size_t>(p.gp_col0[static_cast<size_t>(g) + 1])] -
+                                                p.gp_cptr[static_cast<size_t>(p.gp_col0[static_cast<size_t>(g)])])
+                         : m * m;
     }
   }
   return p.nunits;

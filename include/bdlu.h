@@ -364,11 +364,14 @@ int32_t bdlu_get_block_lu(bdlu_solver* h, int32_t b, double* lu_rowmajor, int32_
  * gp_gate_eval reasons, ubtf_block_solver.cpp:197-235: 1 zero pivot, 2 a row
  * swap, 3 a tiny pivot, 4 smallest pivot below USERALGO_GP_MIN_ABS_DIAG) and
  * it was factored dense since, 5 when its pattern kept it dense (no
- * structural diagonal after fill, or fill above "sparse_fill_max").  Writes
+ * structural diagonal after fill, or fill above "sparse_fill_max");
+ * lu_nnz[u] the entries its factor stores (m*m for a dense unit, those of
+ * L + U over the fill pattern for a sparse one, 1 for a scalar).  Writes
  * min(cap, nunits) entries of each non-NULL array; returns nunits, or
  * -(status).  The reference's counterpart is its per-block diagnostics
  * (BlockFactor::gp_tried / gp_reject_reason, ubtf_block_solver.h:74-84). */
-int32_t bdlu_get_unit_routes(const bdlu_solver* h, int32_t* start, int32_t* route, int32_t* reason, int32_t cap);
+int32_t bdlu_get_unit_routes(const bdlu_solver* h, int32_t* start, int32_t* route, int32_t* reason, int64_t* lu_nnz,
+                             int32_t cap);
 
 /* Pattern and value signatures of the canonical matrix after analyze
  * (compute_matrix_sig, compute_matrix_sig2, compute_matrix_value_sig,

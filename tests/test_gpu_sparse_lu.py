@@ -161,7 +161,7 @@ def test_sparse_route_multi_rhs_and_export():
     check_solution(s, o, n, r, c, v, nrhs=8)
 
     def dense(coo, shape):
-        rr, cc, vv = coo
+        rr, cc, vv = (np.array(t) for t in zip(*coo))
         return sp.csr_matrix((vv, (rr, cc)), shape=shape).toarray()
 
     L = dense(s.getL(), (n, n))
