@@ -41,7 +41,10 @@ U(0.5, 2) with random sign), coupled above the blocks, randomly permuted;
 steps of one value-only refactor (values x (1 + U(-0.01, 0.01))) and one
 1-rhs solve on the dense route and on the sparse-LU route (option
 "sparse_lu" = 2, no fill limit), device-timed; reports the fill of the
-sparse factors and the speed-up per class.
+sparse factors and the speed-up per class.  Then single blocks of 1,000,
+2,000 and 4,000 rows with 0.05 .. 1 extra entries per row on the global
+route (one unit in its own order, so the diagonal stays dominant and the
+sparse factor is accepted): the per-block crossover of fill and size.
 
 Prints one JSON line on rank 0.  `value` is device-timed (inputs resident in
 HBM, CUDA events per step on the launching stream, L2 flushed between steps
@@ -84,6 +87,9 @@ PREC_BLOCKS, PREC_CONFIG, PREC_NRHS = 200, 3, 16
 SPARSE_WORKLOAD = "sparse-units"
 SPARSE_EXTRAS = (0.1, 0.25, 0.5, 1.0, 2.0, 4.0)
 SPARSE_BLOCKS, SPARSE_MIN_ROWS, SPARSE_MAX_ROWS, SPARSE_SEED = 300, 200, 600, 20261277
+# Single sparse blocks on the global route (no BTF, so the block keeps its
+# own diagonal and the sparse factor is accepted): rows x extra entries/row.
+SPARSE_SINGLE = tuple((m, e) for m in (1000, 2000, 4000) for e in (0.05, 0.1, 0.25, 0.5, 1.0))
 
 
 def parse():
@@ -99,6 +105,8 @@ def parse():
     ap.add_argument("--rate", type=float, default=2000.0, help="serve-64: Poisson arrival rate (requests/s)")
     ap.add_argument("--sparse-extra", type=float, nargs="*", default=None,
                     help="sparse-units: the classes to run (extra entries per row), default all")
+    ap.add_argument("--sparse-single", type=int, default=None, choices=[0, 1],
+                    help="sparse-units: 1 only the single-block classes, 0 only the many-block classes")
     ap.add_argument("--duration", type=float, default=2.0, help="serve-64: seconds of open-loop arrivals")
     ap.add_argument("--slots", type=int, default=16, help="serve-64: concurrent request slots")
     ap.add_argument("--precision", type=int, default=0, choices=[0, 1, 2],
@@ -1176,12 +1184,14 @@ def run_circuit(args, rank, world):
         dist.destroy_process_group()
 
 
-def sparse_units_system(seed, blocks, extra, lo=SPARSE_MIN_ROWS, hi=SPARSE_MAX_ROWS):
+def sparse_units_system(seed, blocks, extra, lo=SPARSE_MIN_ROWS, hi=SPARSE_MAX_ROWS, single=False):
     """Upper block triangular system of `blocks` sparse irreducible blocks of
     U{lo..hi} rows: a cyclic chain, the diagonal and extra*m random entries
     per block, magnitudes U(0.5, 2) with random sign; every third row couples
     to a later block (N(0, 0.1)); random row and column permutations.
-    Returns the canonical COO (rows sorted, duplicates summed)."""
+    single: one block left in its own order with its diagonal scaled by 4
+    (the global route factors it as it is).  Returns the canonical COO (rows
+    sorted, duplicates summed)."""
     import scipy.sparse as sp
     rng = np.random.default_rng(seed)
     sizes = rng.integers(lo, hi + 1, blocks)
@@ -1197,7 +1207,7 @@ def sparse_units_system(seed, blocks, extra, lo=SPARSE_MIN_ROWS, hi=SPARSE_MAX_R
     r = np.concatenate(rows)
     c = np.concatenate(cols)
     v = rng.uniform(0.5, 2.0, len(r)) * rng.choice([-1.0, 1.0], len(r))
-    cr, cc = [], []
+    cr, cc = [np.zeros(0, np.int64)], [np.zeros(0, np.int64)]
     for b, m in enumerate(sizes[:-1]):
         i = np.arange(int(starts[b]), int(starts[b + 1]), 3)
         cr.append(i)
@@ -1206,7 +1216,11 @@ def sparse_units_system(seed, blocks, extra, lo=SPARSE_MIN_ROWS, hi=SPARSE_MAX_R
     r = np.concatenate([r, cr])
     c = np.concatenate([c, cc])
     v = np.concatenate([v, 0.1 * rng.standard_normal(len(cr))])
-    p, q = rng.permutation(n), rng.permutation(n)
+    if single:
+        v[:n] *= 4.0  # the diagonal entries come first
+        p = q = np.arange(n)
+    else:
+        p, q = rng.permutation(n), rng.permutation(n)
     A = sp.csr_matrix((v, (np.argsort(p)[r], np.argsort(q)[c])), shape=(n, n))
     A.sum_duplicates()
     A.eliminate_zeros()
@@ -1227,19 +1241,34 @@ def run_sparse_units(args, rank, world):
         return
     classes = []
     steps, warm = max(1, args.steps), max(1, args.warmup)
-    for ci, extra in enumerate(SPARSE_EXTRAS):
+    plan = [("blocks", ci, SPARSE_BLOCKS, SPARSE_MIN_ROWS, SPARSE_MAX_ROWS, e) for ci, e in enumerate(SPARSE_EXTRAS)]
+    plan += [("single", 100 + ci, 1, m, m, e) for ci, (m, e) in enumerate(SPARSE_SINGLE)]
+    for kind, ci, blocks, lo, hi, extra in plan:
         if args.sparse_extra and extra not in args.sparse_extra:
             continue
-        n, r, c, v = sparse_units_system(SPARSE_SEED + ci, SPARSE_BLOCKS, extra)
+        if args.sparse_single is not None and (kind == "single") != bool(args.sparse_single):
+            continue
+        n, r, c, v = sparse_units_system(SPARSE_SEED + ci, blocks, extra, lo, hi, single=kind == "single")
         rng = np.random.default_rng(ci)
         vals = [v * (1.0 + rng.uniform(-0.01, 0.01, len(v))) for _ in range(steps + warm)]
         b = rng.uniform(-1.0, 1.0, n)
-        res = {"extra_per_row": extra, "n": n, "nnz": int(len(v))}
+        res = {"kind": kind, "blocks": blocks, "rows": [lo, hi], "extra_per_row": extra, "n": n, "nnz": int(len(v))}
         for label, mode in (("dense", 0), ("sparse", 2)):
             s = bd.Solver()
             s.set_option("sparse_lu", mode)
             s.set_option("sparse_fill_max", 1.0)
-            assert s.set_matrix((r, c, v), n) and s.analyze() and s.factor(), s.last_error_message()
+            s.set_option("sparse_max_n", 8192)
+            # A single block on the global route: one unit in its own order.
+            saved = os.environ.get("BLOCKDAGLU_MODE")
+            if kind == "single":
+                os.environ["BLOCKDAGLU_MODE"] = "klu"
+            try:
+                assert s.set_matrix((r, c, v), n) and s.analyze() and s.factor(), s.last_error_message()
+            finally:
+                if saved is None:
+                    os.environ.pop("BLOCKDAGLU_MODE", None)
+                else:
+                    os.environ["BLOCKDAGLU_MODE"] = saved
             fac, sol = [], []
             for k in range(steps + warm):
                 x = b.copy()
@@ -1275,7 +1304,7 @@ def run_sparse_units(args, rank, world):
             "data": "synthetic",
             "config": {"workload": SPARSE_WORKLOAD, "blocks": SPARSE_BLOCKS,
                        "block_rows": [SPARSE_MIN_ROWS, SPARSE_MAX_ROWS],
-                       "value_from": "lowest-fill class on the sparse-LU route, device-timed factor + 1-rhs solve"},
+                       "value_from": "first class run, on the sparse-LU route, device-timed factor + 1-rhs solve"},
             "classes": classes, "largest_fill_where_sparse_wins": max(wins) if wins else None,
             "roofline": None, "cpu_baseline": None, "gpu_launches": None}
     print(json.dumps(line), flush=True)

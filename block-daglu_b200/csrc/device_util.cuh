@@ -12,6 +12,7 @@ constexpr int kFailReusedPivot = 2;  // a reused pivot order met a zero pivot
 constexpr int kFailSync = 3;         // a bounded wait of the solve ran out
 constexpr int kFailRefactorSync = 4; // a bounded wait of the tile-graph refactor ran out
 constexpr int kFailSparseReject = 6; // a sparse-LU unit failed the pivot test (gp.h): factor it dense
+constexpr int kFailSparseSync = 7;   // a bounded wait between sparse-LU columns ran out
 
 __device__ __forceinline__ void report_failure(int32_t* status, int32_t unit) {
   if (atomicCAS(status, 0, kFailZeroPivot) == 0) status[1] = unit;

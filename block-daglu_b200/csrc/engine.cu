@@ -1057,24 +1057,16 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
     if (!upload_vec(allocs_, plan.gp_aptr, &g.aptr, err)) return false;
     if (!upload_vec(allocs_, plan.gp_arow, &g.arow, err)) return false;
     if (!upload_vec(allocs_, plan.gp_asrc, &g.asrc, err)) return false;
-    if (!upload_vec(allocs_, plan.gp_clvl0, &g.clvl0, err)) return false;
-    if (!upload_vec(allocs_, plan.gp_clvlb, &g.clvlb, err)) return false;
-    if (!upload_vec(allocs_, plan.gp_corder, &g.corder, err)) return false;
     if (!upload_vec(allocs_, plan.gp_lrp, &g.lrp, err)) return false;
     if (!upload_vec(allocs_, plan.gp_lci, &g.lci, err)) return false;
     if (!upload_vec(allocs_, plan.gp_lpos, &g.lpos, err)) return false;
     if (!upload_vec(allocs_, plan.gp_urp, &g.urp, err)) return false;
     if (!upload_vec(allocs_, plan.gp_uci, &g.uci, err)) return false;
     if (!upload_vec(allocs_, plan.gp_upos, &g.upos, err)) return false;
-    if (!upload_vec(allocs_, plan.gp_flvl0, &g.flvl0, err)) return false;
-    if (!upload_vec(allocs_, plan.gp_flvlb, &g.flvlb, err)) return false;
-    if (!upload_vec(allocs_, plan.gp_frow, &g.frow, err)) return false;
-    if (!upload_vec(allocs_, plan.gp_blvl0, &g.blvl0, err)) return false;
-    if (!upload_vec(allocs_, plan.gp_blvlb, &g.blvlb, err)) return false;
-    if (!upload_vec(allocs_, plan.gp_brow, &g.brow, err)) return false;
     if (!alloc_dev(allocs_, static_cast<size_t>(std::max<int64_t>(plan.gp_nnz, 1)), &g.val, err)) return false;
     if (!alloc_dev(allocs_, plan.sparse_units.size(), &g.gstat, err)) return false;
     g.maxm = plan.gp_maxm;
+    g.wait_limit = dp_.wait_limit;
     if (!upload_vec(allocs_, plan.lvl_sparse, &lvl_sparse_, err)) return false;
   }
   return true;
@@ -1366,6 +1358,10 @@ int Engine::factor_status(cudaStream_t stream, std::string& err) {
   if (st[0] == kFailReusedPivot) {
     err = "reused pivot order met a zero pivot in diagonal block " + std::to_string(st[1]);
     return 2;
+  }
+  if (st[0] == kFailSparseSync) {
+    err = "sparse LU: a bounded wait between columns ran out";
+    return -1;
   }
   if (st[0] == kFailSparseReject) {
     err = "sparse LU of diagonal block " + std::to_string(st[1]) + " failed its pivot test";

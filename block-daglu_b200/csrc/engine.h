@@ -136,6 +136,7 @@ class Engine {
     const int32_t v = polls > 0 ? polls : kWaitLimitDefault;
     if (v == dp_.wait_limit) return;
     dp_.wait_limit = v;
+    gp_.wait_limit = v;
     drop_graphs();
   }
   // Waits for `stream`: spinning (cudaStreamSynchronize), or, with

@@ -48,20 +48,23 @@ struct GpConfig {
 // (ubtf_block_solver.cpp:87-182), BLOCKDAGLU_* names first.
 GpConfig gp_config_from_env();
 
-// Largest unit whose work vectors fit the factor kernel's shared memory.
+// Largest sparse unit: the solve keeps four right-hand sides of unknowns and
+// a flag per row in shared memory (6144 * 36 bytes, within 227 KB), the
+// factor one work vector per warp and a flag per column.
 constexpr int32_t kGpMaxRows = 6144;
+// Reason a sparse factor records when a bounded wait on another column ran
+// out (not a pivot-test reason).
+constexpr int32_t kGpReasonSync = 9;
 
 // Symbolic no-pivot LU of one unit from its local entries (row, col, src).
 // Returns false if some column has no diagonal entry in the filled pattern
 // (the reference's gate rejects such a block: a swap or a zero pivot), or if
 // fill_limit >= 0 and the pattern exceeds fill_limit entries (the symbolic
-// stops early).  Outputs per column: entries (rows ascending; the first
-// udiag[j] rows are above the diagonal, then the diagonal, then L), A's
-// entries, and the dependency level of each column.
+// stops early).  Outputs per column: entries (rows ascending: those above
+// the diagonal, the diagonal at dpos[j], then L) and A's entries.
 struct GpSymbolic {
   std::vector<int32_t> cptr, row, dpos;  // dpos[j]: index of the diagonal in row[]
   std::vector<int32_t> aptr, arow, asrc;
-  std::vector<int32_t> clevel;
   int64_t nnz = 0;
   double flops = 0.0;
 };
@@ -78,31 +81,23 @@ struct GpDev {
   const int32_t* aptr;
   const int32_t* arow;
   const int32_t* asrc;
-  const int32_t* clvl0;
-  const int32_t* clvlb;
-  const int32_t* corder;
   const int32_t* lrp;
   const int32_t* lci;
   const int32_t* lpos;
   const int32_t* urp;
   const int32_t* uci;
   const int32_t* upos;
-  const int32_t* flvl0;
-  const int32_t* flvlb;
-  const int32_t* frow;
-  const int32_t* blvl0;
-  const int32_t* blvlb;
-  const int32_t* brow;
   double* val;      // gp_nnz factor values, column-compressed
   int32_t* gstat;   // per sparse unit: 0, or the reason its pivot test failed
   int32_t maxm;     // largest sparse unit
+  int32_t wait_limit;  // polls of a bounded wait on another column or row (DevPlan::wait_limit)
   double diag_tol;
   double pivot_tol;
   double min_abs_diag;
 };
 
-// Appends unit u's symbolic to the plan's sparse-unit tables (solve rows and
-// levels included).
+// Appends unit u's symbolic to the plan's sparse-unit tables (the solve's
+// row tables included).
 void gp_append_unit(Plan& p, int32_t u, const GpSymbolic& s);
 
 }  // namespace bdlu

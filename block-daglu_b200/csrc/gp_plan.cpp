@@ -96,7 +96,6 @@ bool gp_symbolic(int32_t m, const std::vector<int32_t>& er, const std::vector<in
   std::vector<int32_t> up, lo;
   out.cptr.assign(1, 0);
   out.dpos.resize(static_cast<size_t>(m));
-  out.clevel.assign(static_cast<size_t>(m), 0);
   for (int32_t j = 0; j < m; ++j) {
     up.clear();
     lo.clear();
@@ -110,18 +109,15 @@ bool gp_symbolic(int32_t m, const std::vector<int32_t>& er, const std::vector<in
     };
     for (int32_t q = out.aptr[static_cast<size_t>(j)]; q < out.aptr[static_cast<size_t>(j) + 1]; ++q)
       visit(out.arow[static_cast<size_t>(q)]);
-    int32_t lev = 0;
     while (!heap.empty()) {
       const int32_t k = heap.top();
       heap.pop();
       up.push_back(k);
-      lev = std::max(lev, out.clevel[static_cast<size_t>(k)] + 1);
       out.flops += 2.0 * static_cast<double>(lcols[static_cast<size_t>(k)].size());
       for (int32_t i : lcols[static_cast<size_t>(k)]) visit(i);
     }
     if (!diag) return false;
     std::sort(lo.begin(), lo.end());
-    out.clevel[static_cast<size_t>(j)] = lev;
     out.flops += static_cast<double>(lo.size());
     out.dpos[static_cast<size_t>(j)] = out.cptr.back() + static_cast<int32_t>(up.size());
     out.row.insert(out.row.end(), up.begin(), up.end());
@@ -135,32 +131,9 @@ bool gp_symbolic(int32_t m, const std::vector<int32_t>& er, const std::vector<in
   return true;
 }
 
-namespace {
-
-// Appends the items of `level` (one per element) grouped by level, ascending
-// within a level: order receives the items, lvlb one boundary per level.
-void append_levels(const std::vector<int32_t>& level, std::vector<int32_t>& order, std::vector<int32_t>& lvl0,
-                   std::vector<int32_t>& lvlb) {
-  int32_t nl = 0;
-  for (int32_t v : level) nl = std::max(nl, v + 1);
-  std::vector<int32_t> cnt(static_cast<size_t>(nl) + 1, 0);
-  for (int32_t v : level) cnt[static_cast<size_t>(v) + 1]++;
-  for (int32_t t = 0; t < nl; ++t) cnt[static_cast<size_t>(t) + 1] += cnt[static_cast<size_t>(t)];
-  const size_t base = order.size();
-  order.resize(base + level.size());
-  std::vector<int32_t> nx(cnt.begin(), cnt.end() - 1);
-  for (size_t i = 0; i < level.size(); ++i)
-    order[base + static_cast<size_t>(nx[static_cast<size_t>(level[i])]++)] = static_cast<int32_t>(i);
-  for (int32_t t = 0; t < nl; ++t) lvlb.push_back(static_cast<int32_t>(base) + cnt[static_cast<size_t>(t) + 1]);
-  lvl0.push_back(lvl0.back() + nl);
-}
-
-}  // namespace
-
 void gp_append_unit(Plan& p, int32_t u, const GpSymbolic& s) {
   if (p.gp_col0.empty()) {
-    for (auto* v : {&p.gp_col0, &p.gp_cptr, &p.gp_aptr, &p.gp_clvl0, &p.gp_clvlb, &p.gp_lrp, &p.gp_urp, &p.gp_flvl0,
-                    &p.gp_flvlb, &p.gp_blvl0, &p.gp_blvlb})
+    for (auto* v : {&p.gp_col0, &p.gp_cptr, &p.gp_aptr, &p.gp_lrp, &p.gp_urp})
       v->assign(1, 0);
   }
   const int32_t m = static_cast<int32_t>(s.cptr.size()) - 1;
@@ -176,7 +149,6 @@ void gp_append_unit(Plan& p, int32_t u, const GpSymbolic& s) {
   p.gp_row.insert(p.gp_row.end(), s.row.begin(), s.row.end());
   p.gp_arow.insert(p.gp_arow.end(), s.arow.begin(), s.arow.end());
   p.gp_asrc.insert(p.gp_asrc.end(), s.asrc.begin(), s.asrc.end());
-  append_levels(s.clevel, p.gp_corder, p.gp_clvl0, p.gp_clvlb);
   // Strict L and strict U by rows, columns ascending (columns are visited in
   // order), with the value positions of the column-compressed factor.
   std::vector<int32_t> lcnt(static_cast<size_t>(m) + 1, 0), ucnt(static_cast<size_t>(m) + 1, 0);
@@ -213,19 +185,6 @@ void gp_append_unit(Plan& p, int32_t u, const GpSymbolic& s) {
         p.gp_upos[w] = base + q;
       }
     }
-  // Row levels: forward rows after the rows their L row reads, backward rows
-  // after the rows their U row reads.
-  std::vector<int32_t> fl(static_cast<size_t>(m), 0), bl(static_cast<size_t>(m), 0);
-  for (int32_t i = 0; i < m; ++i)
-    for (int32_t q = lcnt[static_cast<size_t>(i)]; q < lcnt[static_cast<size_t>(i) + 1]; ++q)
-      fl[static_cast<size_t>(i)] =
-          std::max(fl[static_cast<size_t>(i)], fl[static_cast<size_t>(p.gp_lci[static_cast<size_t>(lbase + q)])] + 1);
-  for (int32_t i = m - 1; i >= 0; --i)
-    for (int32_t q = ucnt[static_cast<size_t>(i)]; q < ucnt[static_cast<size_t>(i) + 1]; ++q)
-      bl[static_cast<size_t>(i)] =
-          std::max(bl[static_cast<size_t>(i)], bl[static_cast<size_t>(p.gp_uci[static_cast<size_t>(ubase + q)])] + 1);
-  append_levels(fl, p.gp_frow, p.gp_flvl0, p.gp_flvlb);
-  append_levels(bl, p.gp_brow, p.gp_blvl0, p.gp_blvlb);
   p.gp_nnz += s.nnz;
   p.gp_maxm = std::max(p.gp_maxm, m);
   p.gp_flops += s.flops;

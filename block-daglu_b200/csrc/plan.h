@@ -101,21 +101,14 @@ struct Plan {
   //     order (device): U above the diagonal, the pivot, L multipliers below.
   //   gp_aptr / gp_arow / gp_asrc: A's entries per column (local row,
   //     canonical source).
-  //   Column levels: unit g's levels t = gp_clvl0[g] .. gp_clvl0[g + 1] - 1
-  //     hold local columns gp_corder[gp_clvlb[t] .. gp_clvlb[t + 1] - 1];
-  //     a column depends only on columns of earlier levels.
   //   Solve: strict L and strict U by rows (local column, value position),
-  //     rows per global row index gp_col0[g] + i, columns ascending; row
-  //     levels of the forward (L) and backward (U) sweeps in the same form.
+  //     rows per global row index gp_col0[g] + i, columns ascending.
   std::vector<int32_t> sparse_units;
   std::vector<int32_t> gp_col0;
   std::vector<int32_t> gp_cptr, gp_row, gp_dpos;
   std::vector<int32_t> gp_aptr, gp_arow, gp_asrc;
-  std::vector<int32_t> gp_clvl0, gp_clvlb, gp_corder;
   std::vector<int32_t> gp_lrp, gp_lci, gp_lpos;
   std::vector<int32_t> gp_urp, gp_uci, gp_upos;
-  std::vector<int32_t> gp_flvl0, gp_flvlb, gp_frow;
-  std::vector<int32_t> gp_blvl0, gp_blvlb, gp_brow;
   std::vector<int32_t> lvl_sparse_ptr, lvl_sparse;  // g by unit level
   std::vector<int32_t> gp_index;                    // per unit: g, or -1
   int64_t gp_nnz = 0;

@@ -1,8 +1,8 @@
 // Independent check of the sparse-LU route's host analysis (gp_plan.cpp):
 // the symbolic factorisation of random unit patterns against a dense
-// boolean elimination without pivoting, the dependency levels of columns and
-// solve rows, the value positions of the row-wise solve tables, and a host
-// emulation of the device kernels' index arithmetic over those tables.
+// boolean elimination without pivoting, the value positions of the row-wise
+// solve tables, and a host emulation of the device kernels' index
+// arithmetic over those tables (columns and rows in the kernels' order).
 // Prints "ok" when every check passes.
 #include <algorithm>
 #include <cmath>
@@ -40,7 +40,8 @@ static std::vector<char> dense_fill(int m, const std::vector<int>& r, const std:
 
 // Host emulation of k_gp_factor and k_gp_solve (gp_lu.cu) for unit g with
 // the kernels' index expressions, every access bounds-checked against the
-// buffers the kernels get; checks L U = A and the solve against A x = b.
+// buffers the kernels get; checks that every column (row) the emulation reads
+// was finished before (the kernels' flags), L U = A and A x = b.
 static void emulate_unit(const Plan& p, int g, int m, const std::vector<int>& r, const std::vector<int>& c,
                          const std::vector<int>& src, const std::vector<double>& a) {
   // The kernel reads vals[asrc]: values indexed by source.
@@ -52,12 +53,12 @@ static void emulate_unit(const Plan& p, int g, int m, const std::vector<int>& r,
   std::vector<double> x(static_cast<size_t>(p.gp_maxm), 0.0);
   auto IN = [](int64_t i, int64_t n) { return i >= 0 && i < n; };
   const int c0 = p.gp_col0[static_cast<size_t>(g)];
-  CHECK(IN(g + 1, static_cast<int64_t>(p.gp_clvl0.size())));
-  for (int t = p.gp_clvl0[static_cast<size_t>(g)]; t < p.gp_clvl0[static_cast<size_t>(g) + 1]; ++t) {
-    CHECK(IN(t + 1, static_cast<int64_t>(p.gp_clvlb.size())));
-    for (int idx = p.gp_clvlb[static_cast<size_t>(t)]; idx < p.gp_clvlb[static_cast<size_t>(t) + 1]; ++idx) {
-      CHECK(IN(idx, static_cast<int64_t>(p.gp_corder.size())));
-      const int j = p.gp_corder[static_cast<size_t>(idx)];
+  CHECK(IN(g + 1, static_cast<int64_t>(p.gp_col0.size())));
+  std::vector<char> done(static_cast<size_t>(m), 0);
+  {
+    // Columns ascending: the order every warp's columns follow, and a
+    // topological order of the column dependencies.
+    for (int j = 0; j < m; ++j) {
       const int cc = c0 + j;
       CHECK(IN(cc + 1, static_cast<int64_t>(p.gp_cptr.size())) && IN(cc + 1, static_cast<int64_t>(p.gp_aptr.size())));
       const int p0 = p.gp_cptr[static_cast<size_t>(cc)], p1 = p.gp_cptr[static_cast<size_t>(cc) + 1];
@@ -76,6 +77,7 @@ static void emulate_unit(const Plan& p, int g, int m, const std::vector<int>& r,
         const int k = p.gp_row[static_cast<size_t>(q)];
         const double u = x[static_cast<size_t>(k)];
         const int kc = c0 + k;
+        CHECK(IN(k, j) && done[static_cast<size_t>(k)]);
         CHECK(IN(kc + 1, static_cast<int64_t>(p.gp_cptr.size())));
         for (int rr = p.gp_dpos[static_cast<size_t>(kc)] + 1; rr < p.gp_cptr[static_cast<size_t>(kc) + 1]; ++rr) {
           CHECK(IN(rr, nv) && IN(p.gp_row[static_cast<size_t>(rr)], p.gp_maxm));
@@ -87,6 +89,7 @@ static void emulate_unit(const Plan& p, int g, int m, const std::vector<int>& r,
         const double v = x[static_cast<size_t>(p.gp_row[static_cast<size_t>(q)])];
         val[static_cast<size_t>(q)] = q > dp ? v / diag : v;
       }
+      done[static_cast<size_t>(j)] = 1;
     }
   }
   // Dense L U against A.
@@ -109,37 +112,35 @@ static void emulate_unit(const Plan& p, int g, int m, const std::vector<int>& r,
       amax = std::max(amax, std::abs(A[static_cast<size_t>(i) * m + j]));
     }
   CHECK(err <= 1e-9 * std::max(1.0, amax));
-  // Solve: forward and backward by row levels, then A x = b.
+  // Solve: rows ascending (L), then descending (U), then A x = b.
   std::vector<double> b(static_cast<size_t>(m)), xs;
   for (int i = 0; i < m; ++i) b[static_cast<size_t>(i)] = std::sin(1.0 + i);
   xs = b;
-  for (int t = p.gp_flvl0[static_cast<size_t>(g)]; t < p.gp_flvl0[static_cast<size_t>(g) + 1]; ++t)
-    for (int idx = p.gp_flvlb[static_cast<size_t>(t)]; idx < p.gp_flvlb[static_cast<size_t>(t) + 1]; ++idx) {
-      CHECK(IN(idx, static_cast<int64_t>(p.gp_frow.size())));
-      const int i = p.gp_frow[static_cast<size_t>(idx)];
-      CHECK(IN(i, m));
+  std::vector<char> ready(static_cast<size_t>(m), 0);
+  for (int i = 0; i < m; ++i)
+    {
       const int gr = c0 + i;
       double sum = xs[static_cast<size_t>(i)];
       for (int q = p.gp_lrp[static_cast<size_t>(gr)]; q < p.gp_lrp[static_cast<size_t>(gr) + 1]; ++q) {
         CHECK(IN(q, static_cast<int64_t>(p.gp_lci.size())) && IN(p.gp_lpos[static_cast<size_t>(q)], nv));
-        CHECK(IN(p.gp_lci[static_cast<size_t>(q)], m));
+        CHECK(IN(p.gp_lci[static_cast<size_t>(q)], m) && ready[static_cast<size_t>(p.gp_lci[static_cast<size_t>(q)])]);
         sum -= val[static_cast<size_t>(p.gp_lpos[static_cast<size_t>(q)])] * xs[static_cast<size_t>(p.gp_lci[static_cast<size_t>(q)])];
       }
       xs[static_cast<size_t>(i)] = sum;
+      ready[static_cast<size_t>(i)] = 1;
     }
-  for (int t = p.gp_blvl0[static_cast<size_t>(g)]; t < p.gp_blvl0[static_cast<size_t>(g) + 1]; ++t)
-    for (int idx = p.gp_blvlb[static_cast<size_t>(t)]; idx < p.gp_blvlb[static_cast<size_t>(t) + 1]; ++idx) {
-      CHECK(IN(idx, static_cast<int64_t>(p.gp_brow.size())));
-      const int i = p.gp_brow[static_cast<size_t>(idx)];
-      CHECK(IN(i, m));
+  std::fill(ready.begin(), ready.end(), 0);
+  for (int i = m - 1; i >= 0; --i)
+    {
       const int gr = c0 + i;
       double sum = xs[static_cast<size_t>(i)];
       for (int q = p.gp_urp[static_cast<size_t>(gr)]; q < p.gp_urp[static_cast<size_t>(gr) + 1]; ++q) {
         CHECK(IN(q, static_cast<int64_t>(p.gp_uci.size())) && IN(p.gp_upos[static_cast<size_t>(q)], nv));
-        CHECK(IN(p.gp_uci[static_cast<size_t>(q)], m));
+        CHECK(IN(p.gp_uci[static_cast<size_t>(q)], m) && ready[static_cast<size_t>(p.gp_uci[static_cast<size_t>(q)])]);
         sum -= val[static_cast<size_t>(p.gp_upos[static_cast<size_t>(q)])] * xs[static_cast<size_t>(p.gp_uci[static_cast<size_t>(q)])];
       }
       xs[static_cast<size_t>(i)] = sum / val[static_cast<size_t>(p.gp_dpos[static_cast<size_t>(gr)])];
+      ready[static_cast<size_t>(i)] = 1;
     }
   double rmax = 0.0;
   for (int i = 0; i < m; ++i) {
@@ -187,9 +188,6 @@ int main() {
       for (int q = q0; q < q1 && static_cast<size_t>(q - q0) < rows.size(); ++q)
         CHECK(s.row[static_cast<size_t>(q)] == rows[static_cast<size_t>(q - q0)]);
       CHECK(s.row[static_cast<size_t>(s.dpos[static_cast<size_t>(j)])] == j);
-      for (int q = q0; q < q1; ++q)
-        if (s.row[static_cast<size_t>(q)] < j)
-          CHECK(s.clevel[static_cast<size_t>(s.row[static_cast<size_t>(q)])] < s.clevel[static_cast<size_t>(j)]);
       for (int q = s.aptr[static_cast<size_t>(j)]; q < s.aptr[static_cast<size_t>(j) + 1]; ++q)
         CHECK(have[static_cast<size_t>(s.arow[static_cast<size_t>(q)]) * m + j]);
     }
@@ -212,20 +210,11 @@ int main() {
     ++units;
     const int c0 = p.gp_col0[static_cast<size_t>(g)];
     CHECK(p.gp_col0[static_cast<size_t>(g) + 1] == c0 + m);
-    std::vector<int> flev(static_cast<size_t>(m), -1), blev(static_cast<size_t>(m), -1);
-    for (int t2 = p.gp_flvl0[static_cast<size_t>(g)]; t2 < p.gp_flvl0[static_cast<size_t>(g) + 1]; ++t2)
-      for (int q = p.gp_flvlb[static_cast<size_t>(t2)]; q < p.gp_flvlb[static_cast<size_t>(t2) + 1]; ++q)
-        flev[static_cast<size_t>(p.gp_frow[static_cast<size_t>(q)])] = t2;
-    for (int t2 = p.gp_blvl0[static_cast<size_t>(g)]; t2 < p.gp_blvl0[static_cast<size_t>(g) + 1]; ++t2)
-      for (int q = p.gp_blvlb[static_cast<size_t>(t2)]; q < p.gp_blvlb[static_cast<size_t>(t2) + 1]; ++q)
-        blev[static_cast<size_t>(p.gp_brow[static_cast<size_t>(q)])] = t2;
     for (int i = 0; i < m; ++i) {
-      CHECK(flev[static_cast<size_t>(i)] >= 0 && blev[static_cast<size_t>(i)] >= 0);
       int prev = -1;
       for (int q = p.gp_lrp[static_cast<size_t>(c0 + i)]; q < p.gp_lrp[static_cast<size_t>(c0 + i) + 1]; ++q) {
         const int k = p.gp_lci[static_cast<size_t>(q)];
         CHECK(k < i && k > prev && f[static_cast<size_t>(i) * m + k]);
-        CHECK(flev[static_cast<size_t>(k)] < flev[static_cast<size_t>(i)]);
         CHECK(p.gp_row[static_cast<size_t>(p.gp_lpos[static_cast<size_t>(q)])] == i);
         CHECK(p.gp_lpos[static_cast<size_t>(q)] >= p.gp_cptr[static_cast<size_t>(c0 + k)] &&
               p.gp_lpos[static_cast<size_t>(q)] < p.gp_cptr[static_cast<size_t>(c0 + k) + 1]);
@@ -235,19 +224,12 @@ int main() {
       for (int q = p.gp_urp[static_cast<size_t>(c0 + i)]; q < p.gp_urp[static_cast<size_t>(c0 + i) + 1]; ++q) {
         const int j = p.gp_uci[static_cast<size_t>(q)];
         CHECK(j > prev && f[static_cast<size_t>(i) * m + j]);
-        CHECK(blev[static_cast<size_t>(j)] < blev[static_cast<size_t>(i)]);
         CHECK(p.gp_row[static_cast<size_t>(p.gp_upos[static_cast<size_t>(q)])] == i);
         CHECK(p.gp_upos[static_cast<size_t>(q)] >= p.gp_cptr[static_cast<size_t>(c0 + j)] &&
               p.gp_upos[static_cast<size_t>(q)] < p.gp_cptr[static_cast<size_t>(c0 + j) + 1]);
         prev = j;
       }
     }
-    // Columns by level: every column exactly once.
-    std::vector<int> seen(static_cast<size_t>(m), 0);
-    for (int t2 = p.gp_clvl0[static_cast<size_t>(g)]; t2 < p.gp_clvl0[static_cast<size_t>(g) + 1]; ++t2)
-      for (int q = p.gp_clvlb[static_cast<size_t>(t2)]; q < p.gp_clvlb[static_cast<size_t>(t2) + 1]; ++q)
-        seen[static_cast<size_t>(p.gp_corder[static_cast<size_t>(q)])]++;
-    for (int j = 0; j < m; ++j) CHECK(seen[static_cast<size_t>(j)] == 1);
   }
   // A column without its diagonal after fill is refused.
   {

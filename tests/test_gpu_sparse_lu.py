@@ -11,7 +11,8 @@ bit-identical (==) to the oracle's, rejected blocks are factored dense
 solution is within 1e-9 of the oracle's and the residual within 1e-12, also
 after value-only refactors, after a refactor whose values make a block fail
 the test, and with 8 right-hand sides; the export identity holds; the fill
-limit of option 2 selects the blocks it names."""
+limit of option 2 selects the blocks it names; the kernels' bounded waits
+run out under a one-poll limit and the handle recovers."""
 import os
 import subprocess
 
@@ -194,6 +195,26 @@ def test_fill_limit_selects_sparse_blocks():
             assert (routes[b][0] == SPARSE) == (reason[b] == 0), (b, m, routes[b], reason[b])
     assert over >= 1
     check_against_oracle(s, n, r, c, v, check_sparse_only=True)
+
+
+@pytest.mark.gpu
+def test_bounded_waits_run_out_and_recover():
+    """A one-poll wait limit makes the columns' and rows' waits on each other
+    run out: the factor and the solve return errors, and the same handle
+    works again with the default limit."""
+    n, r, c, v = sparse_block_system(0, SIZES, 0.5)
+    s = engine(n, r, c, v)
+    x = np.ones(n)
+    s.set_option("wait_limit", 1)
+    assert not s.solve_in_place(x.copy())
+    assert "bounded wait" in s.last_error_message()
+    assert not s.refactor_values(v)
+    assert "bounded wait between columns" in s.last_error_message()
+    s.set_option("wait_limit", 0)
+    assert s.refactor_values(v), s.last_error_message()
+    o, counts = check_against_oracle(s, n, r, c, v, check_sparse_only=True)
+    assert counts["sparse"] >= 4
+    check_solution(s, o, n, r, c, v)
 
 
 @pytest.mark.gpu
