@@ -82,19 +82,70 @@ __global__ void __launch_bounds__(32 * kGpWarps) k_gp_factor(GpDev g, const doub
     __syncwarp();
     for (int q = g.aptr[c] + lane; q < g.aptr[c + 1]; q += 32) x[g.arow[q]] = vals[g.asrc[q]];
     __syncwarp();
+    // The update steps, 32 at a time: lane t holds step t's row k and the
+    // bounds of L(:, k), so a step reads no index from global memory; a
+    // step's L entries are loaded before any is applied, and the next
+    // step's first 32 are loaded while this one is applied when its column
+    // is already done.
     int st = kDone;
-    for (int q = p0; q < dp; ++q) {
-      const int k = g.row[q];
-      st = warp_wait(done, k, abort_flag, g.wait_limit);
-      if (st != kDone) break;
-      const double u = x[k];
-      const int kc = c0 + k;
-      const int l1 = g.cptr[kc + 1];
-      for (int r = g.dpos[kc] + 1 + lane; r < l1; r += 32) {
-        const int i = g.row[r];
-        x[i] = __dsub_rn(x[i], __dmul_rn(g.val[r], u));
+    const int nsteps = dp - p0;
+    for (int t0 = 0; t0 < nsteps && st == kDone; t0 += 32) {
+      const int cnt = min(32, nsteps - t0);
+      int my_k = 0, my_l0 = 0, my_l1 = 0;
+      if (lane < cnt) {
+        my_k = g.row[p0 + t0 + lane];
+        my_l0 = g.dpos[c0 + my_k] + 1;
+        my_l1 = g.cptr[c0 + my_k + 1];
       }
-      __syncwarp();
+      bool have = false;  // the first chunk of step t is in (pi, pv)
+      int pi = -1;
+      double pv = 0.0;
+      for (int t = 0; t < cnt; ++t) {
+        const int k = __shfl_sync(0xffffffffu, my_k, t);
+        const int l0 = __shfl_sync(0xffffffffu, my_l0, t);
+        const int l1 = __shfl_sync(0xffffffffu, my_l1, t);
+        st = warp_wait(done, k, abort_flag, g.wait_limit);
+        if (st != kDone) break;
+        int i0 = pi;
+        double v0 = pv;
+        if (!have) {
+          const int r = l0 + lane;
+          i0 = r < l1 ? g.row[r] : -1;
+          v0 = r < l1 ? g.val[r] : 0.0;
+        }
+        have = false;
+        if (t + 1 < cnt) {
+          const int kn = __shfl_sync(0xffffffffu, my_k, t + 1);
+          const int n0 = __shfl_sync(0xffffffffu, my_l0, t + 1);
+          const int n1 = __shfl_sync(0xffffffffu, my_l1, t + 1);
+          int dn = kPending;
+          if (lane == 0) dn = done[kn];
+          dn = __shfl_sync(0xffffffffu, dn, 0);
+          if (dn == kDone) {
+            __threadfence_block();
+            const int r = n0 + lane;
+            pi = r < n1 ? g.row[r] : -1;
+            pv = r < n1 ? g.val[r] : 0.0;
+            have = true;
+          }
+        }
+        const double u = x[k];
+        if (i0 >= 0) x[i0] = __dsub_rn(x[i0], __dmul_rn(v0, u));
+        for (int rb = l0 + 32; rb < l1; rb += 128) {
+          int ii[4];
+          double vv[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = rb + 32 * q + lane;
+            ii[q] = r < l1 ? g.row[r] : -1;
+            vv[q] = r < l1 ? g.val[r] : 0.0;
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (ii[q] >= 0) x[ii[q]] = __dsub_rn(x[ii[q]], __dmul_rn(vv[q], u));
+        }
+        __syncwarp();
+      }
     }
     if (st != kDone) {
       // A column this one reads failed, or the wait ran out: stop, and make
@@ -153,34 +204,71 @@ __global__ void __launch_bounds__(32 * kGpWarps) k_gp_factor(GpDev g, const doub
   }
 }
 
+// Uniform poll until every lane with `need` sees ready[col] leave kPending,
+// at most `limit` polls; false if a wait gave up, the CTA aborted, or an
+// unknown it waited for was given up.
+__device__ __forceinline__ bool warp_wait_cols(bool need, int col, const volatile int* ready, const volatile int* abort,
+                                               int limit) {
+  for (int it = 0;; ++it) {
+    if (__all_sync(0xffffffffu, !need || ready[col] != kPending)) break;
+    if (*abort || it >= limit) return false;
+    if (it > 64) __nanosleep(64);
+  }
+  if (__any_sync(0xffffffffu, need && ready[col] != kDone)) return false;
+  __threadfence_block();
+  return true;
+}
+
 // Warp-wide sum of v * x[c] over the entries [q0, q1) of one row (column
 // indices ci[q], values at positions pos[q]); each entry's unknown is waited
-// for through ready[].  Returns false if a wait gave up.
+// for through ready[].  The entries whose unknowns are final when the row
+// starts are summed and reduced across the warp first; an entry still
+// pending (usually the one row the row was waiting for) is kept by its lane
+// and added after its wait, so the reduction is off the dependent chain.
+// Returns false if a wait gave up.
 __device__ __forceinline__ bool row_dot(const GpDev& g, const int32_t* __restrict__ ci,
                                         const int32_t* __restrict__ pos, int q0, int q1, const double* xs, int ld,
-                                        int nk, const volatile int* ready, const volatile int* abort, double (&acc)[kGpSolveRhs]) {
+                                        int nk, const volatile int* ready, const volatile int* abort,
+                                        double (&acc)[kGpSolveRhs]) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int kk = 0; kk < kGpSolveRhs; ++kk) acc[kk] = 0.0;
+  int lcol = -1;  // this lane's deferred entry
+  double lv = 0.0;
   for (int q = q0; q < q1; q += 32) {
     const bool in = q + lane < q1;
     const int col = in ? ci[q + lane] : 0;
     const double v = in ? g.val[pos[q + lane]] : 0.0;
-    // Uniform poll until every lane's unknown is ready.
-    for (int it = 0;; ++it) {
-      const bool ok = !in || ready[col] != kPending;
-      if (__all_sync(0xffffffffu, ok)) break;
-      if (*abort || it >= g.wait_limit) return false;
-      if (it > 64) __nanosleep(64);
+    const int st = in ? ready[col] : kDone;
+    if (__any_sync(0xffffffffu, st == kGiveUp)) return false;
+    bool defer = in && st == kPending && lcol < 0;
+    if (defer) {
+      lcol = col;
+      lv = v;
     }
-    if (__any_sync(0xffffffffu, in && ready[col] != kDone)) return false;
+    // A lane that already defers one entry waits for its next pending one.
+    if (!warp_wait_cols(in && st == kPending && !defer, col, ready, abort, g.wait_limit)) return false;
     __threadfence_block();
 #pragma unroll
     for (int kk = 0; kk < kGpSolveRhs; ++kk)
-      if (kk < nk && in) acc[kk] = fma(v, xs[kk * ld + col], acc[kk]);
+      if (kk < nk && in && !defer) acc[kk] = fma(v, xs[kk * ld + col], acc[kk]);
   }
 #pragma unroll
   for (int kk = 0; kk < kGpSolveRhs; ++kk) acc[kk] = warp_sum(acc[kk]);
+  const unsigned late = __ballot_sync(0xffffffffu, lcol >= 0);
+  if (late == 0u) return true;
+  if (!warp_wait_cols(lcol >= 0, lcol, ready, abort, g.wait_limit)) return false;
+  double t[kGpSolveRhs];
+#pragma unroll
+  for (int kk = 0; kk < kGpSolveRhs; ++kk) t[kk] = (kk < nk && lcol >= 0) ? lv * xs[kk * ld + lcol] : 0.0;
+  if (__popc(late) == 1) {
+    const int who = __ffs(late) - 1;
+#pragma unroll
+    for (int kk = 0; kk < kGpSolveRhs; ++kk) acc[kk] += __shfl_sync(0xffffffffu, t[kk], who);
+  } else {
+#pragma unroll
+    for (int kk = 0; kk < kGpSolveRhs; ++kk) acc[kk] += warp_sum(t[kk]);
+  }
   return true;
 }
 
