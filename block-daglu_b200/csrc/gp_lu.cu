@@ -82,70 +82,19 @@ __global__ void __launch_bounds__(32 * kGpWarps) k_gp_factor(GpDev g, const doub
     __syncwarp();
     for (int q = g.aptr[c] + lane; q < g.aptr[c + 1]; q += 32) x[g.arow[q]] = vals[g.asrc[q]];
     __syncwarp();
-    // The update steps, 32 at a time: lane t holds step t's row k and the
-    // bounds of L(:, k), so a step reads no index from global memory; a
-    // step's L entries are loaded before any is applied, and the next
-    // step's first 32 are loaded while this one is applied when its column
-    // is already done.
     int st = kDone;
-    const int nsteps = dp - p0;
-    for (int t0 = 0; t0 < nsteps && st == kDone; t0 += 32) {
-      const int cnt = min(32, nsteps - t0);
-      int my_k = 0, my_l0 = 0, my_l1 = 0;
-      if (lane < cnt) {
-        my_k = g.row[p0 + t0 + lane];
-        my_l0 = g.dpos[c0 + my_k] + 1;
-        my_l1 = g.cptr[c0 + my_k + 1];
+    for (int q = p0; q < dp; ++q) {
+      const int k = g.row[q];
+      st = warp_wait(done, k, abort_flag, g.wait_limit);
+      if (st != kDone) break;
+      const double u = x[k];
+      const int kc = c0 + k;
+      const int l1 = g.cptr[kc + 1];
+      for (int r = g.dpos[kc] + 1 + lane; r < l1; r += 32) {
+        const int i = g.row[r];
+        x[i] = __dsub_rn(x[i], __dmul_rn(g.val[r], u));
       }
-      bool have = false;  // the first chunk of step t is in (pi, pv)
-      int pi = -1;
-      double pv = 0.0;
-      for (int t = 0; t < cnt; ++t) {
-        const int k = __shfl_sync(0xffffffffu, my_k, t);
-        const int l0 = __shfl_sync(0xffffffffu, my_l0, t);
-        const int l1 = __shfl_sync(0xffffffffu, my_l1, t);
-        st = warp_wait(done, k, abort_flag, g.wait_limit);
-        if (st != kDone) break;
-        int i0 = pi;
-        double v0 = pv;
-        if (!have) {
-          const int r = l0 + lane;
-          i0 = r < l1 ? g.row[r] : -1;
-          v0 = r < l1 ? g.val[r] : 0.0;
-        }
-        have = false;
-        if (t + 1 < cnt) {
-          const int kn = __shfl_sync(0xffffffffu, my_k, t + 1);
-          const int n0 = __shfl_sync(0xffffffffu, my_l0, t + 1);
-          const int n1 = __shfl_sync(0xffffffffu, my_l1, t + 1);
-          int dn = kPending;
-          if (lane == 0) dn = done[kn];
-          dn = __shfl_sync(0xffffffffu, dn, 0);
-          if (dn == kDone) {
-            __threadfence_block();
-            const int r = n0 + lane;
-            pi = r < n1 ? g.row[r] : -1;
-            pv = r < n1 ? g.val[r] : 0.0;
-            have = true;
-          }
-        }
-        const double u = x[k];
-        if (i0 >= 0) x[i0] = __dsub_rn(x[i0], __dmul_rn(v0, u));
-        for (int rb = l0 + 32; rb < l1; rb += 128) {
-          int ii[4];
-          double vv[4];
-#pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int r = rb + 32 * q + lane;
-            ii[q] = r < l1 ? g.row[r] : -1;
-            vv[q] = r < l1 ? g.val[r] : 0.0;
-          }
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if (ii[q] >= 0) x[ii[q]] = __dsub_rn(x[ii[q]], __dmul_rn(vv[q], u));
-        }
-        __syncwarp();
-      }
+      __syncwarp();
     }
     if (st != kDone) {
       // A column this one reads failed, or the wait ran out: stop, and make

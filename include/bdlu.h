@@ -159,7 +159,7 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  *     USERALGO_GP_PIVOT_TOL or USERALGO_GP_MIN_ABS_DIAG); accepted factors
  *     are bit-identical to the reference's.  A rejected block is factored
  *     dense, for this factor and later ones of the handle.  2 the same for
- *     blocks whose fill is at most "sparse_fill_max" (default 0.1) of m^2.
+ *     blocks whose fill is at most "sparse_fill_max" (default 0.01) of m^2.
  *     Environment settings that relax the gate, scale rows or drop entries
  *     turn the route off.  "sparse_max_n" overrides USERALGO_GP_MAX_N.
  *   "analysis_only": 1 makes analyze stop after the host analysis (no device
