@@ -10,7 +10,7 @@
 //                     so factors are bit-identical
 //   k_scatter_large   value scatter into the arena slots of large units (the
 //                     blocked LU and large-unit solves are in large.cu)
-//   k_solve_scalar / k_solve_dense
+//   k_solve_level     one solve level's scalar rows and small dense units
 //                     level-scheduled block back-substitution with the
 //                     off-diagonal update fused in (ubtf_block_solver.cpp:
 //                     2260-2401): rhs = b - A_cpl x, then the unit's L/U solve
@@ -505,26 +505,6 @@ __global__ void k_scatter_large(DevPlan dp, const double* __restrict__ vals, con
 // ---------------------------------------------------------------------------
 // Solve.  xp holds the solution in permuted order (n x nrhs, ld n).
 // ---------------------------------------------------------------------------
-__global__ void k_solve_scalar(DevPlan dp, const int32_t* __restrict__ rows, int32_t count,
-                               const double* __restrict__ rhs, int32_t ldr, double* __restrict__ xp,
-                               const int32_t* __restrict__ nrhs_p) {
-  const int32_t nrhs = *nrhs_p;
-  const int lane = threadIdx.x & 31;
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= count) return;
-  const int r = rows[w];
-  const int p0 = dp.cpl_ptr[r], p1 = dp.cpl_ptr[r + 1];
-  const int n = dp.n;
-  const double d = dp.sdiag[r];
-  const int src = dp.P[r];
-  for (int k = 0; k < nrhs; ++k) {
-    double acc = 0.0;
-    for (int q = p0 + lane; q < p1; q += 32) acc = fma(dp.cpl_val[q], xp[dp.cpl_col[q] + static_cast<size_t>(k) * n], acc);
-    acc = warp_sum(acc);
-    if (lane == 0) xp[r + static_cast<size_t>(k) * n] = (rhs[src + static_cast<size_t>(k) * ldr] - acc) / d;
-  }
-}
-
 // Small dense units (column-major LU, final row order in dp.lperm).  The
 // unit's m x m factor is copied to shared memory as it lies in the arena;
 // each warp then takes one right-hand side: it forms the pivoted rhs of its
@@ -538,14 +518,51 @@ __global__ void k_solve_scalar(DevPlan dp, const int32_t* __restrict__ rows, int
 constexpr int kSlots = 6;
 static_assert(32 * kSlots >= kLuRowsMax, "register slots must cover the small-unit limit");
 
+// Programmatic dependent launch: the next kernel of the stream may start
+// its prologue once every CTA of this one has started; griddepcontrol.wait
+// blocks until the kernels this one depends on have completed and their
+// writes are visible (it returns at once when the launch had no
+// programmatic dependency).
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// One solve level's scalar rows and small dense units in one launch: CTAs
+// below scal_ctas take the scalar rows (a warp per row: rhs - A_cpl x over
+// the coupling row, divided by the diagonal); the others take one dense unit
+// each.  From the second level on the kernel is launched as a programmatic
+// dependent of the previous one: a dense CTA issues the bulk copy of its
+// factor slot and computes its row order before it waits for the previous
+// level, so the copy and the launch overlap the previous level's tail.
 template <int kS>
-__global__ void __launch_bounds__(kThreads, 4) k_solve_dense(DevPlan dp, const int32_t* __restrict__ units,
+__global__ void __launch_bounds__(kThreads, 4) k_solve_level(DevPlan dp, const int32_t* __restrict__ srows,
+                                                           int32_t nsrows, int32_t scal_ctas,
+                                                           const int32_t* __restrict__ units,
                                                            const double* __restrict__ rhs, int32_t ldr,
                                                            double* __restrict__ xp,
                                                            const int32_t* __restrict__ nrhs_p) {
+  pdl_launch_dependents();
   const int32_t nrhs = *nrhs_p;
+  if (static_cast<int32_t>(blockIdx.x) < scal_ctas) {
+    pdl_wait();
+    const int lane = threadIdx.x & 31;
+    const int n = dp.n;
+    constexpr int kW = kThreads / 32;
+    for (int w = blockIdx.x * kW + (threadIdx.x >> 5); w < nsrows; w += scal_ctas * kW) {
+      const int r = srows[w];
+      const int p0 = dp.cpl_ptr[r], p1 = dp.cpl_ptr[r + 1];
+      const double d = dp.sdiag[r];
+      const int src = dp.P[r];
+      for (int k = 0; k < nrhs; ++k) {
+        double acc = 0.0;
+        for (int q = p0 + lane; q < p1; q += 32) acc = fma(dp.cpl_val[q], xp[dp.cpl_col[q] + static_cast<size_t>(k) * n], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) xp[r + static_cast<size_t>(k) * n] = (rhs[src + static_cast<size_t>(k) * ldr] - acc) / d;
+      }
+    }
+    return;
+  }
   extern __shared__ __align__(16) double T[];
-  const int u = units[blockIdx.x];
+  const int u = units[blockIdx.x - scal_ctas];
   const int s = dp.ustart[u];
   const int m = dp.ustart[u + 1] - s;
   const int n = dp.n;
@@ -593,6 +610,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_solve_dense(DevPlan dp, const i
         "l"(LU), "r"(bytes), "r"(mbar_s)
         : "memory");
   }
+  // Everything above reads only the factors; the right-hand sides read the
+  // unknowns of earlier levels.
+  pdl_wait();
   if (nmine > 0) form(warp);
   // Bounded wait for the copy (phase 0); on a timeout the unit reports a
   // synchronisation failure, waits once more for the copy in flight, and
@@ -960,15 +980,15 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_lu_small<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_solve_dense<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        attr_err = cudaFuncSetAttribute(k_solve_level<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_solve_dense<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        attr_err = cudaFuncSetAttribute(k_solve_level<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_solve_dense<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        attr_err = cudaFuncSetAttribute(k_solve_level<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_solve_dense<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        attr_err = cudaFuncSetAttribute(k_solve_level<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_solve_dense<kSlots>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
+        attr_err = cudaFuncSetAttribute(k_solve_level<kSlots>, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_lu_warp<2, kWarpLuW2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         kWarpLuW2 * 64 * 64 * static_cast<int>(sizeof(double)));
@@ -1442,63 +1462,77 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_
   const Plan& p = plan_;
   const int32_t nl = p.umax_level + 1;
   if (p.large_tiles > 0) cudaMemsetAsync(d_sync_, 0, static_cast<size_t>(sync_words_) * sizeof(int32_t), stream);
-  // Within a level the scalar rows, the small dense units and the large
-  // units are independent: when a level has more than one kind, the others
+  // Within a level the scalar rows and small dense units run as one launch
+  // on `stream`; large units and sparse-LU units, when the level has any,
   // run on auxiliary streams forked from `stream` and joined back, so the
-  // level costs about its slowest part instead of their sum.
+  // level costs about its slowest part instead of their sum.  From the
+  // second level on the fused launch is a programmatic dependent of the
+  // work before it (k_solve_level: its factor staging overlaps that work's
+  // tail; it waits for all of it before reading any unknown).
+  bool prev = false;  // a kernel of an earlier level precedes on `stream`
   for (int32_t l = 0; l < nl; ++l) {
     const int32_t s0 = p.lvl_scalar_ptr[static_cast<size_t>(l)], s1 = p.lvl_scalar_ptr[static_cast<size_t>(l) + 1];
     const int32_t d0 = p.lvl_dense_ptr[static_cast<size_t>(l)], d1 = p.lvl_dense_ptr[static_cast<size_t>(l) + 1];
     const int32_t g0 = p.lvl_large_ptr[static_cast<size_t>(l)], g1 = p.lvl_large_ptr[static_cast<size_t>(l) + 1];
     const int32_t q0 = p.lvl_sparse_ptr.empty() ? 0 : p.lvl_sparse_ptr[static_cast<size_t>(l)];
     const int32_t q1 = p.lvl_sparse_ptr.empty() ? 0 : p.lvl_sparse_ptr[static_cast<size_t>(l) + 1];
-    const bool has_s = s1 > s0, has_d = d1 > d0, has_g = g1 > g0, has_p = q1 > q0;
-    const int kinds = static_cast<int>(has_s) + static_cast<int>(has_d) + static_cast<int>(has_g) +
-                      static_cast<int>(has_p);
-    cudaStream_t st_s = stream, st_d = stream, st_g = stream, st_p = stream;
+    const bool has_sd = s1 > s0 || d1 > d0, has_g = g1 > g0, has_p = q1 > q0;
+    const int kinds = static_cast<int>(has_sd) + static_cast<int>(has_g) + static_cast<int>(has_p);
+    cudaStream_t st_g = stream, st_p = stream;
     if (kinds > 1) {
       cudaEventRecord(fork_ev_[0], stream);
       int used = 0;
-      if (has_d && (has_s)) st_d = aux_[used++];
-      if (has_g && (has_s || has_d)) st_g = aux_[used++];
-      if (has_p && (has_s || has_d || has_g)) st_p = aux_[used++];
+      if (has_g && has_sd) st_g = aux_[used++];
+      if (has_p && (has_sd || has_g)) st_p = aux_[used++];
       for (int q = 0; q < used; ++q) cudaStreamWaitEvent(aux_[q], fork_ev_[0], 0);
     }
     if (has_p) {
       ++launches_solve_;
       gp_solve_launch(dp_, gp_, lvl_sparse_ + q0, q1 - q0, rhs, ldr, xp, nrhs, st_p);
     }
-    if (has_s) {
-      ++launches_solve_;
-      const int warps_per_cta = kThreads / 32;
-      k_solve_scalar<<<(s1 - s0 + warps_per_cta - 1) / warps_per_cta, kThreads, 0, st_s>>>(
-          dp_, lvl_scalar_ + s0, s1 - s0, rhs, ldr, xp, nrhs);
-    }
-    if (has_d) {
+    if (has_sd) {
       ++launches_solve_;
       const size_t mm = static_cast<size_t>(p.lvl_dense_maxm[static_cast<size_t>(l)]);
       const size_t smem = mm * mm * sizeof(double) + 16;
-      const int32_t nu = d1 - d0;
-      const int32_t* lst = lvl_dense_ + d0;
+      const int32_t nsr = s1 - s0, nu = d1 - d0;
+      const int32_t scal_ctas =
+          nsr > 0 ? std::min<int32_t>((nsr + kThreads / 32 - 1) / (kThreads / 32), 4 * num_sms_) : 0;
+      cudaLaunchAttribute attr{};
+      attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr.val.programmaticStreamSerializationAllowed = 1;
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3(static_cast<unsigned>(scal_ctas + nu));
+      cfg.blockDim = dim3(kThreads);
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = stream;
+      cfg.attrs = &attr;
+      cfg.numAttrs = prev ? 1 : 0;
+      const int32_t* sl = lvl_scalar_ + s0;
+      const int32_t* dl = lvl_dense_ + d0;
       switch ((mm + 31) / 32) {
-        case 1: k_solve_dense<1><<<nu, kThreads, smem, st_d>>>(dp_, lst, rhs, ldr, xp, nrhs); break;
-        case 2: k_solve_dense<2><<<nu, kThreads, smem, st_d>>>(dp_, lst, rhs, ldr, xp, nrhs); break;
-        case 3: k_solve_dense<3><<<nu, kThreads, smem, st_d>>>(dp_, lst, rhs, ldr, xp, nrhs); break;
-        case 4: k_solve_dense<4><<<nu, kThreads, smem, st_d>>>(dp_, lst, rhs, ldr, xp, nrhs); break;
-        default: k_solve_dense<kSlots><<<nu, kThreads, smem, st_d>>>(dp_, lst, rhs, ldr, xp, nrhs); break;
+        case 0:
+        case 1: cudaLaunchKernelEx(&cfg, k_solve_level<1>, dp_, sl, nsr, scal_ctas, dl, rhs, ldr, xp, nrhs); break;
+        case 2: cudaLaunchKernelEx(&cfg, k_solve_level<2>, dp_, sl, nsr, scal_ctas, dl, rhs, ldr, xp, nrhs); break;
+        case 3: cudaLaunchKernelEx(&cfg, k_solve_level<3>, dp_, sl, nsr, scal_ctas, dl, rhs, ldr, xp, nrhs); break;
+        case 4: cudaLaunchKernelEx(&cfg, k_solve_level<4>, dp_, sl, nsr, scal_ctas, dl, rhs, ldr, xp, nrhs); break;
+        default:
+          cudaLaunchKernelEx(&cfg, k_solve_level<kSlots>, dp_, sl, nsr, scal_ctas, dl, rhs, ldr, xp, nrhs);
+          break;
       }
+      prev = true;
     }
     large_solve_level(dp_, p, l, lvl_large_, lvl_large_tile0_, d_sync_, rhs, ldr, xp, nrhs, wide, st_g,
                       &launches_solve_);
     if (kinds > 1) {
       int q = 0;
-      for (cudaStream_t sx : {st_d, st_g, st_p}) {
+      for (cudaStream_t sx : {st_g, st_p}) {
         if (sx == stream) continue;
         cudaEventRecord(aux_ev_[q], sx);
         cudaStreamWaitEvent(stream, aux_ev_[q], 0);
         ++q;
       }
     }
+    if (has_g || has_p) prev = true;
   }
 }
 

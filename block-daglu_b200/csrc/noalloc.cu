@@ -16,7 +16,7 @@
 // full-row swaps, multiply then subtract), reading a caller's dense matrix
 // instead of scattered coordinates and writing the factors to the static
 // scratch; the solve kernel applies the pivots and the L and U sweeps as
-// k_solve_dense does.
+// k_solve_level does.
 #include <cuda_runtime.h>
 
 #include <cstdio>
