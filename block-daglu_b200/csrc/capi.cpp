@@ -707,13 +707,10 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
   if (k == "lu_small_threads") {
     // Launch width of the shared-memory LU: 0 the autotuner's choice (or the
     // default rule), 1 one thread per row with the rows in registers (units
-    // up to 96 rows), 2 a thread grid holding a block of the unit in
-    // registers (units up to 96 rows), 32 one warp per unit (units up to 64
-    // rows), 64 / 128 /
+    // up to 96 rows), 32 one warp per unit (units up to 64 rows), 64 / 128 /
     // 256 threads per unit (units up to that many rows).  All give the same
     // factors; a width a bucket cannot take falls back to the tuned one.
-    if (value != 0.0 && value != 1.0 && value != 2.0 && value != 32.0 && value != 64.0 && value != 128.0 &&
-        value != 256.0)
+    if (value != 0.0 && value != 1.0 && value != 32.0 && value != 64.0 && value != 128.0 && value != 256.0)
       return BDLU_INVALID_DIMENSION;
     h->lu_small_threads = static_cast<int32_t>(value);
     return BDLU_OK;

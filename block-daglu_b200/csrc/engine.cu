@@ -221,201 +221,6 @@ __global__ void __launch_bounds__(kT) k_lu_small(DevPlan dp, const double* __res
 }
 
 // ---------------------------------------------------------------------------
-// Register-blocked LU (width code kLuRegWidth): one CTA of TR x TR threads per
-// unit of up to TR*RB rows.  Thread (ti, tj) holds the elements (ti + TR a,
-// tj + TR b), a, b < RB, in registers for the whole factorisation, so an
-// update step moves only the multiplier column and the pivot row through
-// shared memory: 2 RB loads per thread for RB^2 updates, where the
-// shared-memory LU loads three operands and stores one per update.  Register
-// slots are always indexed by unrolled loop counters (a predicate picks the
-// slot of a given row or column), so nothing spills to local memory.
-// Per step k, two barriers:
-//   after the previous step: every thread combines the column-k candidates
-//     (first strict maximum of |a|, ties to the smaller row; the signed
-//     value rides along) and the old a_kk;
-//   the owners of column k form the multipliers (row p's is old a_kk / a_pk,
-//     as after a full-row swap) into their registers and the multiplier
-//     buffer; the owners of rows k and p write both rows to the swap buffers
-//     (old row p is the new row k, the update's pivot row);
-//   after the second barrier rows k and p are exchanged in registers, every
-//     thread updates its active elements (a - l*u, multiply then subtract)
-//     and the owners of column k+1 publish its candidates.
-// The arithmetic per element is the micro-kernel's, so factors, pivots and
-// the row order are bit-identical to k_lu_small's.
-constexpr int kLuRegWidth = 2;
-
-// Column c's candidates from its owners (tj == c % TR) of k_lu_reg: the
-// first strict maximum of |a| over rows >= c with its signed value, per
-// owner thread, and the diagonal entry.
-template <int TR, int RB>
-__device__ __forceinline__ void lu_reg_publish(const double (&r)[RB][RB], int c, int m, int ti, int tj, double* s_best,
-                                               double* s_val, int* s_bi, double* s_akk) {
-  const bool owner = c < m && tj == c % TR;
-  const int cb = c / TR;
-  double best = 0.0, sv = 0.0, dg = 0.0;
-  int bi = m;
-  bool has_dg = false;
-#pragma unroll
-  for (int b = 0; b < RB; ++b) {
-#pragma unroll
-    for (int a = 0; a < RB; ++a) {
-      const int i = ti + TR * a;
-      const double v = r[a][b];
-      const bool in = owner && b == cb && i >= c && i < m;
-      if (in && (bi == m || fabs(v) > best)) {
-        best = fabs(v);
-        sv = v;
-        bi = i;
-      }
-      if (owner && b == cb && i == c) {
-        dg = v;
-        has_dg = true;
-      }
-    }
-  }
-  if (!owner) return;
-  if (has_dg) *s_akk = dg;
-  s_best[ti] = best;
-  s_val[ti] = sv;
-  s_bi[ti] = bi;
-}
-
-template <int TR, int RB>
-__global__ void __launch_bounds__(TR * TR, TR >= 16 ? 2 : 4) k_lu_reg(DevPlan dp, const double* __restrict__ vals,
-                                                  const int32_t* __restrict__ units) {
-  constexpr int T = TR * TR;
-  constexpr int M = TR * RB;
-  extern __shared__ double A[];  // m*m staging of the scattered values (column-major), then the row order
-  __shared__ double lbuf[M], ubuf[M], sbuf[M];
-  __shared__ double s_best[TR], s_val[TR], s_akk;
-  __shared__ int s_bi[TR];
-  const int u = units[blockIdx.x];
-  const int s = dp.ustart[u];
-  const int m = dp.ustart[u + 1] - s;
-  const int tid = threadIdx.x;
-  const int ti = tid % TR, tj = tid / TR;
-  for (int i = tid; i < m * m; i += T) A[i] = 0.0;
-  __syncthreads();
-  for (int64_t e = dp.dent_ptr[u] + tid; e < dp.dent_ptr[u + 1]; e += T) A[dp.dent_pos[e]] = vals[dp.dent_src[e]];
-  __syncthreads();
-  double r[RB][RB];
-#pragma unroll
-  for (int a = 0; a < RB; ++a)
-#pragma unroll
-    for (int b = 0; b < RB; ++b) {
-      const int i = ti + TR * a, j = tj + TR * b;
-      r[a][b] = (i < m && j < m) ? A[j * m + i] : 0.0;
-    }
-  int32_t* piv = dp.piv + s;
-  lu_reg_publish<TR, RB>(r, 0, m, ti, tj, s_best, s_val, s_bi, &s_akk);
-  __syncthreads();
-  for (int k = 0; k < m; ++k) {
-    double best = s_best[0], pv = s_val[0];
-    int p = s_bi[0];
-#pragma unroll
-    for (int w = 1; w < TR; ++w) {
-      const double ob = s_best[w];
-      const int oi = s_bi[w];
-      if (oi != m && (p == m || ob > best || (ob == best && oi < p))) {
-        best = ob;
-        p = oi;
-        pv = s_val[w];
-      }
-    }
-    if (p == m || best == 0.0) {
-      if (tid == 0) report_failure(dp.status, u);
-      return;
-    }
-    const double akk = s_akk;
-    if (tid == 0) piv[k] = p;
-    const int kb = k / TR, kt = k % TR, pb = p / TR, pt = p % TR;
-    if (tj == kt) {
-#pragma unroll
-      for (int b = 0; b < RB; ++b) {
-        if (b != kb) continue;
-#pragma unroll
-        for (int a = 0; a < RB; ++a) {
-          const int i = ti + TR * a;
-          if (i > k && i < m) {
-            const double l = __ddiv_rn(i == p ? akk : r[a][b], pv);
-            r[a][b] = l;
-            lbuf[i] = l;
-          }
-          if (i == k) r[a][b] = pv;
-        }
-      }
-    }
-#pragma unroll
-    for (int a = 0; a < RB; ++a) {
-      const int i = ti + TR * a;
-      if (i != k && i != p) continue;
-#pragma unroll
-      for (int b = 0; b < RB; ++b) {
-        const int j = tj + TR * b;
-        if (j >= m || j == k) continue;
-        if (i == p) ubuf[j] = r[a][b];  // old row p: the new row k
-        if (i == k) sbuf[j] = r[a][b];  // old row k: the new row p
-      }
-    }
-    __syncthreads();
-    double lv[RB], uv[RB];
-#pragma unroll
-    for (int a = 0; a < RB; ++a) {
-      const int i = ti + TR * a;
-      if (p != k && (i == k || i == p)) {
-#pragma unroll
-        for (int b = 0; b < RB; ++b) {
-          const int j = tj + TR * b;
-          if (j < m && j != k) r[a][b] = (i == k) ? ubuf[j] : sbuf[j];
-        }
-      }
-      lv[a] = (i > k && i < m) ? lbuf[i] : 0.0;
-    }
-#pragma unroll
-    for (int b = 0; b < RB; ++b) {
-      const int j = tj + TR * b;
-      uv[b] = (j > k && j < m) ? ubuf[j] : 0.0;
-    }
-#pragma unroll
-    for (int a = 0; a < RB; ++a) {
-      const int i = ti + TR * a;
-      if (i <= k || i >= m) continue;
-#pragma unroll
-      for (int b = 0; b < RB; ++b) {
-        const int j = tj + TR * b;
-        if (j > k && j < m) r[a][b] = __dsub_rn(r[a][b], __dmul_rn(lv[a], uv[b]));
-      }
-    }
-    lu_reg_publish<TR, RB>(r, k + 1, m, ti, tj, s_best, s_val, s_bi, &s_akk);
-    __syncthreads();
-  }
-  double* out = dp.lu + dp.lu_off[u];
-#pragma unroll
-  for (int a = 0; a < RB; ++a)
-#pragma unroll
-    for (int b = 0; b < RB; ++b) {
-      const int i = ti + TR * a, j = tj + TR * b;
-      if (i < m && j < m) out[j * m + i] = r[a][b];
-    }
-  // Final row order (row k of the factor is local row lperm[k]) for the solve.
-  int32_t* ord = reinterpret_cast<int32_t*>(A);
-  for (int k = tid; k < m; k += T) ord[k] = k;
-  __syncthreads();
-  if (tid == 0) {
-    for (int k = 0; k < m; ++k) {
-      const int p = piv[k];
-      if (p != k) {
-        const int32_t t = ord[k];
-        ord[k] = ord[p];
-        ord[p] = t;
-      }
-    }
-  }
-  __syncthreads();
-  for (int k = tid; k < m; k += T) dp.lperm[s + k] = ord[k];
-}
-
-// ---------------------------------------------------------------------------
 // Column-warp LU: one warp per unit of up to 32*R rows (the C2 "column-warp"
 // path), several units per CTA, no CTA barriers.  Lane l holds rows l,
 // l + 32, ... of the unit in registers (all columns, statically indexed: the
@@ -1190,10 +995,6 @@ bool Engine::upload(const Plan& plan, const Decomposition& dec, const CanonicalC
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_lu_queue, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn);
       if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_lu_reg<16, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, 80 * 80 * 8);
-      if (attr_err == cudaSuccess)
-        attr_err = cudaFuncSetAttribute(k_lu_reg<16, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 96 * 8);
-      if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_lu_rows<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 64 * 8);
       if (attr_err == cudaSuccess)
         attr_err = cudaFuncSetAttribute(k_lu_rows<96>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 96 * 8);
@@ -1304,15 +1105,6 @@ void Engine::launch_lu_small(int threads, int32_t units, int32_t mb, cudaStream_
                               st>>>(dp_, d_vals, list, units);
     return;
   }
-  if (threads == kLuRegWidth && mb <= 96) {
-    if (mb <= 16) k_lu_reg<8, 2><<<units, 64, smem, st>>>(dp_, d_vals, list);
-    else if (mb <= 32) k_lu_reg<8, 4><<<units, 64, smem, st>>>(dp_, d_vals, list);
-    else if (mb <= 48) k_lu_reg<8, 6><<<units, 64, smem, st>>>(dp_, d_vals, list);
-    else if (mb <= 64) k_lu_reg<16, 4><<<units, 256, smem, st>>>(dp_, d_vals, list);
-    else if (mb <= 80) k_lu_reg<16, 5><<<units, 256, smem, st>>>(dp_, d_vals, list);
-    else k_lu_reg<16, 6><<<units, 256, smem, st>>>(dp_, d_vals, list);
-    return;
-  }
   if (threads == kLuRowsWidth && mb <= 64) {
     k_lu_rows<64><<<units, 64, smem, st>>>(dp_, d_vals, list);
     return;
@@ -1339,11 +1131,10 @@ static int32_t lu_bucket_class(int32_t mb) {
 
 // Admissible widths of a bucket of units up to mb rows: 32 (one warp per
 // unit, up to 64 rows), kLuRowsWidth (one thread per row, rows in registers,
-// up to 96 rows), kLuRegWidth (a thread grid with a block of the unit in
-// registers, up to 96 rows), and CTA widths with one thread per row at least.
+// up to 96 rows), and CTA widths with one thread per row at least.
 static bool lu_width_ok(int t, int32_t mb) {
   if (t == 32) return mb <= 64;
-  if (t == kLuRowsWidth || t == kLuRegWidth) return mb <= 96;
+  if (t == kLuRowsWidth) return mb <= 96;
   return (t == 64 || t == 128 || t == kThreads) && t >= mb;
 }
 
@@ -1370,10 +1161,10 @@ cudaError_t Engine::tune_lu_small(const double* d_vals, cudaStream_t stream) {
     if (tu.lu_small_threads(lu_bucket_class(mb)) != 0) continue;
     if (!e0 && ((e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess)) break;
     const int32_t q0 = p.small_bucket_ptr[bkt], q1 = p.small_bucket_ptr[bkt + 1];
-    int widths[6], count = 0;
-    for (int t : {32, kLuRowsWidth, kLuRegWidth, 64, 128, kThreads})
+    int widths[5], count = 0;
+    for (int t : {32, kLuRowsWidth, 64, 128, kThreads})
       if (lu_width_ok(t, mb)) widths[count++] = t;
-    float ms[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    float ms[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     int best = widths[count - 1];
     float best_ms = 1e30f;
     for (int c = 0; c < count && e == cudaSuccess; ++c) {

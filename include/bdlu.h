@@ -185,10 +185,8 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  *     pattern (see bdlu_tuner_report).
  *   "lu_small_threads": launch width of the small-unit LU: 0 (default) the
  *     autotuner's, 1 one thread per row with the rows in registers (units up
- *     to 96 rows), 2 a grid of 8 x 8 or 16 x 16 threads each holding a block
- *     of the unit in registers (units up to 96 rows), 32 one warp per unit
- *     (units up to 64 rows), 64 / 128 / 256 threads per unit (units up to
- *     that many rows).  Same factors.
+ *     to 96 rows), 32 one warp per unit (units up to 64 rows), 64 / 128 / 256
+ *     threads per unit (units up to that many rows).  Same factors.
  *   "small_launch": -1 (default) the autotuner's, 0 one launch per size
  *     bucket, 1 one persistent launch over a task queue.  Same factors.
  *   "wait_limit": polls a bounded wait between tiles (large-unit solve

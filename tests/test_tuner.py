@@ -69,12 +69,11 @@ def test_tuner_picks_refactor_schedule_per_pattern(cuda_device, monkeypatch):
     assert os.path.exists(rep["cache"])
 
 
-@pytest.mark.parametrize("width", [1, 2, 32, 64, 128, 256])
+@pytest.mark.parametrize("width", [1, 32, 64, 128, 256])
 def test_every_lu_width_bit_identical_to_oracle(cuda_device, monkeypatch, width):
     """Each launch width of the small-unit LU (1: one thread per row, rows in
-    registers; 2: a thread grid with a block of the unit in registers; 32: one
-    warp per unit, rows in registers; 64 / 128 / 256 threads per unit, unit in
-    shared memory) gives the reference
+    registers; 32: one warp per unit, rows in registers; 64 / 128 / 256
+    threads per unit, unit in shared memory) gives the reference
     micro-kernel's factors and pivots bit for bit on every block of the
     2,000-row block system (units of 10-90 rows; a bucket a width cannot take
     runs the tuned width)."""
