@@ -531,7 +531,7 @@ def run_batch(args, rank, world):
         achieved = traffic / (ph["solve"] * 1e-3) / 1e9
         peak = peaks.get("hbm_gbs", 6650.0)
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": None, "kernel": "solve sweep, 8 rhs (k_solve_scalar / k_solve_dense levels)",
+                    "traffic": None, "kernel": "solve sweep, 8 rhs (k_solve_level levels)",
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"}
     else:
         n8 = 8192
@@ -1094,7 +1094,7 @@ def measure_circuit(args, world, dist, dev):
         achieved = traffic / (ph["solve"] * 1e-3) / 1e9
         peak = peaks.get("hbm_gbs", 6650.0)
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": None, "kernel": "solve sweep (k_solve_scalar / k_solve_dense / k_trsv_tiles levels)",
+                    "traffic": None, "kernel": "solve sweep (k_solve_level / k_trsv_tiles levels)",
                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peaks else "fallback 6650 GB/s"}
     else:
         dgemm = measured_dgemm(dev)
