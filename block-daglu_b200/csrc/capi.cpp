@@ -388,13 +388,22 @@ int bdlu_solve_checked_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, 
       if (!all_finite(B + static_cast<size_t>(k) * ldb, h->n))
         return fail(h, BDLU_NON_FINITE_VALUE, "right-hand side contains NaN or infinity");
   std::string err;
-  double* d_B = h->engine->rhs_buffer(nrhs, err);
-  if (!d_B) return fail(h, BDLU_SOLVE_FAILED, err);
-  cudaError_t e = cudaMemcpy2DAsync(d_B, static_cast<size_t>(h->n) * sizeof(double), B,
-                                    static_cast<size_t>(ldb) * sizeof(double), static_cast<size_t>(h->n) * sizeof(double),
-                                    static_cast<size_t>(nrhs),
-                                    device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream);
-  if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("rhs upload: ") + cudaGetErrorString(e));
+  // The right-hand sides go to the engine's buffer.  A factor redone below
+  // may re-plan the pattern (a sparse-LU unit moved to the dense route),
+  // which replaces every engine buffer, so each redo stages them again from
+  // B, which holds them until the solution is copied out.
+  double* d_B = nullptr;
+  cudaError_t e = cudaSuccess;
+  auto stage = [&]() -> int {
+    d_B = h->engine->rhs_buffer(nrhs, err);
+    if (!d_B) return fail(h, BDLU_SOLVE_FAILED, err);
+    e = cudaMemcpy2DAsync(d_B, static_cast<size_t>(h->n) * sizeof(double), B, static_cast<size_t>(ldb) * sizeof(double),
+                          static_cast<size_t>(h->n) * sizeof(double), static_cast<size_t>(nrhs),
+                          device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return fail(h, BDLU_SOLVE_FAILED, std::string("rhs upload: ") + cudaGetErrorString(e));
+    return BDLU_OK;
+  };
+  if (const int st = stage()) return st;
   const int iters = refine_iters_for(h);
   auto relres = [](const bdlu::SolveResidual& q) {
     const double denom = q.a_inf * q.x_inf + q.b_inf;
@@ -410,19 +419,19 @@ int bdlu_solve_checked_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, 
   };
   auto redo_factor = [&]() -> int {
     if (const int st = do_factor(h, stream, false)) return st;
-    if (!h->engine->restore_rhs(d_B, h->n, nrhs, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
-    return BDLU_OK;
+    return stage();
   };
   if (const int st = solve_once()) return st;
-  // A zero pivot met by an earlier device-side refactor surfaces here; a
-  // refactor that reused the pivot order of large blocks is then redone with
-  // pivoting.
+  // A zero pivot met by a refactor queued without its own status wait
+  // surfaces here; a refactor that reused the pivot order of large blocks
+  // is then redone with pivoting, and one whose sparse-LU unit failed its
+  // pivot test is redone with that unit on the dense route.
   int fst = h->engine->factor_status(stream, err);
   if (fst == 1 || fst < 0 || (fst == 2 && !h->engine->last_factor_reused())) {
     h->factored = false;
     return fail(h, fst < 0 ? BDLU_BACKEND_UNAVAILABLE : BDLU_FACTORIZATION_FAILED, err);
   }
-  if (fst == 2) {
+  if (fst == 2 || fst == 3) {
     if (const int st = redo_factor()) return st;
     if (const int st = solve_once()) return st;
   }
@@ -453,7 +462,7 @@ int bdlu_solve_checked_on(bdlu_solver* h, double* B, int32_t ldb, int32_t nrhs, 
       if (h->last_residual <= kReuseResidualLimit || h->prec_level == 0) break;
       h->prec_level = (h->prec_level == 1) ? 2 : 0;
       if (const int st = do_factor(h, stream, h->engine->last_factor_reused())) return st;
-      if (!h->engine->restore_rhs(d_B, h->n, nrhs, stream, err)) return fail(h, BDLU_SOLVE_FAILED, err);
+      if (const int st = stage()) return st;
       if (const int st = solve_once()) return st;
     }
   }
@@ -560,7 +569,8 @@ int bdlu_refactor_values_device(bdlu_solver* h, const double* d_vals, int64_t nn
   h->engine->set_wait_limit(h->wait_limit);
   if (!h->engine->factor_async(h->engine->values_buffer(), s, err, h->reuse_pivots))
     return fail(h, BDLU_BACKEND_UNAVAILABLE, err);
-  // Zero pivots are reported by the next synchronising call (bdlu_solve_status).
+  // Zero pivots, and sparse-LU units that fail their pivot test, are reported
+  // by the next host-buffer solve, which factors again.
   h->factored = true;
   h->exported = false;
   return BDLU_OK;

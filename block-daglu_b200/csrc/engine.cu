@@ -1608,14 +1608,6 @@ bool Engine::refine_async(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t s
   return true;
 }
 
-bool Engine::restore_rhs(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream, std::string& err) {
-  const int32_t n = plan_.n;
-  BDLU_CUDA(cudaMemcpy2DAsync(d_B, static_cast<size_t>(ldb) * sizeof(double), d_b0_, static_cast<size_t>(n) * sizeof(double),
-                              static_cast<size_t>(n) * sizeof(double), static_cast<size_t>(nrhs), cudaMemcpyDeviceToDevice,
-                              stream));
-  return true;
-}
-
 bool Engine::last_residual(cudaStream_t stream, SolveResidual& out, std::string& err) {
   out = SolveResidual{0, 0, 0, 0};
   if (last_nrhs_ <= 0) return true;

@@ -100,8 +100,6 @@ class Engine {
   // followed by `refine_iters` FP64 refinement steps and the residual norms.
   bool solve_async(double* d_B, int32_t ldb, int32_t nrhs, int32_t refine_iters, cudaStream_t stream,
                    std::string& err);
-  // Copies the right-hand sides saved by the last solve_async back into d_B.
-  bool restore_rhs(double* d_B, int32_t ldb, int32_t nrhs, cudaStream_t stream, std::string& err);
   // One FP64 refinement step on the solution in d_B (from the last solve):
   // r = b - A x, x += A^{-1} r with the current factors; then the residual
   // norms of the new x (read by last_residual).

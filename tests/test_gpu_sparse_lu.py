@@ -10,9 +10,11 @@ bit-identical (==) to the oracle's, rejected blocks are factored dense
 (bit-identical up to 169 rows, pivots equal and within 1e-11 above); the
 solution is within 1e-9 of the oracle's and the residual within 1e-12, also
 after value-only refactors, after a refactor whose values make a block fail
-the test, and with 8 right-hand sides; the export identity holds; the fill
+the test (also through the refactor + solve call that queues the refactor
+with no status wait), and with 8 right-hand sides; the export identity holds; the fill
 limit of option 2 selects the blocks it names; the kernels' bounded waits
 run out under a one-poll limit and the handle recovers."""
+import ctypes
 import os
 import subprocess
 
@@ -151,6 +153,36 @@ def test_refactor_that_fails_the_pivot_test_moves_the_block_dense():
     # The block stays dense for the handle, with the original values too.
     assert s.refactor_values(v), s.last_error_message()
     assert route_of_blocks(s)[b][0] != SPARSE
+
+
+@pytest.mark.gpu
+def test_refactor_solve_without_status_wait_moves_the_failing_block_dense():
+    """bdlu_refactor_solve queues the refactor with no status wait of its own;
+    the solve finds the failed pivot test after its first sweep, factors
+    again with the block on the dense route (a re-plan that replaces every
+    engine buffer) and solves from the caller's right-hand sides."""
+    n, r, c, v = sparse_block_system(0, SIZES, 0.5)
+    s = engine(n, r, c, v)
+    d = s.decomposition()
+    R, P, Q = d["R"], d["P"], d["Q"]
+    routes = route_of_blocks(s)
+    b = max((b for b in range(len(R) - 1) if routes[b] and routes[b][0] == SPARSE),
+            key=lambda b: R[b + 1] - R[b])
+    k = np.nonzero((r == P[R[b]]) & (c == Q[R[b]]))[0]
+    v2 = v.copy()
+    v2[k] *= 1e-9
+    rhs = np.asfortranarray(np.random.default_rng(21).uniform(-1, 1, (n, 2)))
+    X = rhs.copy(order="F")
+    lib = s._lib
+    assert lib.bdlu_refactor_solve(s._h, v2.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), len(v2),
+                                   X.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n, 2) == 0, \
+        s.last_error_message()
+    assert route_of_blocks(s)[b][0] != SPARSE
+    o, _ = check_against_oracle(s, n, r, c, v2)
+    for col in range(2):
+        x_o = o.solve(rhs[:, col])
+        assert np.max(np.abs(X[:, col] - x_o) / np.maximum(1.0, np.abs(x_o))) <= X_TOL
+        assert oracle.metrics(r, c, v2, X[:, col], rhs[:, col])[0] <= RESID_TOL
 
 
 @pytest.mark.gpu
