@@ -161,7 +161,10 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  *     dense, for this factor and later ones of the handle.  2 the same for
  *     blocks whose fill is at most "sparse_fill_max" (default 0.01) of m^2.
  *     Environment settings that relax the gate, scale rows or drop entries
- *     turn the route off.  "sparse_max_n" overrides USERALGO_GP_MAX_N.
+ *     turn the route off.  "sparse_max_n" overrides USERALGO_GP_MAX_N.  A
+ *     device-pointer refactor does not wait for the factor's status: a block
+ *     that fails the test there is found, like a zero pivot, by the next
+ *     host-buffer solve, which factors again with the block dense.
  *   "analysis_only": 1 makes analyze stop after the host analysis (no device
  *     upload); factor then reports BDLU_BACKEND_UNAVAILABLE.  For structure
  *     inspection on machines without a GPU.
