@@ -123,6 +123,7 @@ int do_factor(bdlu_solver* h, cudaStream_t stream, bool reuse) {
   h->engine->set_precision(h->mixed ? h->prec_level : 0);
   h->engine->set_lu_small_width(h->lu_small_threads);
   h->engine->set_blocking_sync(h->blocking_sync);
+  h->engine->set_programmatic_launch(h->programmatic_launch);
   h->engine->set_small_mode(h->small_mode);
   const int32_t sched = schedule_for(h);
   h->engine->set_refactor_schedule(sched);
@@ -730,6 +731,16 @@ int bdlu_set_option(bdlu_solver* h, const char* key, double value) {
     // spinning (for processes where many threads wait at once).
     h->blocking_sync = value != 0.0;
     if (h->engine) h->engine->set_blocking_sync(h->blocking_sync);
+    return BDLU_OK;
+  }
+  if (k == "programmatic_launch") {
+    // 1 (default): from the second solve level on, each level's launch is a
+    // programmatic dependent of the previous one (its factor staging and
+    // launch overlap the previous level).  0: plain stream order, for
+    // processes that run many solves on many streams at once.
+    if (value != 0.0 && value != 1.0) return BDLU_INVALID_DIMENSION;
+    h->programmatic_launch = value != 0.0;
+    if (h->engine) h->engine->set_programmatic_launch(h->programmatic_launch);
     return BDLU_OK;
   }
   if (k == "small_launch") {

@@ -49,6 +49,7 @@ struct bdlu_solver {
   int32_t lu_small_threads = 0;   // forced shared-memory LU width (0: autotuned; Engine::set_lu_small_width)
   int32_t small_mode = -1;        // small units per bucket (0) or in one queue launch (1); -1 autotuned
   bool blocking_sync = false;     // waits sleep on blocking-sync events (Engine::set_blocking_sync)
+  bool programmatic_launch = true;  // Engine::set_programmatic_launch
   // Sparse-LU route (gp.h): configuration of the current analysis (the
   // environment's, overridden by the options below; -1 = not set) and, by
   // first permuted row, the reasons of units a factor's pivot test sent to

@@ -1506,7 +1506,7 @@ void Engine::solve_core(const double* rhs, int32_t ldr, double* xp, const int32_
       cfg.dynamicSmemBytes = smem;
       cfg.stream = stream;
       cfg.attrs = &attr;
-      cfg.numAttrs = prev ? 1 : 0;
+      cfg.numAttrs = (prev && pdl_) ? 1 : 0;
       const int32_t* sl = lvl_scalar_ + s0;
       const int32_t* dl = lvl_dense_ + d0;
       switch ((mm + 31) / 32) {

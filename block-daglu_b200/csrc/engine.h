@@ -142,6 +142,15 @@ class Engine {
   // threads waiting at once, as the serving loop's workers do).
   cudaError_t wait(cudaStream_t stream);
   void set_blocking_sync(bool b) { blocking_sync_ = b; }
+  // Solve levels launched as programmatic dependents of the previous level
+  // (on by default).  Off where many streams share the GPU: a dependent's
+  // CTAs hold their SM slots while they wait for the previous level, slots
+  // the other streams' ready work could use.  Captured graphs are dropped.
+  void set_programmatic_launch(bool on) {
+    if (on == pdl_) return;
+    pdl_ = on;
+    drop_graphs();
+  }
   // Residual norms of the last solve (synchronises the stream), worst column.
   bool last_residual(cudaStream_t stream, SolveResidual& out, std::string& err);
 
@@ -186,6 +195,7 @@ class Engine {
   static constexpr size_t kReadbackBytes = 32 + kReadbackNorms * sizeof(unsigned long long);
   char* readback_ = nullptr;
   bool blocking_sync_ = false;
+  bool pdl_ = true;
   cudaEvent_t wait_ev_ = nullptr;
   bool readback_pinned_ = true;
   int32_t forced_small_mode_ = -1;

@@ -327,6 +327,10 @@ int32_t bdlu_server_add_pattern(bdlu_server* s, const int32_t* rows, const int32
   // Many workers wait for the device at once: they sleep on blocking-sync
   // events instead of each spinning a host core.
   if (st == BDLU_OK) st = bdlu_set_option(p->h, "blocking_sync", 1);
+  // Plain stream order for the solve levels: with many request streams in
+  // flight, a level launched ahead as a programmatic dependent holds SM
+  // slots while it waits, which the other streams' ready work could use.
+  if (st == BDLU_OK) st = bdlu_set_option(p->h, "programmatic_launch", 0);
   if (st == BDLU_OK) {
     std::lock_guard<std::mutex> lk(s->mu);
     st = bdlu_set_option(p->h, "precision", s->precision);

@@ -190,6 +190,11 @@ int bdlu_phase_times(bdlu_solver* h, double* ms, int32_t cap);
  *     autotuner's, 1 one thread per row with the rows in registers (units up
  *     to 96 rows), 32 one warp per unit (units up to 64 rows), 64 / 128 / 256
  *     threads per unit (units up to that many rows).  Same factors.
+ *   "programmatic_launch": 1 (default) launches each solve level from the
+ *     second on as a programmatic dependent of the previous one (its factor
+ *     staging and launch overlap the previous level); 0 keeps plain stream
+ *     order, for processes that run many solves on many streams at once
+ *     (the serving loop does).  Same results.
  *   "small_launch": -1 (default) the autotuner's, 0 one launch per size
  *     bucket, 1 one persistent launch over a task queue.  Same factors.
  *   "wait_limit": polls a bounded wait between tiles (large-unit solve
