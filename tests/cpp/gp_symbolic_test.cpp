@@ -2,13 +2,15 @@
 // the symbolic factorisation of random unit patterns against a dense
 // boolean elimination without pivoting, the value positions of the row-wise
 // solve tables, and a host emulation of the device kernels' index
-// arithmetic over those tables (columns and rows in the kernels' order).
-// Prints "ok" when every check passes.
+// arithmetic over those tables (columns and rows in the kernels' order); and
+// the route's configuration from the environment.  Prints "ok" when every
+// check passes.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <random>
+#include <string>
 #include <vector>
 
 #include "gp.h"
@@ -151,7 +153,49 @@ static void emulate_unit(const Plan& p, int g, int m, const std::vector<int>& r,
   CHECK(rmax <= 1e-8);
 }
 
+// The route's configuration from the reference's environment knobs
+// (ubtf_block_solver.cpp:87-182), BLOCKDAGLU_ names over USERALGO_ ones.
+static void check_config() {
+  static const char* kNames[] = {"SPARSE_LU_KERNEL", "GP_MAX_N", "GP_FORCE", "DENSE_BLOCK_MAX", "GP_DIAG_TOL",
+                                 "GP_PIVOT_TOL", "GP_MIN_ABS_DIAG", "GP_REQUIRE_NO_SWAPS", "GP_SWAP_MAX",
+                                 "GP_SWAP_MAX_N", "GP_REQUIRE_NO_TINY_PIVOTS", "GP_SCALE", "GP_DROP_TOL"};
+  auto clear = [] {
+    for (const char* n : kNames) {
+      unsetenv((std::string("USERALGO_") + n).c_str());
+      unsetenv((std::string("BLOCKDAGLU_") + n).c_str());
+    }
+  };
+  clear();
+  GpConfig c = gp_config_from_env();
+  CHECK(c.mode == 0 && c.max_n == 4096 && c.dense_max == 64 && !c.force && !c.unsupported);
+  CHECK(c.diag_tol == 1e-3 && c.pivot_tol == 1e-12 && c.min_abs_diag == 1e-12);
+  setenv("USERALGO_SPARSE_LU_KERNEL", "GPLU", 1);
+  CHECK(gp_config_from_env().mode == 1);
+  setenv("BLOCKDAGLU_SPARSE_LU_KERNEL", "klu", 1);
+  CHECK(gp_config_from_env().mode == 0);
+  unsetenv("BLOCKDAGLU_SPARSE_LU_KERNEL");
+  setenv("USERALGO_GP_MAX_N", "80", 1);
+  setenv("USERALGO_GP_DIAG_TOL", "0.5", 1);
+  setenv("USERALGO_GP_MIN_ABS_DIAG", "-1", 1);  // negative: ignored
+  c = gp_config_from_env();
+  CHECK(c.max_n == 80 && c.diag_tol == 0.5 && c.min_abs_diag == 1e-12 && !c.unsupported);
+  setenv("USERALGO_GP_MAX_N", "0", 1);  // not positive: ignored
+  CHECK(gp_config_from_env().max_n == 4096);
+  // Settings the device route does not implement turn it off.
+  const char* relax[][2] = {{"USERALGO_GP_REQUIRE_NO_SWAPS", "0"}, {"USERALGO_GP_SWAP_MAX", "2"},
+                            {"USERALGO_GP_REQUIRE_NO_TINY_PIVOTS", "0"}, {"USERALGO_GP_SCALE", "1"},
+                            {"BLOCKDAGLU_GP_DROP_TOL", "1e-3"}};
+  for (const auto& kv : relax) {
+    setenv(kv[0], kv[1], 1);
+    CHECK(gp_config_from_env().unsupported);
+    unsetenv(kv[0]);
+  }
+  CHECK(!gp_config_from_env().unsupported);
+  clear();
+}
+
 int main() {
+  check_config();
   std::mt19937 rng(12345);
   Plan p;
   int units = 0;
