@@ -4,7 +4,8 @@ against the oracle (or_factor_gp, itself bit-identical to the reference's own
 gp_lu.cpp, tests/test_gp_oracle.py), on the engine's own ordering.
 
 CPU: the host symbolic analysis against a dense boolean elimination
-(tests/cpp/gp_symbolic_test.cpp).
+(tests/cpp/gp_symbolic_test.cpp) and the plan's routing of sparse units
+(tests/cpp/gp_plan_test.cpp).
 GPU: the same blocks take the sparse route; accepted sparse factors are
 bit-identical (==) to the oracle's, rejected blocks are factored dense
 (bit-identical up to 169 rows, pivots equal and within 1e-11 above); the
@@ -34,17 +35,30 @@ LARGE_TOL = 1e-11
 SPARSE = 3  # bdlu_get_unit_routes route of a sparse unit
 
 
-def test_symbolic_matches_dense_elimination(tmp_path):
+def run_cpp_check(tmp_path, name):
     lib = os.path.join(ROOT, "block-daglu_b200", "lib")
-    exe = str(tmp_path / "gp_symbolic")
+    exe = str(tmp_path / name)
     cmd = ["g++", "-std=c++17", "-O1", "-Wall", "-Wextra", "-Werror", "-I" + os.path.join(ROOT, "include"),
            "-I" + os.path.join(ROOT, "block-daglu_b200", "csrc"), "-I/usr/local/cuda/include",
-           os.path.join(ROOT, "tests", "cpp", "gp_symbolic_test.cpp"), "-L" + lib, "-lbdlu", "-Wl,-rpath," + lib,
-           "-o", exe]
+           os.path.join(ROOT, "tests", "cpp", name + ".cpp"), "-L" + lib, "-lbdlu", "-Wl,-rpath," + lib, "-o", exe]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     r = subprocess.run([exe], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip().splitlines()[-1] == "ok", r.stdout + r.stderr
+
+
+def test_symbolic_matches_dense_elimination(tmp_path):
+    """gp_symbolic against a dense boolean elimination, the kernels' index
+    arithmetic emulated with bounds checks, and the environment knobs."""
+    run_cpp_check(tmp_path, "gp_symbolic_test")
+
+
+def test_plan_routes_sparse_units(tmp_path):
+    """build_plan with the route on: sparse units leave the dense tables and
+    arena, appear once per level, and map back to the canonical entries; the
+    fill limit, earlier rejections and an unsupported setting keep units
+    dense."""
+    run_cpp_check(tmp_path, "gp_plan_test")
 
 
 def engine(n, r, c, v, mode=1, fill_max=None):
